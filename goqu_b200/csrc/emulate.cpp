@@ -1,0 +1,95 @@
+// Host emulation of the tile-pass programs, for CPU tests of the scheduler.
+//
+// Runs the exact device code path of tile_core.cuh (the same run_phase /
+// apply_op functions and the same program tables) with CTAs, phases and
+// threads executed one after another, so that scheduling, swizzle and index
+// tables can be checked against the oracle without a GPU. It is built into
+// libgqb200_emu.so, which only the tests load.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "schedule.hpp"
+#include "tile_core.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+template <class T>
+void run_program(std::vector<gq::cplx<T>>& st, const gq::Program& prog) {
+    std::vector<gq::cplx<T>> pool(prog.pool.size());
+    for (size_t i = 0; i < pool.size(); ++i) pool[i] = {(T)prog.pool[i].re, (T)prog.pool[i].im};
+    for (const gq::PassDesc& pd : prog.passes) {
+        const int m = pd.m;
+        const uint32_t tpb = 1u << (m - gq::RQ);
+        const uint64_t n_cta = 1ull << pd.n_outer;
+        std::vector<gq::cplx<T>> sm(1u << m);
+        for (uint64_t cta = 0; cta < n_cta; ++cta) {
+            const uint64_t base = gq::cta_base(pd, cta);
+            for (uint32_t lin = 0; lin < (1u << m); ++lin) {
+                uint64_t goff;
+                uint32_t slot;
+                gq::linear_slot(pd, lin, goff, slot);
+                sm[slot] = st[base | goff];
+            }
+            for (int p = 0; p < pd.n_phases; ++p) {
+                const gq::PhaseDesc& ph = prog.phases[pd.phase0 + p];
+                for (uint32_t t = 0; t < tpb; ++t)
+                    gq::run_phase<T>(sm.data(), ph, prog.ops.data(), pool.data(), t, m - gq::RQ, base);
+            }
+            for (uint32_t lin = 0; lin < (1u << m); ++lin) {
+                uint64_t goff;
+                uint32_t slot;
+                gq::linear_slot(pd, lin, goff, slot);
+                st[base | goff] = sm[slot];
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gqx_last_error(void) { return g_err.c_str(); }
+
+// Applies ops to a host state (2^nq interleaved doubles) through the
+// scheduler and the tile-pass code, emulated on the CPU. precision GQ_C64
+// runs the float instantiation. Returns GQ_OK or an error code.
+int gqx_emulate_sv(int nq, int precision, double* state, const gq_op* ops, size_t n_ops, int tile_qubits,
+                   int budget, int64_t* passes_out, int64_t* phases_out) {
+    const int nphys = nq < gq::RQ ? gq::RQ : nq;
+    std::vector<gq::NGate> gates;
+    for (size_t i = 0; i < n_ops; ++i) {
+        int rc = gq::normalize_op(ops[i], nq, gates, g_err);
+        if (rc != GQ_OK) return rc;
+    }
+    gq::SchedOptions opt;
+    if (tile_qubits > 0) opt.tile_qubits = tile_qubits;
+    if (budget > 0) opt.budget = budget;
+    opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
+    opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    gq::Program prog;
+    gq::schedule(gates, nphys, opt, prog);
+    const uint64_t n = 1ull << nphys;
+    if (precision == GQ_C64) {
+        std::vector<gq::cplx<float>> st(n, {0.f, 0.f});
+        for (uint64_t i = 0; i < (1ull << nq); ++i) st[i] = {(float)state[2 * i], (float)state[2 * i + 1]};
+        run_program<float>(st, prog);
+        for (uint64_t i = 0; i < (1ull << nq); ++i) {
+            state[2 * i] = st[i].x;
+            state[2 * i + 1] = st[i].y;
+        }
+    } else {
+        std::vector<gq::cplx<double>> st(n, {0.0, 0.0});
+        std::memcpy(st.data(), state, sizeof(double) * 2 * (1ull << nq));
+        run_program<double>(st, prog);
+        std::memcpy(state, st.data(), sizeof(double) * 2 * (1ull << nq));
+    }
+    if (passes_out) *passes_out = (int64_t)prog.passes.size();
+    if (phases_out) *phases_out = (int64_t)prog.phases.size();
+    return GQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,514 @@
+// Gate analysis and pass / phase scheduling (see schedule.hpp).
+#include "schedule.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <random>
+
+namespace gq {
+
+namespace {
+
+inline bool is_one(Z z) { return z.re == 1.0 && z.im == 0.0; }
+inline bool is_zero(Z z) { return z.re == 0.0 && z.im == 0.0; }
+inline bool eq(Z a, Z b) { return a.re == b.re && a.im == b.im; }
+
+int popc(uint64_t v) { return __builtin_popcountll(v); }
+
+// Is local position p (bit k-1-p of the local index) a control of m?
+bool is_control(const std::vector<Z>& m, int k, int p) {
+    const int dim = 1 << k, bit = 1 << (k - 1 - p);
+    for (int r = 0; r < dim; ++r)
+        for (int c = 0; c < dim; ++c) {
+            if ((r & bit) && (c & bit)) continue;
+            const Z v = m[r * dim + c];
+            if (r == c ? !is_one(v) : !is_zero(v)) return false;
+        }
+    return true;
+}
+
+// Restricts m to the block where local position p is 1.
+std::vector<Z> restrict_to_one(const std::vector<Z>& m, int k, int p) {
+    const int dim = 1 << k, bit = 1 << (k - 1 - p), nd = dim >> 1;
+    std::vector<Z> out(nd * nd);
+    auto squeeze = [&](int x) {  // drop bit `bit` from x
+        const int lo = x & (bit - 1), hi = (x >> 1) & ~(bit - 1);
+        return hi | lo;
+    };
+    for (int r = 0; r < dim; ++r) {
+        if (!(r & bit)) continue;
+        for (int c = 0; c < dim; ++c) {
+            if (!(c & bit)) continue;
+            out[squeeze(r) * nd + squeeze(c)] = m[r * dim + c];
+        }
+    }
+    return out;
+}
+
+int cost_of(KType t) {
+    switch (t) {
+        case K_U1: return 8;
+        case K_U2: return 16;
+        case K_U3: return 32;
+        case K_U4: return 64;
+        case K_DIAG: return 3;
+        case K_RESET: return 4;
+        default: return 1;
+    }
+}
+
+// Bit 63 is no qubit: it marks ops that commute with every unitary but not
+// with a reset (a phase on the whole state), so only a deferred reset, which
+// blocks all bits, holds them back.
+constexpr uint64_t kGlobalBit = 1ull << 63;
+
+void finish(NGate& g) {
+    g.nd_mask = 0;
+    g.d_mask = g.ctrl | kGlobalBit;
+    if (g.type == K_DIAG) {
+        for (int q : g.targets) g.d_mask |= 1ull << q;
+    } else if (g.type != K_PHASE) {
+        for (int q : g.targets) g.nd_mask |= 1ull << q;
+    }
+    g.cost = cost_of(g.type);
+}
+
+}  // namespace
+
+int analyze_matrix(const std::vector<Z>& m0, const std::vector<int>& qubits0, uint64_t ctrl, int src,
+                   std::vector<NGate>& out, std::string& err) {
+    std::vector<Z> m = m0;
+    std::vector<int> qubits = qubits0;
+    // Split off controls until none is left.
+    for (bool found = true; found && !qubits.empty();) {
+        found = false;
+        const int k = (int)qubits.size();
+        for (int p = 0; p < k; ++p) {
+            if (is_control(m, k, p)) {
+                ctrl |= 1ull << qubits[p];
+                m = restrict_to_one(m, k, p);
+                qubits.erase(qubits.begin() + p);
+                found = true;
+                break;
+            }
+        }
+    }
+    const int t = (int)qubits.size();
+    const int dim = 1 << t;
+    NGate g;
+    g.ctrl = ctrl;
+    g.src = src;
+    g.targets = qubits;
+    if (t == 0) {
+        if (is_one(m[0])) return GQ_OK;  // identity
+        g.type = K_PHASE;
+        g.data = {m[0]};
+        finish(g);
+        out.push_back(g);
+        return GQ_OK;
+    }
+    bool diag = true;
+    for (int r = 0; r < dim && diag; ++r)
+        for (int c = 0; c < dim; ++c)
+            if (r != c && !is_zero(m[r * dim + c])) {
+                diag = false;
+                break;
+            }
+    if (diag) {
+        bool all_eq = true, all_one = true;
+        for (int i = 0; i < dim; ++i) {
+            all_eq = all_eq && eq(m[i * dim + i], m[0]);
+            all_one = all_one && is_one(m[i * dim + i]);
+        }
+        if (all_one) return GQ_OK;
+        if (all_eq) {  // a phase times identity on the targets
+            g.type = K_PHASE;
+            g.targets.clear();
+            g.data = {m[0]};
+        } else {
+            g.type = K_DIAG;
+            g.data.resize(dim);
+            for (int i = 0; i < dim; ++i) g.data[i] = m[i * dim + i];
+        }
+        finish(g);
+        out.push_back(g);
+        return GQ_OK;
+    }
+    if (t == 1 && is_zero(m[0]) && is_zero(m[3])) {
+        g.type = K_X;
+        g.data = {m[1], m[2]};
+        g.pure = is_one(m[1]) && is_one(m[2]);
+        finish(g);
+        out.push_back(g);
+        return GQ_OK;
+    }
+    if (t == 2) {
+        bool swap = true;
+        for (int r = 0; r < 4 && swap; ++r)
+            for (int c = 0; c < 4; ++c) {
+                const int want = (r == 1) ? 2 : (r == 2) ? 1 : r;
+                const Z v = m[r * 4 + c];
+                if (c == want ? !is_one(v) : !is_zero(v)) {
+                    swap = false;
+                    break;
+                }
+            }
+        if (swap) {
+            g.type = K_SWAP;
+            finish(g);
+            out.push_back(g);
+            return GQ_OK;
+        }
+    }
+    if (t > RQ) {
+        err = "gate acts densely on " + std::to_string(t) + " qubits after control extraction (max 4)";
+        return GQ_EUNSUPPORTED;
+    }
+    g.type = (KType)(K_U1 + (t - 1));
+    g.data = m;
+    finish(g);
+    out.push_back(g);
+    return GQ_OK;
+}
+
+int normalize_op(const gq_op& op, int nphys, std::vector<NGate>& out, std::string& err) {
+    if (op.kind == GQ_OP_BARRIER) return GQ_OK;
+    if (op.num_qubits < 1 || op.num_qubits > GQ_MAX_OP_QUBITS) {
+        err = "op has " + std::to_string(op.num_qubits) + " qubits";
+        return GQ_EINVAL;
+    }
+    uint64_t seen = 0;
+    for (int i = 0; i < op.num_qubits; ++i) {
+        const int q = op.qubits[i];
+        if (q < 0 || q >= nphys) {
+            err = "qubit " + std::to_string(q) + " out of range";
+            return GQ_EINVAL;
+        }
+        if (seen & (1ull << q)) {
+            err = "duplicate qubit " + std::to_string(q);
+            return GQ_EINVAL;
+        }
+        seen |= 1ull << q;
+    }
+    if (op.kind == GQ_OP_RESET) {
+        NGate g;
+        g.type = K_RESET;
+        g.targets = {op.qubits[0]};
+        finish(g);
+        g.barrier = true;
+        out.push_back(g);
+        return GQ_OK;
+    }
+    if (op.kind == GQ_OP_CHANNEL) {
+        err = "Kraus channels apply to density matrices only";
+        return GQ_EINVAL;
+    }
+    if (!op.matrix) {
+        err = "op has no matrix";
+        return GQ_EINVAL;
+    }
+    int nc = 0;
+    uint64_t ctrl = 0;
+    if (op.kind == GQ_OP_CONTROLLED) {
+        nc = op.num_controls;
+        if (nc < 0 || nc >= op.num_qubits) {
+            err = "bad control count";
+            return GQ_EINVAL;
+        }
+        for (int i = 0; i < nc; ++i) ctrl |= 1ull << op.qubits[i];
+    }
+    const int k = op.num_qubits - nc;
+    if (k > 10) {
+        err = "inner gate on " + std::to_string(k) + " qubits";
+        return GQ_EUNSUPPORTED;
+    }
+    const int dim = 1 << k;
+    std::vector<Z> m(dim * dim);
+    std::memcpy(m.data(), op.matrix, sizeof(Z) * dim * dim);
+    std::vector<int> qs(op.qubits + nc, op.qubits + op.num_qubits);
+    return analyze_matrix(m, qs, ctrl, -1, out, err);
+}
+
+namespace {
+
+struct PhasePlan {
+    uint64_t rmask = 0;
+    std::vector<int> gates;
+};
+
+// Greedy partition of `list` (a valid order) into groups whose non-diagonal
+// qubits fit in `limit` qubits of `allowed`. A gate that does not fit is
+// deferred, and every later gate that does not commute with a deferred gate
+// (shares a qubit non-diagonally) is deferred behind it, so each group is a
+// valid reordering of the sequence.
+template <class Fits>
+void greedy_groups(const std::vector<NGate>& gates, std::vector<int> list, Fits fits,
+                   std::vector<std::vector<int>>& groups, std::vector<uint64_t>& masks, uint64_t seed_mask) {
+    while (!list.empty()) {
+        uint64_t used = seed_mask, bnd = 0, bd = 0;
+        std::vector<int> take, rest;
+        int budget_used = 0;
+        for (size_t i = 0; i < list.size(); ++i) {
+            const NGate& g = gates[list[i]];
+            const bool free = !(g.nd_mask & (bnd | bd)) && !(g.d_mask & bnd) && (!g.barrier || (bnd | bd) == 0);
+            if (free && fits(used | g.nd_mask, budget_used + g.cost, take.empty())) {
+                used |= g.nd_mask;
+                budget_used += g.cost;
+                take.push_back(list[i]);
+                continue;
+            }
+            rest.push_back(list[i]);
+            bnd |= g.barrier ? ~0ull : g.nd_mask;
+            bd |= g.d_mask;
+        }
+        groups.push_back(take);
+        masks.push_back(used);
+        list.swap(rest);
+    }
+}
+
+int rank_gf2(std::vector<uint32_t> v) {
+    int r = 0;
+    for (int bit = 31; bit >= 0; --bit) {
+        int piv = -1;
+        for (size_t i = r; i < v.size(); ++i)
+            if ((v[i] >> bit) & 1u) {
+                piv = (int)i;
+                break;
+            }
+        if (piv < 0) continue;
+        std::swap(v[r], v[piv]);
+        for (size_t i = 0; i < v.size(); ++i)
+            if ((int)i != r && ((v[i] >> bit) & 1u)) v[i] ^= v[r];
+        ++r;
+    }
+    return r;
+}
+
+}  // namespace
+
+void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& opt, Program& prog) {
+    const int m = std::min(opt.tile_qubits, nphys);
+    const int low = std::min(opt.low_qubits, m);
+    const int W = opt.swizzle_width;
+    const uint64_t all = (nphys >= 64) ? ~0ull : ((1ull << nphys) - 1);
+    const uint64_t low_mask = (1ull << low) - 1;
+    prog.gates += (int64_t)gates.size();
+
+    std::vector<int> remaining(gates.size());
+    for (size_t i = 0; i < gates.size(); ++i) remaining[i] = (int)i;
+
+    std::mt19937_64 rng(12345);
+    while (!remaining.empty()) {
+        // ---- pass: the tile holds the targets of every absorbed gate.
+        std::vector<std::vector<int>> pgroups;
+        std::vector<uint64_t> pmasks;
+        {
+            std::vector<int> take, rest;
+            uint64_t T = low_mask, bnd = 0, bd = 0;
+            int used = 0;
+            for (size_t i = 0; i < remaining.size(); ++i) {
+                const NGate& g = gates[remaining[i]];
+                const bool free =
+                    !(g.nd_mask & (bnd | bd)) && !(g.d_mask & bnd) && (!g.barrier || (bnd | bd) == 0);
+                const uint64_t nt = T | g.nd_mask;
+                if (free && popc(nt) <= m && (used + g.cost <= opt.budget || take.empty())) {
+                    T = nt;
+                    used += g.cost;
+                    take.push_back(remaining[i]);
+                    continue;
+                }
+                rest.push_back(remaining[i]);
+                bnd |= g.barrier ? ~0ull : g.nd_mask;
+                bd |= g.d_mask;
+                if ((bnd & all) == all) {  // only unconditioned global phases could still pass
+                    rest.insert(rest.end(), remaining.begin() + i + 1, remaining.end());
+                    break;
+                }
+            }
+            pgroups.push_back(take);
+            pmasks.push_back(T);
+            remaining.swap(rest);
+        }
+        uint64_t T = pmasks[0];
+        for (int q = 0; q < nphys && popc(T) < m; ++q) T |= 1ull << q;  // fill with low qubits
+        const std::vector<int>& absorbed = pgroups[0];
+
+        // ---- phases: register sets of RQ qubits inside the tile.
+        std::vector<std::vector<int>> groups;
+        std::vector<uint64_t> rmasks;
+        greedy_groups(
+            gates, absorbed, [&](uint64_t u, int, bool) { return popc(u) <= RQ; }, groups, rmasks, 0);
+        if (groups.empty()) {  // a pass with no gate cannot happen; keep one empty phase
+            groups.push_back({});
+            rmasks.push_back(0);
+        }
+
+        PassDesc pd;
+        std::memset(&pd, 0, sizeof(pd));
+        pd.m = m;
+        pd.phase0 = (int32_t)prog.phases.size();
+        pd.n_phases = (int32_t)groups.size();
+        int tile_q[MAX_TILE], tb_of[64];
+        int nt = 0;
+        for (int q = 0; q < nphys; ++q) {
+            if (T & (1ull << q)) {
+                tb_of[q] = nt;
+                tile_q[nt++] = q;
+            } else {
+                pd.outer_q[pd.n_outer++] = q;
+            }
+        }
+        for (int b = 0; b < m; ++b) pd.tile_q[b] = tile_q[b];
+
+        // Register sets filled to RQ qubits (highest free tile qubits first).
+        std::vector<uint64_t> rfull(groups.size());
+        for (size_t p = 0; p < groups.size(); ++p) {
+            uint64_t R = rmasks[p];
+            for (int b = m - 1; b >= 0 && popc(R) < RQ; --b) R |= 1ull << tile_q[b];
+            rfull[p] = R;
+        }
+
+        // Swizzle: slot = i ^ S*(i >> W) on the low W bits; choose S so that the
+        // W lowest thread bits of every phase hit distinct bank groups.
+        uint32_t S[MAX_TILE] = {0};
+        const int tbits = m - RQ;
+        if (W > 0 && m > W && tbits >= W) {
+            int best_ok = -1;
+            uint32_t best[MAX_TILE] = {0};
+            for (int attempt = 0; attempt < 512; ++attempt) {
+                uint32_t cand[MAX_TILE] = {0};
+                if (attempt > 0)
+                    for (int b = W; b < m; ++b) cand[b] = (uint32_t)(rng() & ((1u << W) - 1));
+                int ok = 0;
+                for (size_t p = 0; p < groups.size(); ++p) {
+                    std::vector<uint32_t> cols;
+                    for (int b = 0; b < m && (int)cols.size() < W; ++b) {
+                        if (rfull[p] & (1ull << tile_q[b])) continue;
+                        cols.push_back(((b < W) ? (1u << b) : 0u) ^ cand[b]);
+                    }
+                    if (rank_gf2(cols) == W) ++ok;
+                }
+                if (ok > best_ok) {
+                    best_ok = ok;
+                    std::memcpy(best, cand, sizeof(best));
+                }
+                if (ok == (int)groups.size()) break;
+            }
+            std::memcpy(S, best, sizeof(S));
+            prog.conflict_phases += (int64_t)groups.size() - best_ok;
+        }
+        for (int b = 0; b < m; ++b) pd.acol[b] = (1u << b) ^ S[b];
+
+        for (size_t p = 0; p < groups.size(); ++p) {
+            PhaseDesc ph;
+            std::memset(&ph, 0, sizeof(ph));
+            const uint64_t R = rfull[p];
+            int rq[RQ], rtb[RQ], nr = 0;
+            for (int b = 0; b < m; ++b)
+                if (R & (1ull << tile_q[b])) {
+                    rq[nr] = tile_q[b];
+                    rtb[nr] = b;
+                    ++nr;
+                }
+            int nb = 0;
+            for (int b = 0; b < m; ++b)
+                if (!(R & (1ull << tile_q[b]))) {
+                    ph.tslot[nb] = pd.acol[b];
+                    ph.tq[nb] = tile_q[b];
+                    ++nb;
+                }
+            for (int j = 0; j < NREG; ++j) {
+                uint32_t s = 0;
+                uint64_t g = 0;
+                for (int k = 0; k < RQ; ++k)
+                    if ((j >> k) & 1) {
+                        s ^= pd.acol[rtb[k]];
+                        g |= 1ull << rq[k];
+                    }
+                ph.rslot[j] = s;
+                ph.rglob[j] = g;
+            }
+            auto kbit = [&](int q) {
+                for (int k = 0; k < RQ; ++k)
+                    if (rq[k] == q) return k;
+                return -1;
+            };
+            ph.op_begin = (int32_t)prog.ops.size();
+            for (int gi : groups[p]) {
+                const NGate& g = gates[gi];
+                KOp op;
+                std::memset(&op, 0, sizeof(op));
+                op.type = g.type;
+                for (int k = 0; k < RQ; ++k)
+                    if (g.ctrl & (1ull << rq[k])) op.creg |= (uint8_t)(1u << k);
+                op.cmask = g.ctrl & ~R;
+                op.mat = (uint32_t)prog.pool.size();
+                const int t = (int)g.targets.size();
+                if (g.type >= K_U1 && g.type <= K_U4) {
+                    // order[p] = target index whose register bit is the p-th smallest
+                    std::vector<int> order(t);
+                    for (int i = 0; i < t; ++i) order[i] = i;
+                    std::sort(order.begin(), order.end(),
+                              [&](int a, int b) { return kbit(g.targets[a]) < kbit(g.targets[b]); });
+                    uint8_t tk[4] = {0, 0, 0, 0};
+                    for (int i = 0; i < t; ++i) tk[i] = (uint8_t)kbit(g.targets[order[i]]);
+                    op.t0 = tk[0];
+                    op.t1 = tk[1];
+                    op.t2 = tk[2];
+                    const int dim = 1 << t;
+                    auto mapidx = [&](int x) {
+                        int o = 0;
+                        for (int pp = 0; pp < t; ++pp)
+                            if ((x >> pp) & 1) o |= 1 << (t - 1 - order[pp]);
+                        return o;
+                    };
+                    for (int r = 0; r < dim; ++r)
+                        for (int c = 0; c < dim; ++c) prog.pool.push_back(g.data[mapidx(r) * dim + mapidx(c)]);
+                } else if (g.type == K_X || g.type == K_RESET) {
+                    op.t0 = (uint8_t)kbit(g.targets[0]);
+                    op.flags = g.pure ? 1 : 0;
+                    prog.pool.insert(prog.pool.end(), g.data.begin(), g.data.end());
+                } else if (g.type == K_SWAP) {
+                    int a = kbit(g.targets[0]), b = kbit(g.targets[1]);
+                    op.t0 = (uint8_t)std::min(a, b);
+                    op.t1 = (uint8_t)std::max(a, b);
+                } else if (g.type == K_PHASE) {
+                    prog.pool.push_back(g.data[0]);
+                } else if (g.type == K_DIAG) {
+                    // Index layout: register targets (ascending register bit)
+                    // in the low bits, the others (ascending qubit) above.
+                    std::vector<int> reg_t, oth_t;  // target positions
+                    for (int i = 0; i < t; ++i) (kbit(g.targets[i]) >= 0 ? reg_t : oth_t).push_back(i);
+                    std::sort(reg_t.begin(), reg_t.end(),
+                              [&](int a, int b) { return kbit(g.targets[a]) < kbit(g.targets[b]); });
+                    std::sort(oth_t.begin(), oth_t.end(), [&](int a, int b) { return g.targets[a] < g.targets[b]; });
+                    op.nreg = (uint8_t)reg_t.size();
+                    for (int i : oth_t) op.dmask |= 1ull << g.targets[i];
+                    const int dim = 1 << t;
+                    for (int v = 0; v < dim; ++v) {
+                        int orig = 0;
+                        for (size_t pp = 0; pp < reg_t.size(); ++pp)
+                            if ((v >> pp) & 1) orig |= 1 << (t - 1 - reg_t[pp]);
+                        for (size_t pp = 0; pp < oth_t.size(); ++pp)
+                            if ((v >> (reg_t.size() + pp)) & 1) orig |= 1 << (t - 1 - oth_t[pp]);
+                        prog.pool.push_back(g.data[orig]);
+                    }
+                    for (int j = 0; j < NREG; ++j) {
+                        uint64_t ri = 0;
+                        for (size_t pp = 0; pp < reg_t.size(); ++pp)
+                            if ((j >> kbit(g.targets[reg_t[pp]])) & 1) ri |= 1ull << pp;
+                        op.ridx |= ri << (4 * j);
+                    }
+                }
+                prog.ops.push_back(op);
+            }
+            ph.op_end = (int32_t)prog.ops.size();
+            prog.phases.push_back(ph);
+        }
+        (void)tb_of;
+        prog.passes.push_back(pd);
+    }
+}
+
+}  // namespace gq

@@ -1,0 +1,65 @@
+// Host-side gate analysis and pass scheduling for the tile-pass kernel.
+//
+// normalize(): each gq_op becomes an NGate by reading its matrix: control
+//   qubits (identity on their |0> block) are split off, and what remains is
+//   classified as a scalar phase, a diagonal, an X-type swap with phases, a
+//   SWAP, or a dense unitary on 1-4 target qubits. goqu routes gates through
+//   pointer-equality and interface tiers (sim/statevector/kernel2q.go:24-114);
+//   reading the structure from the matrix covers those tiers and every other
+//   gate with the same structure.
+// schedule(): packs the gate list into passes (one launch each) and phases
+//   (register sets of 4 qubits) and emits the device program.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/gqb200.h"
+#include "tile_core.cuh"
+
+namespace gq {
+
+struct Z {
+    double re, im;
+};
+
+struct NGate {
+    KType type = K_NONE;
+    std::vector<int> targets;  // U: matrix order (first = MSB); DIAG: table order
+    uint64_t ctrl = 0;         // control qubits (all must be 1)
+    std::vector<Z> data;       // U: 4^t matrix; X: {p0,p1}; DIAG: 2^t table; PHASE: {s}
+    bool pure = false;         // X: plain swap
+    uint64_t nd_mask = 0;      // qubits acted on non-diagonally (must be in registers)
+    uint64_t d_mask = 0;       // qubits acted on diagonally (controls, diagonal targets)
+    bool barrier = false;      // reset: nonlinear, commutes with nothing
+    int cost = 0;              // FMA per amplitude, for the pass budget
+    int src = -1;              // index of the gq_op it came from
+};
+
+struct SchedOptions {
+    int tile_qubits = 12;  // m
+    int low_qubits = 3;    // lowest qubits always in a tile (coalesced runs)
+    int budget = 96;       // FMA-per-amplitude budget of a pass
+    int swizzle_width = 3; // log2 of the 16-byte (c128) / 8-byte (c64) slots of one bank sweep
+};
+
+struct Program {
+    std::vector<PassDesc> passes;
+    std::vector<PhaseDesc> phases;
+    std::vector<KOp> ops;
+    std::vector<Z> pool;
+    int64_t gates = 0;
+    int64_t conflict_phases = 0;  // phases whose lane groups could not be made conflict free
+};
+
+// Appends the NGates of one op (0 when it is an identity or a barrier).
+// Returns GQ_OK or an error code with `err` set.
+int normalize_op(const gq_op& op, int nphys, std::vector<NGate>& out, std::string& err);
+// Builds an NGate from a dense matrix on `qubits` (first = MSB) with extra
+// controls; used for gates and for density-matrix superoperators.
+int analyze_matrix(const std::vector<Z>& m, const std::vector<int>& qubits, uint64_t ctrl, int src,
+                   std::vector<NGate>& out, std::string& err);
+void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& opt, Program& prog);
+
+}  // namespace gq

@@ -1,0 +1,395 @@
+// Tile-pass core shared by the sm_100a kernel and the host emulator.
+//
+// A pass streams the state through the SMs once. Each CTA owns a tile of 2^m
+// amplitudes: the amplitudes whose index bits outside the pass's m tile qubits
+// equal the CTA's base. The tile is staged in shared memory under an XOR
+// swizzle; the pass then runs "phases": in each phase every thread holds 16
+// amplitudes in registers, spanning 4 register qubits, and applies the gates
+// of that phase to them (controls and diagonal factors may sit on any qubit,
+// since every amplitude's global index is known). Phases exchange data through
+// shared memory. Everything the device needs (tile qubits, swizzle columns,
+// per-phase index tables, ops, matrices) comes from a program the host
+// scheduler emits, so the code below is pure index arithmetic plus complex
+// FMAs and is compiled both for sm_100a and for the host emulator.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define GQ_HD __host__ __device__ __forceinline__
+#else
+#define GQ_HD inline
+#endif
+
+namespace gq {
+
+constexpr int RQ = 4;          // register qubits per thread
+constexpr int NREG = 1 << RQ;  // amplitudes per thread
+constexpr int MAX_TILE = 13;   // tile qubits (2^13 amplitudes per CTA)
+constexpr int MAX_QUBITS = 48; // physical qubits of a state (DM: 2n)
+
+template <class T>
+struct alignas(2 * sizeof(T)) cplx {
+    T x, y;
+};
+
+template <class T>
+GQ_HD cplx<T> cmul(cplx<T> a, cplx<T> b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <class T>
+GQ_HD cplx<T> cfma(cplx<T> m, cplx<T> a, cplx<T> acc) {  // acc + m*a
+    acc.x = acc.x + m.x * a.x;
+    acc.x = acc.x - m.y * a.y;
+    acc.y = acc.y + m.x * a.y;
+    acc.y = acc.y + m.y * a.x;
+    return acc;
+}
+
+enum KType : uint8_t {
+    K_NONE = 0,
+    K_U1 = 1,    // dense 2x2 on register bit t0
+    K_U2 = 2,    // dense 4x4 on register bits t0 < t1 (t0 is local index bit 0)
+    K_U3 = 3,    // dense 8x8 on t0 < t1 < t2
+    K_U4 = 4,    // dense 16x16 on all four register bits
+    K_X = 5,     // [[0,p0],[p1,0]] on t0 (pure swap when flags & 1)
+    K_SWAP = 6,  // swap of register bits t0 < t1
+    K_DIAG = 7,  // diagonal factor d[index]; index = pext(g, dmask) << nreg | ridx[j]
+    K_PHASE = 8, // scalar factor when all controls are set
+    K_RESET = 9, // deterministic reset of register bit t0 (sim/statevector/sim.go:168-186)
+};
+
+// One op as placed in a phase (40 bytes).
+struct KOp {
+    uint8_t type;
+    uint8_t t0, t1, t2;  // target register bits, ascending
+    uint8_t creg;        // control register bits (all must be 1)
+    uint8_t nreg;        // K_DIAG: register-bit part of the table index
+    uint8_t flags;
+    uint8_t pad;
+    uint32_t mat;        // offset into the complex pool
+    uint32_t pad2;
+    uint64_t cmask;      // controls outside the registers (global mask)
+    uint64_t dmask;      // K_DIAG: diagonal qubits outside the registers (global mask)
+    uint64_t ridx;       // K_DIAG: 4-bit register part of the index for each slot j
+};
+
+struct PhaseDesc {
+    int32_t op_begin, op_end;
+    uint32_t rslot[NREG];      // shared-memory slot offset of register slot j
+    uint64_t rglob[NREG];      // global index offset of register slot j
+    uint32_t tslot[MAX_TILE];  // shared-memory slot column of thread bit b
+    int32_t tq[MAX_TILE];      // global qubit of thread bit b
+};
+
+struct PassDesc {
+    int32_t m;        // tile qubits
+    int32_t n_phases;
+    int32_t phase0;   // first PhaseDesc of this pass
+    int32_t n_outer;  // qubits outside the tile (CTA index bits)
+    uint32_t acol[MAX_TILE];     // shared-memory slot of tile bit b (linear staging)
+    int32_t tile_q[MAX_TILE];    // global qubit of tile bit b (ascending)
+    int32_t outer_q[MAX_QUBITS]; // global qubit of CTA-index bit k
+};
+
+template <class T>
+GQ_HD cplx<T> ldc(const cplx<T>* p, uint32_t i) {
+#if defined(__CUDA_ARCH__)
+    return __ldg(p + i);
+#else
+    return p[i];
+#endif
+}
+
+GQ_HD uint64_t pext64(uint64_t v, uint64_t mask) {
+    uint64_t r = 0;
+    int k = 0;
+    while (mask) {
+#if defined(__CUDA_ARCH__)
+        int b = __ffsll((long long)mask) - 1;
+#else
+        int b = __builtin_ctzll(mask);
+#endif
+        r |= ((v >> b) & 1ull) << k;
+        ++k;
+        mask &= mask - 1;
+    }
+    return r;
+}
+
+// ---- register-level gate bodies (S* are register bits, compile-time) -------
+
+template <class T, int S>
+GQ_HD void k_u1(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
+    const cplx<T> m0 = ldc(m, 0), m1 = ldc(m, 1), m2 = ldc(m, 2), m3 = ldc(m, 3);
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (j & (1 << S)) continue;
+        if ((j & creg) != creg) continue;
+        const cplx<T> a0 = a[j], a1 = a[j | (1 << S)];
+        cplx<T> o0 = {T(0), T(0)}, o1 = {T(0), T(0)};
+        o0 = cfma(m0, a0, o0);
+        o0 = cfma(m1, a1, o0);
+        o1 = cfma(m2, a0, o1);
+        o1 = cfma(m3, a1, o1);
+        a[j] = o0;
+        a[j | (1 << S)] = o1;
+    }
+}
+
+template <class T, int S0, int S1>
+GQ_HD void k_u2(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (j & ((1 << S0) | (1 << S1))) continue;
+        if ((j & creg) != creg) continue;
+        const int idx[4] = {j, j | (1 << S0), j | (1 << S1), j | (1 << S0) | (1 << S1)};
+        cplx<T> v[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[c] = a[idx[c]];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            cplx<T> o = {T(0), T(0)};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) o = cfma(ldc(m, r * 4 + c), v[c], o);
+            a[idx[r]] = o;
+        }
+    }
+}
+
+template <class T, int S0, int S1, int S2>
+GQ_HD void k_u3(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (j & ((1 << S0) | (1 << S1) | (1 << S2))) continue;
+        if ((j & creg) != creg) continue;
+        int idx[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            idx[c] = j | ((c & 1) ? (1 << S0) : 0) | ((c & 2) ? (1 << S1) : 0) | ((c & 4) ? (1 << S2) : 0);
+        cplx<T> v[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = a[idx[c]];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            cplx<T> o = {T(0), T(0)};
+#pragma unroll
+            for (int c = 0; c < 8; ++c) o = cfma(ldc(m, r * 8 + c), v[c], o);
+            a[idx[r]] = o;
+        }
+    }
+}
+
+template <class T>
+GQ_HD void k_u4(cplx<T> (&a)[NREG], const cplx<T>* m) {
+    cplx<T> v[NREG];
+#pragma unroll
+    for (int c = 0; c < NREG; ++c) v[c] = a[c];
+#pragma unroll
+    for (int r = 0; r < NREG; ++r) {
+        cplx<T> o = {T(0), T(0)};
+#pragma unroll
+        for (int c = 0; c < NREG; ++c) o = cfma(ldc(m, r * NREG + c), v[c], o);
+        a[r] = o;
+    }
+}
+
+template <class T, int S>
+GQ_HD void k_x(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg, bool pure) {
+    if (pure) {
+#pragma unroll
+        for (int j = 0; j < NREG; ++j) {
+            if (j & (1 << S)) continue;
+            if ((j & creg) != creg) continue;
+            const cplx<T> t = a[j];
+            a[j] = a[j | (1 << S)];
+            a[j | (1 << S)] = t;
+        }
+        return;
+    }
+    const cplx<T> p0 = ldc(m, 0), p1 = ldc(m, 1);
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (j & (1 << S)) continue;
+        if ((j & creg) != creg) continue;
+        const cplx<T> a0 = a[j], a1 = a[j | (1 << S)];
+        a[j] = cmul(p0, a1);
+        a[j | (1 << S)] = cmul(p1, a0);
+    }
+}
+
+template <class T, int S0, int S1>
+GQ_HD void k_swap(cplx<T> (&a)[NREG], uint32_t creg) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (!(j & (1 << S0)) || (j & (1 << S1))) continue;  // j has S0=1, S1=0
+        if ((j & creg) != creg) continue;
+        const int k = (j & ~(1 << S0)) | (1 << S1);
+        const cplx<T> t = a[j];
+        a[j] = a[k];
+        a[k] = t;
+    }
+}
+
+template <class T, int S>
+GQ_HD void k_reset(cplx<T> (&a)[NREG]) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (j & (1 << S)) continue;
+        const cplx<T> a0 = a[j], a1 = a[j | (1 << S)];
+        const T s = a0.x * a0.x + a0.y * a0.y + a1.x * a1.x + a1.y * a1.y;
+#if defined(__CUDA_ARCH__)
+        const T norm = sqrt(s);
+#else
+        const T norm = (T)__builtin_sqrt((double)s);
+#endif
+        a[j] = norm > T(1e-15) ? cplx<T>{norm, T(0)} : cplx<T>{T(0), T(0)};
+        a[j | (1 << S)] = {T(0), T(0)};
+    }
+}
+
+template <class T>
+GQ_HD void k_diag(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* d, uint64_t g0) {
+    const uint32_t hi = (uint32_t)(pext64(g0, op.dmask) << op.nreg);
+    const uint32_t creg = op.creg;
+    if (op.nreg == 0) {
+        const cplx<T> f = ldc(d, hi);
+        if (f.x == T(1) && f.y == T(0)) return;
+#pragma unroll
+        for (int j = 0; j < NREG; ++j)
+            if ((j & creg) == creg) a[j] = cmul(f, a[j]);
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if ((j & creg) != creg) continue;
+        const uint32_t idx = hi | (uint32_t)((op.ridx >> (4 * j)) & 15u);
+        a[j] = cmul(ldc(d, idx), a[j]);
+    }
+}
+
+template <class T>
+GQ_HD void k_phase(cplx<T> (&a)[NREG], const cplx<T> s, uint32_t creg) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j)
+        if ((j & creg) == creg) a[j] = cmul(s, a[j]);
+}
+
+// Applies one op to the thread's 16 amplitudes. g0 is the global index of the
+// thread's register slot 0 (its thread bits and the CTA's base).
+template <class T>
+GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint64_t g0) {
+    if ((g0 & op.cmask) != op.cmask) return;
+    const cplx<T>* m = pool + op.mat;
+    const uint32_t creg = op.creg;
+    switch (op.type) {
+        case K_U1:
+            switch (op.t0) {
+                case 0: k_u1<T, 0>(a, m, creg); break;
+                case 1: k_u1<T, 1>(a, m, creg); break;
+                case 2: k_u1<T, 2>(a, m, creg); break;
+                default: k_u1<T, 3>(a, m, creg); break;
+            }
+            break;
+        case K_U2:
+            switch (op.t0 * 4 + op.t1) {
+                case 1: k_u2<T, 0, 1>(a, m, creg); break;
+                case 2: k_u2<T, 0, 2>(a, m, creg); break;
+                case 3: k_u2<T, 0, 3>(a, m, creg); break;
+                case 6: k_u2<T, 1, 2>(a, m, creg); break;
+                case 7: k_u2<T, 1, 3>(a, m, creg); break;
+                default: k_u2<T, 2, 3>(a, m, creg); break;
+            }
+            break;
+        case K_U3:
+            switch (op.t0 * 16 + op.t1 * 4 + op.t2) {
+                case 0 * 16 + 1 * 4 + 2: k_u3<T, 0, 1, 2>(a, m, creg); break;
+                case 0 * 16 + 1 * 4 + 3: k_u3<T, 0, 1, 3>(a, m, creg); break;
+                case 0 * 16 + 2 * 4 + 3: k_u3<T, 0, 2, 3>(a, m, creg); break;
+                default: k_u3<T, 1, 2, 3>(a, m, creg); break;
+            }
+            break;
+        case K_U4:
+            k_u4<T>(a, m);
+            break;
+        case K_X: {
+            const bool pure = op.flags & 1;
+            switch (op.t0) {
+                case 0: k_x<T, 0>(a, m, creg, pure); break;
+                case 1: k_x<T, 1>(a, m, creg, pure); break;
+                case 2: k_x<T, 2>(a, m, creg, pure); break;
+                default: k_x<T, 3>(a, m, creg, pure); break;
+            }
+            break;
+        }
+        case K_SWAP:
+            switch (op.t0 * 4 + op.t1) {
+                case 1: k_swap<T, 0, 1>(a, creg); break;
+                case 2: k_swap<T, 0, 2>(a, creg); break;
+                case 3: k_swap<T, 0, 3>(a, creg); break;
+                case 6: k_swap<T, 1, 2>(a, creg); break;
+                case 7: k_swap<T, 1, 3>(a, creg); break;
+                default: k_swap<T, 2, 3>(a, creg); break;
+            }
+            break;
+        case K_DIAG:
+            k_diag<T>(a, op, m, g0);
+            break;
+        case K_PHASE:
+            k_phase<T>(a, ldc(m, 0), creg);
+            break;
+        case K_RESET:
+            switch (op.t0) {
+                case 0: k_reset<T, 0>(a); break;
+                case 1: k_reset<T, 1>(a); break;
+                case 2: k_reset<T, 2>(a); break;
+                default: k_reset<T, 3>(a); break;
+            }
+            break;
+        default:
+            break;
+    }
+}
+
+// Global index base of a CTA: bit k of the CTA index goes to outer_q[k].
+GQ_HD uint64_t cta_base(const PassDesc& p, uint64_t cta) {
+    uint64_t g = 0;
+    for (int k = 0; k < p.n_outer; ++k) g |= ((cta >> k) & 1ull) << p.outer_q[k];
+    return g;
+}
+
+// Linear staging: element it*TPB + t of the tile. Returns its global index
+// offset (without the CTA base) and its shared-memory slot.
+GQ_HD void linear_slot(const PassDesc& p, uint32_t lin, uint64_t& goff, uint32_t& slot) {
+    uint64_t g = 0;
+    uint32_t s = 0;
+    for (int b = 0; b < p.m; ++b)
+        if ((lin >> b) & 1u) {
+            g |= 1ull << p.tile_q[b];
+            s ^= p.acol[b];
+        }
+    goff = g;
+    slot = s;
+}
+
+// One thread's work in one phase: gather 16 amplitudes from the staged tile,
+// apply the phase's ops, scatter them back. Threads of a phase touch disjoint
+// slots, so phases only need a barrier between them.
+template <class T>
+GQ_HD void run_phase(cplx<T>* sm, const PhaseDesc& ph, const KOp* ops, const cplx<T>* pool, uint32_t t,
+                     int thread_bits, uint64_t base) {
+    uint32_t sbase = 0;
+    uint64_t g0 = base;
+    for (int b = 0; b < thread_bits; ++b)
+        if ((t >> b) & 1u) {
+            sbase ^= ph.tslot[b];
+            g0 |= 1ull << ph.tq[b];
+        }
+    cplx<T> a[NREG];
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) a[j] = sm[sbase ^ ph.rslot[j]];
+    for (int o = ph.op_begin; o < ph.op_end; ++o) apply_op<T>(a, ops[o], pool, g0);
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) sm[sbase ^ ph.rslot[j]] = a[j];
+}
+
+}  // namespace gq

@@ -1,0 +1,211 @@
+/*
+ * gqb200.h - C ABI of the B200 (sm_100a) statevector / density-matrix engine.
+ *
+ * The engine sits behind goqu's simulator API (github.com/splch/goqu):
+ *   sim/sim.go:9-22                 sim.Simulator {Run, Evolve, StateVector, Close}
+ *   sim/statevector/sim.go:27-382   statevector.New/Run/Evolve/Apply/StateVector/Expect*
+ *   sim/densitymatrix/sim.go:32-313 densitymatrix.New/WithNoise/Run/Evolve/DensityMatrix/...
+ *   algorithm/gradient/gradient.go  CostFunc / ParameterShift (plus a new adjoint method)
+ *   sweep/run.go:27-171             RunSim (batches of bound circuits)
+ * Every function is plain C: pointers, sizes and integer status codes. No
+ * CUDA or C++ types cross the boundary. All functions return GQ_OK (0) on
+ * success; on failure they return a GQ_E* code and gq_last_error() returns a
+ * message for the calling thread.
+ *
+ * Conventions (identical to goqu):
+ *  - amplitude index bit q is qubit q (qubit 0 is the least significant bit);
+ *  - a k-qubit gate matrix is row-major, 2^k x 2^k, interleaved (re, im)
+ *    doubles; its local index uses the FIRST listed qubit as the most
+ *    significant bit (circuit/gate/fixed.go:169-171, 316-317);
+ *  - a density matrix is row-major rho[r * 2^n + c].
+ * A handle is not thread-safe; distinct handles may be used concurrently.
+ */
+#ifndef GQB200_H
+#define GQB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GQ_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define GQ_OK 0
+#define GQ_EINVAL 1        /* bad argument (qubit out of range, size mismatch, ...) */
+#define GQ_ENOMEM 2        /* device or host allocation failed                      */
+#define GQ_ECUDA 3         /* a CUDA runtime call failed                            */
+#define GQ_EUNSUPPORTED 4  /* op kind / size the engine does not handle             */
+#define GQ_ENODEVICE 5     /* no usable sm_100 device                               */
+#define GQ_EDEVICE 6       /* a kernel reported an error status (bounded wait, ...) */
+
+/* ---- precision ----------------------------------------------------------- */
+#define GQ_C128 0 /* complex128 state, FP64 arithmetic                        */
+#define GQ_C64 1  /* complex64 state, FP32 gate arithmetic, FP64 reductions   */
+
+/* ---- op kinds --------------------------------------------------------------
+ * The kind mirrors the dispatch goqu's CPU simulator performs, so the Go shim
+ * can forward what its own type switch found:
+ *   sim/statevector/sim.go:92-157       (Apply: 1q / 2q / 3q / controlled)
+ *   sim/statevector/kernel2q.go:24-114  (pointer-equality and interface tiers)
+ *   sim/statevector/kernel3q.go:10-47
+ *   sim/statevector/kernel_controlled.go:11-41
+ * The GPU engine analyses the matrix itself (diagonal / permutation / control
+ * structure), so the kind is a hint for it; the matrix is always required.   */
+#define GQ_OP_MATRIX 0          /* generic 1-, 2- or 3-qubit matrix                */
+#define GQ_OP_CNOT 1            /* gate.CNOT  (fixed.go:183)                       */
+#define GQ_OP_CZ 2              /* gate.CZ    (fixed.go:199)                       */
+#define GQ_OP_SWAP 3            /* gate.SWAP  (fixed.go:215)                       */
+#define GQ_OP_CY 4              /* gate.CY    (fixed.go:229)                       */
+#define GQ_OP_ISWAP 5           /* gate.ISWAP (fixed.go:245)                       */
+#define GQ_OP_SYCAMORE 6        /* gate.Sycamore (fixed.go:387)                    */
+#define GQ_OP_CCX 7             /* gate.CCX   (fixed.go:329)                       */
+#define GQ_OP_CSWAP 8           /* gate.CSWAP (fixed.go:349)                       */
+#define GQ_OP_CCZ 9             /* gate.CCZ   (fixed.go:364)                       */
+#define GQ_OP_CTRL_DIAG_2Q 10   /* gate.ControlDiagonal2Q (CP, CRZ; gate.go:62-66) */
+#define GQ_OP_DIAG_2Q 11        /* gate.Diagonal2Q (RZZ, ZZ; gate.go:55-59)         */
+#define GQ_OP_CTRL_U_2Q 12      /* gate.ControlU2Q (CRX, CRY; gate.go:69-75)        */
+#define GQ_OP_CONTROLLED 13     /* gate.ControlledGate with >= 4 qubits: controls
+                                   first, `matrix` is the INNER gate's matrix      */
+#define GQ_OP_RESET 14          /* deterministic reset (sim/statevector/sim.go:168) */
+#define GQ_OP_CHANNEL 15        /* density matrix only: Kraus channel; `matrix`
+                                   holds num_kraus matrices back to back           */
+#define GQ_OP_BARRIER 16        /* no-op (barrier / delay / measure on the SV path) */
+
+#define GQ_MAX_OP_QUBITS 16
+#define GQ_MAX_OP_PARAMS 3
+
+/* One operation of a circuit, in circuit order. */
+typedef struct gq_op {
+    int32_t kind;
+    int32_t num_qubits;   /* qubits listed in `qubits`                           */
+    int32_t num_controls; /* GQ_OP_CONTROLLED: how many leading qubits are controls */
+    int32_t num_kraus;    /* GQ_OP_CHANNEL: number of Kraus matrices             */
+    int32_t qubits[GQ_MAX_OP_QUBITS];
+    const double* matrix; /* interleaved complex, row-major (see conventions)    */
+    /* Adjoint differentiation (optional): the op's matrix depends on up to three
+     * circuit parameters; dmatrix[k] = d(matrix)/d(param[param_index[k]]) with
+     * the chain rule of the bound expression already applied. Unused slots
+     * have param_index = -1 and dmatrix = NULL.                                 */
+    int32_t param_index[GQ_MAX_OP_PARAMS];
+    int32_t reserved;
+    const double* dmatrix[GQ_MAX_OP_PARAMS];
+} gq_op;
+
+/* One Pauli string in symplectic form (sim/pauli/pauli.go:19-24, 146-169):
+ * bit q of x_mask set for X or Y on qubit q, bit q of z_mask set for Z or Y. */
+typedef struct gq_pauli_term {
+    double coeff_re;
+    double coeff_im;
+    uint64_t x_mask;
+    uint64_t z_mask;
+} gq_pauli_term;
+
+/* Work counters of the most recent apply / run on a handle. */
+typedef struct gq_stats {
+    int64_t gates_in;        /* ops received (unitary gates, after skipping no-ops) */
+    int64_t passes;          /* full-state passes launched                       */
+    int64_t kernel_launches; /* kernels of this library launched                  */
+    int64_t phases;          /* register phases summed over all passes            */
+    int64_t state_bytes;     /* bytes of one state (2^n * amplitude size)          */
+    double last_ms;          /* device time of the last apply (CUDA events)        */
+} gq_stats;
+
+/* ---- library ------------------------------------------------------------- */
+int gq_abi_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char* gq_last_error(void);
+/* Number of visible sm_100 devices. */
+int gq_device_count(int* count);
+
+/* ---- statevector: replaces statevector.New/Sim (sim/statevector/sim.go) ---- */
+typedef struct gq_sv gq_sv;
+
+/* New(n): state |0...0>. num_qubits in [1, 34] (goqu caps at 28; the GPU
+ * engine is bounded by device memory). Replaces sim/statevector/sim.go:27-35. */
+int gq_sv_create(int num_qubits, int precision, gq_sv** out);
+int gq_sv_destroy(gq_sv* sv);
+int gq_sv_num_qubits(const gq_sv* sv, int* out);
+/* Reset to |0...0> (sim/statevector/sim.go:71-76). */
+int gq_sv_reset(gq_sv* sv);
+/* Apply ops to the current state (sim/statevector/sim.go:92-157). */
+int gq_sv_apply(gq_sv* sv, const gq_op* ops, size_t n_ops);
+/* Evolve: reset then apply (sim/statevector/sim.go:83-86). */
+int gq_sv_evolve(gq_sv* sv, const gq_op* ops, size_t n_ops);
+/* Copy the state to host memory: 2^n interleaved complex values, double for
+ * GQ_C128, float for GQ_C64 (StateVector, sim/statevector/sim.go:61-65).       */
+int gq_sv_get_state(gq_sv* sv, void* host_out, size_t bytes);
+int gq_sv_set_state(gq_sv* sv, const void* host_in, size_t bytes);
+/* p_i = re^2 + im^2 in FP64 (sim/statevector/sim.go:274-280). */
+int gq_sv_probabilities(gq_sv* sv, double* host_out, size_t n);
+/* Inverse-CDF sampling: for each uniform r (caller-supplied, in [0,1)), the
+ * first index i with r < sum_{j<=i} p_j summed sequentially in FP64, else
+ * 2^n - 1 (sampleIndex, sim/statevector/sim.go:288-298). Bit-exact with that
+ * sequential sum. */
+int gq_sv_sample(gq_sv* sv, const double* uniforms, size_t shots, uint64_t* idx_out);
+/* Run for static circuits: Evolve then sample (sim/statevector/sim.go:40-58). */
+int gq_sv_run(gq_sv* sv, const gq_op* ops, size_t n_ops, const double* uniforms,
+              size_t shots, uint64_t* idx_out);
+/* sum_t coeff_t <psi|P_t|psi> as a complex number (pauli.ExpectSum,
+ * sim/pauli/expect_sv.go:21-97); ExpectPauliSum is its real part.            */
+int gq_sv_expect_pauli_sum(gq_sv* sv, const gq_pauli_term* terms, size_t n_terms,
+                           double* out_re, double* out_im);
+/* sum_i (-1)^popcount(i & mask) p_i, unrounded (ExpectationValue before its
+ * 1e-14 rounding, sim/statevector/sim.go:368-382).                           */
+int gq_sv_expect_z_mask(gq_sv* sv, uint64_t mask, double* out);
+/* Adjoint-method gradient of E(theta) = Re <psi(theta)|H|psi(theta)> for the
+ * circuit `ops` applied to |0...0> (new: goqu only has ParameterShift and
+ * FiniteDifference, algorithm/gradient/gradient.go:49-86). grad_out has
+ * n_params entries; op parameters use gq_op.param_index / dmatrix.
+ * The handle's state holds psi(theta) afterwards.                            */
+int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops,
+                           const gq_pauli_term* terms, size_t n_terms,
+                           size_t n_params, double* grad_out, double* energy_out);
+int gq_sv_stats(const gq_sv* sv, gq_stats* out);
+
+/* Engine options (per handle). */
+#define GQ_OPT_TILE_QUBITS 1    /* qubits staged per CTA tile (4..12, default auto) */
+#define GQ_OPT_PASS_BUDGET 2    /* FMA-per-amplitude budget of one pass (0 = auto) */
+#define GQ_OPT_LOW_QUBITS 3     /* lowest qubits always in a tile (coalescing)      */
+#define GQ_OPT_TIMING 4         /* 1: record CUDA events around every apply        */
+int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
+
+/* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */
+typedef struct gq_dm gq_dm;
+
+/* New(n): rho = |0><0|, num_qubits in [1, 15] (goqu: [1, 14],
+ * sim/densitymatrix/sim.go:32-40). */
+int gq_dm_create(int num_qubits, gq_dm** out);
+int gq_dm_destroy(gq_dm* dm);
+int gq_dm_reset(gq_dm* dm);
+/* Apply gates (rho <- U rho U^dagger) and Kraus channels (GQ_OP_CHANNEL,
+ * rho <- sum_k E_k rho E_k^dagger) in order (sim/densitymatrix/sim.go:87-191,
+ * 220-255). GQ_OP_RESET is the trace-preserving reset of sim.go:195-217.     */
+int gq_dm_apply(gq_dm* dm, const gq_op* ops, size_t n_ops);
+int gq_dm_evolve(gq_dm* dm, const gq_op* ops, size_t n_ops);
+/* Copy rho (dim*dim interleaved complex doubles) to host. */
+int gq_dm_get(gq_dm* dm, double* host_out, size_t bytes);
+int gq_dm_set(gq_dm* dm, const double* host_in, size_t bytes);
+/* diag(rho), negatives clamped to 0 (diagonalProbs, measure.go:11-20). */
+int gq_dm_diagonal_probs(gq_dm* dm, double* host_out, size_t n);
+/* sum_t coeff_t Tr(rho P_t) (pauli.ExpectSumDM, sim/pauli/expect_dm.go:9-30). */
+int gq_dm_expect_pauli_sum(gq_dm* dm, const gq_pauli_term* terms, size_t n_terms,
+                           double* out_re, double* out_im);
+int gq_dm_trace(gq_dm* dm, double* out_re, double* out_im);
+/* |Tr(rho^2)| (Purity, sim/densitymatrix/sim.go:265-276). */
+int gq_dm_purity(gq_dm* dm, double* out);
+/* |<psi|rho|psi>| for a host pure state (Fidelity, sim.go:280-291). */
+int gq_dm_fidelity(gq_dm* dm, const double* psi, size_t n, double* out);
+/* Readout-error mixing of `probs` in place, qubit by qubit with (p01, p10)
+ * pairs (ApplyReadoutError, measure.go:29-71); p01[q] < 0 skips qubit q.     */
+int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* uniforms,
+                 size_t shots, uint64_t* idx_out);
+int gq_dm_stats(const gq_dm* dm, gq_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GQB200_H */
