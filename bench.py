@@ -1,0 +1,300 @@
+"""Benchmark: 28-qubit complex128 random-circuit simulation on B200.
+
+Workload (one step): goqu statevector Evolve of a seeded 28-qubit circuit of
+40 layers (U3 with uniform [0, 2 pi) angles on every qubit, then a CNOT
+brickwork) followed by a 28-qubit QFT (algorithm/qpe/qpe.go:170-182): 2080
+gates on a 4 GiB complex128 state, which is 32x the B200 L2 cache, so every
+pass streams HBM (no flush needed). The device is timed with CUDA events on the
+engine's stream; e2e is the public C-ABI call gq_sv_run (Evolve + 1024
+inverse-CDF shots) with the op stream coming from host memory and the sampled
+indices copied back, timed on the host around the call.
+
+--impl reference times the CPU restatement of goqu's pure-Go path (the oracle,
+threaded like goqu's auto-parallel kernels) on this host's cores, on a bounded
+sample of the same circuit (the first gates of the 2080). Multi-GPU runs
+(torchrun) are independent replicas, one 28-qubit state per GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+N_QUBITS = 28
+LAYERS = 40
+SEED = 2028
+SHOTS = 1024
+WORKLOAD = f"statevector {N_QUBITS}q complex128: {LAYERS} U3+CNOT brickwork layers + QFT{N_QUBITS} (2080 gates), {SHOTS} shots"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for k, name in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def build_workload():
+    from goqu_b200 import encode, workloads
+    c = workloads.random_layers_qft(N_QUBITS, LAYERS, SEED)
+    return c, encode.statevector_ops(c), workloads.count_gates(c)
+
+
+def cpu_baseline(stream, gates_total, budget_s=20.0):
+    """Oracle (goqu's CPU algorithm restated, threaded like goqu) on the first
+    gates of the same circuit at full size."""
+    from oracle import binding as orc
+    from goqu_b200 import encode as enc
+    threads = os.cpu_count() or 1
+    state = orc.zero_state(N_QUBITS)
+    sub = enc.OpStream(N_QUBITS)
+    done = 0
+    t_used = 0.0
+    # apply gates one at a time until the time budget is spent
+    ops = stream.array()
+    import ctypes
+    for i in range(len(stream)):
+        one = (type(ops[0]) * 1)(ops[i])
+        t0 = time.perf_counter()
+        rc = orc.lib().or_sv_apply(N_QUBITS, state.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                   ctypes.cast(one, ctypes.POINTER(type(ops[0]))), 1, threads)
+        t_used += time.perf_counter() - t0
+        assert rc == 0
+        done += 1
+        if t_used > budget_s:
+            break
+    del sub
+    rate = done / t_used
+    return {"value": rate, "unit": "gates/s", "cores": threads, "kind": "port",
+            "sample": f"first {done} of {gates_total} gates at {N_QUBITS} qubits (complex128, {t_used:.1f} s), "
+                      f"oracle threaded like goqu's GOMAXPROCS workers"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from goqu_b200 import encode  # noqa: F401
+    c, stream, gates = build_workload()
+    budget = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_baseline(stream, gates, budget_s=min(budget, 3.0))
+    vals = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_baseline(stream, gates, budget_s=budget)
+        vals.append(last["value"])
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": "28q gates/s", "value": value, "unit": "gates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * gates / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "gates": gates, "seed": SEED,
+                       "l2": "state 4 GiB > 126 MB L2 (no flush needed)"},
+            "cpu_baseline": dict(last, value=value),
+            "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_gpu(args, world, rank, local):
+    import ctypes
+
+    from goqu_b200 import _abi, statevector
+    c, stream, gates = build_workload()
+    sim = statevector.New(N_QUBITS, _abi.GQ_C64 if args.precision == "c64" else _abi.GQ_C128)
+    sim.set_option(_abi.GQ_OPT_TIMING, 1)
+    if args.tile:
+        sim.set_option(_abi.GQ_OPT_TILE_QUBITS, args.tile)
+    if args.budget:
+        sim.set_option(_abi.GQ_OPT_PASS_BUDGET, args.budget)
+    lib = _abi.lib()
+    u = statevector.uniforms(SHOTS, np.random.default_rng(SEED))
+    u_p = u.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    idx = np.empty(SHOTS, dtype=np.uint64)
+    idx_p = idx.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+    # ---- device-resident throughput: Evolve only, CUDA events on the engine stream
+    for _ in range(args.warmup):
+        sim.evolve_ops(stream)
+    barrier(world)
+    step_ms, pass_ms, launches, passes = [], [], 0, 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            sim.evolve_ops(stream)
+            st = sim.stats()
+            step_ms.append(st["last_ms"])
+            pass_ms.append(st["pass_ms"])
+            launches += st["kernel_launches"]
+            passes += st["passes"]
+    barrier(world)
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
+    value = world * gates * args.steps / (total_ms / 1000.0)
+
+    # ---- end to end through the public C ABI: gq_sv_run from host buffers
+    for _ in range(2):
+        _abi.check(lib.gq_sv_run(sim.handle, stream.ptr(), len(stream), u_p, SHOTS, idx_p))
+    barrier(world)
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        _abi.check(lib.gq_sv_run(sim.handle, stream.ptr(), len(stream), u_p, SHOTS, idx_p))
+        st = sim.stats()
+        h2d += st["h2d_bytes"]
+        d2h += st["d2h_bytes"]
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = world * gates * args.steps / e2e_s
+
+    # ---- roofline of the dominant kernel (the tile pass)
+    peak, peak_kind = peaks()
+    amp_bytes = 8 if args.precision == "c64" else 16
+    alg_bytes = 2 * amp_bytes * (1 << N_QUBITS)  # one read + one write of the state per pass
+    per_launch_ms = float(np.sum(pass_ms)) / max(1, passes)
+    achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "tile_pass_traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            tj = json.load(f)
+        traffic = tj.get(args.precision, {}).get("bytes_per_launch")
+
+    line = {
+        "metric": "28q gates/s", "value": value, "unit": "gates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "c64" else "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "gates": gates, "seed": SEED,
+                   "precision": args.precision, "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "state 4 GiB > 126 MB L2 (no flush needed)",
+                   "passes_per_step": passes / args.steps, "pass_ms_per_step": float(np.mean(pass_ms))},
+        "e2e": {"value": e2e, "unit": "gates/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": per_launch_ms},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(stream, gates, budget_s=args.cpu_seconds)
+    sim.Close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
+    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--budget", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_gpu(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

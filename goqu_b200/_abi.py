@@ -81,6 +81,9 @@ class gq_stats(ctypes.Structure):
         ("phases", ctypes.c_int64),
         ("state_bytes", ctypes.c_int64),
         ("last_ms", ctypes.c_double),
+        ("pass_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_int64),
+        ("d2h_bytes", ctypes.c_int64),
     ]
 
 
@@ -139,6 +142,7 @@ SIGNATURES = {
     "gq_dm_fidelity": (_I, [_VP, _DBL_P, _SZ, _DBL_P]),
     "gq_dm_sample": (_I, [_VP, _DBL_P, _DBL_P, _DBL_P, _SZ, _U64P]),
     "gq_dm_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
+    "gq_dm_set_option": (_I, [_VP, _I, ctypes.c_int64]),
 }
 
 

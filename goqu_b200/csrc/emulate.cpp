@@ -92,4 +92,24 @@ int gqx_emulate_sv(int nq, int precision, double* state, const gq_op* ops, size_
     return GQ_OK;
 }
 
+// Density matrix: rho (dim*dim interleaved doubles, row-major) evolved by the
+// density-matrix op stream through dm_gates, the scheduler and the tile code.
+int gqx_emulate_dm(int nq, double* rho, const gq_op* ops, size_t n_ops, int tile_qubits, int budget) {
+    const int nvec = 2 * nq;
+    const int nphys = nvec < gq::RQ ? gq::RQ : nvec;
+    std::vector<gq::NGate> gates;
+    int rc = gq::dm_gates(nq, ops, n_ops, gates, g_err);
+    if (rc != GQ_OK) return rc;
+    gq::SchedOptions opt;
+    opt.tile_qubits = tile_qubits > 0 ? tile_qubits : 11;
+    if (budget > 0) opt.budget = budget;
+    gq::Program prog;
+    gq::schedule(gates, nphys, opt, prog);
+    std::vector<gq::cplx<double>> st(1ull << nphys, {0.0, 0.0});
+    std::memcpy(st.data(), rho, sizeof(double) * 2 * (1ull << nvec));
+    run_program<double>(st, prog);
+    std::memcpy(rho, st.data(), sizeof(double) * 2 * (1ull << nvec));
+    return GQ_OK;
+}
+
 }  // extern "C"

@@ -1,0 +1,777 @@
+// C ABI of the engine (include/gqb200.h): handles, program upload, launches.
+//
+// A handle owns its device state, a program buffer, a scratch buffer and a
+// CUDA stream; nothing is allocated per gate. Statevectors hold 2^max(n,4)
+// amplitudes (qubits above n stay |0>), density matrices are vectorised as a
+// 2n-qubit state (row index in the high n bits), so both run the same tile
+// passes. There is no CPU fallback: without an sm_100 device every call fails.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gqb200.h"
+#include "kernels.cuh"
+#include "schedule.hpp"
+
+using namespace gq;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define GQ_CUDA(x)                                                                        \
+    do {                                                                                  \
+        cudaError_t e_ = (x);                                                             \
+        if (e_ != cudaSuccess) return fail(GQ_ECUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define GQ_TRY(x)                  \
+    do {                           \
+        int rc_ = (x);             \
+        if (rc_ != GQ_OK) return rc_; \
+    } while (0)
+
+int check_device(int* dev_out) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return fail(GQ_ENODEVICE, "no CUDA device visible");
+    int dev = 0;
+    GQ_CUDA(cudaGetDevice(&dev));
+    cudaDeviceProp p;
+    GQ_CUDA(cudaGetDeviceProperties(&p, dev));
+    if (p.major != 10) return fail(GQ_ENODEVICE, std::string("device is not sm_100: ") + p.name);
+    *dev_out = dev;
+    return GQ_OK;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return GQ_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(GQ_ENOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+        }
+        cap = bytes;
+        return GQ_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return GQ_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(GQ_ENOMEM, "cudaMallocHost failed");
+        }
+        cap = bytes;
+        return GQ_OK;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+template <class T>
+int set_smem_attr() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        err = cudaFuncSetAttribute(k_tile_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(cplx<T>) << TileShape<T>::kMaxTile));
+    });
+    if (err != cudaSuccess) return fail(GQ_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
+    return GQ_OK;
+}
+
+// State of one simulator: device amplitudes plus the buffers to drive them.
+struct Engine {
+    int device = 0;
+    int prec = GQ_C128;
+    int nphys = 0;              // physical qubits of the vector
+    uint64_t n_amps = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf state, prog, scratch, scratch2, aux;
+    PinnedBuf staging, hostio;
+    cudaEvent_t staged = nullptr, ev0 = nullptr, ev1 = nullptr, ev_pass0 = nullptr, ev_pass1 = nullptr;
+    bool pass_timed = false;
+    bool staged_pending = false;
+    SchedOptions opt;
+    bool timing = false;
+    gq_stats stats{};
+
+    size_t amp_bytes() const { return prec == GQ_C64 ? 8 : 16; }
+    int max_tile() const { return prec == GQ_C64 ? TileShape<float>::kMaxTile : TileShape<double>::kMaxTile; }
+
+    int init(int nphys_, int prec_) {
+        GQ_TRY(check_device(&device));
+        prec = prec_;
+        nphys = nphys_;
+        n_amps = 1ull << nphys;
+        GQ_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        GQ_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+        GQ_CUDA(cudaEventCreate(&ev0));
+        GQ_CUDA(cudaEventCreate(&ev1));
+        GQ_CUDA(cudaEventCreate(&ev_pass0));
+        GQ_CUDA(cudaEventCreate(&ev_pass1));
+        GQ_TRY(state.ensure(n_amps * amp_bytes()));
+        opt.tile_qubits = max_tile();
+        opt.low_qubits = prec == GQ_C64 ? 4 : 3;
+        opt.swizzle_width = prec == GQ_C64 ? 4 : 3;
+        opt.budget = 96;
+        stats.state_bytes = (int64_t)(n_amps * amp_bytes());
+        GQ_TRY(prec == GQ_C64 ? set_smem_attr<float>() : set_smem_attr<double>());
+        return reset_basis(0);
+    }
+
+    void destroy() {
+        if (stream) cudaStreamSynchronize(stream);
+        state.release();
+        prog.release();
+        scratch.release();
+        scratch2.release();
+        aux.release();
+        staging.release();
+        hostio.release();
+        if (staged) cudaEventDestroy(staged);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (ev_pass0) cudaEventDestroy(ev_pass0);
+        if (ev_pass1) cudaEventDestroy(ev_pass1);
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+
+    int reset_basis(uint64_t idx) {
+        GQ_CUDA(cudaMemsetAsync(state.p, 0, n_amps * amp_bytes(), stream));
+        if (prec == GQ_C64)
+            k_set_amp<float><<<1, 1, 0, stream>>>((cplx<float>*)state.p, idx, 1.f, 0.f);
+        else
+            k_set_amp<double><<<1, 1, 0, stream>>>((cplx<double>*)state.p, idx, 1.0, 0.0);
+        GQ_CUDA(cudaGetLastError());
+        stats.kernel_launches += 1;
+        return GQ_OK;
+    }
+
+    // Host staging buffer is reused: wait for the previous upload to finish.
+    int stage(size_t bytes, void** host) {
+        if (staged_pending) {
+            GQ_CUDA(cudaEventSynchronize(staged));
+            staged_pending = false;
+        }
+        GQ_TRY(staging.ensure(bytes));
+        *host = staging.p;
+        return GQ_OK;
+    }
+    int upload(DevBuf& dst, size_t bytes) {
+        GQ_TRY(dst.ensure(bytes));
+        stats.h2d_bytes += (int64_t)bytes;
+        GQ_CUDA(cudaMemcpyAsync(dst.p, staging.p, bytes, cudaMemcpyHostToDevice, stream));
+        GQ_CUDA(cudaEventRecord(staged, stream));
+        staged_pending = true;
+        return GQ_OK;
+    }
+
+    template <class T>
+    int run_program_t(const Program& pr) {
+        if (pr.passes.empty()) return GQ_OK;
+        const size_t o_pass = 0;
+        const size_t o_phase = align16(o_pass + sizeof(PassDesc) * pr.passes.size());
+        const size_t o_ops = align16(o_phase + sizeof(PhaseDesc) * pr.phases.size());
+        const size_t o_pool = align16(o_ops + sizeof(KOp) * pr.ops.size());
+        const size_t total = align16(o_pool + sizeof(cplx<T>) * std::max<size_t>(1, pr.pool.size()));
+        void* hp = nullptr;
+        GQ_TRY(stage(total, &hp));
+        char* h = (char*)hp;
+        std::memcpy(h + o_pass, pr.passes.data(), sizeof(PassDesc) * pr.passes.size());
+        std::memcpy(h + o_phase, pr.phases.data(), sizeof(PhaseDesc) * pr.phases.size());
+        if (!pr.ops.empty()) std::memcpy(h + o_ops, pr.ops.data(), sizeof(KOp) * pr.ops.size());
+        cplx<T>* pool = (cplx<T>*)(h + o_pool);
+        for (size_t i = 0; i < pr.pool.size(); ++i) pool[i] = {(T)pr.pool[i].re, (T)pr.pool[i].im};
+        GQ_TRY(upload(prog, total));
+        char* d = (char*)prog.p;
+        if (timing) GQ_CUDA(cudaEventRecord(ev_pass0, stream));
+        for (size_t i = 0; i < pr.passes.size(); ++i) {
+            const PassDesc& pd = pr.passes[i];
+            const unsigned threads = 1u << (pd.m - RQ);
+            const size_t smem = sizeof(cplx<T>) << pd.m;
+            const unsigned grid = 1u << pd.n_outer;
+            k_tile_pass<T><<<grid, threads, smem, stream>>>((cplx<T>*)state.p, (const PassDesc*)(d + o_pass) + i,
+                                                            (const PhaseDesc*)(d + o_phase), (const KOp*)(d + o_ops),
+                                                            (const cplx<T>*)(d + o_pool));
+        }
+        GQ_CUDA(cudaGetLastError());
+        if (timing) {
+            GQ_CUDA(cudaEventRecord(ev_pass1, stream));
+            pass_timed = true;
+        }
+        stats.passes += (int64_t)pr.passes.size();
+        stats.kernel_launches += (int64_t)pr.passes.size();
+        stats.phases += (int64_t)pr.phases.size();
+        return GQ_OK;
+    }
+
+    int run_gates(const std::vector<NGate>& gates) {
+        Program pr;
+        schedule(gates, nphys, opt, pr);
+        stats.gates_in += pr.gates;
+        return prec == GQ_C64 ? run_program_t<float>(pr) : run_program_t<double>(pr);
+    }
+
+    void clear_stats() {
+        const int64_t sb = stats.state_bytes;
+        stats = gq_stats{};
+        stats.state_bytes = sb;
+    }
+
+    // Timing brackets of one apply/evolve call (GQ_OPT_TIMING): events on the
+    // handle's stream around the whole call and around its tile passes.
+    int time_begin() {
+        pass_timed = false;
+        if (timing) GQ_CUDA(cudaEventRecord(ev0, stream));
+        return GQ_OK;
+    }
+    int time_end() {
+        if (!timing) return GQ_OK;
+        GQ_CUDA(cudaEventRecord(ev1, stream));
+        GQ_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        GQ_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        stats.last_ms = ms;
+        if (pass_timed) {
+            GQ_CUDA(cudaEventElapsedTime(&ms, ev_pass0, ev_pass1));
+            stats.pass_ms = ms;
+        }
+        return GQ_OK;
+    }
+
+    // ---- reductions -----------------------------------------------------
+    int reduce_grid() const { return 148 * 4; }
+
+    int finish_reduce(int nblocks, double* re, double* im) {
+        k_final_reduce<<<1, 1024, 0, stream>>>((const double2*)scratch.p, nblocks, (double2*)scratch.p + nblocks);
+        GQ_CUDA(cudaGetLastError());
+        GQ_TRY(hostio.ensure(64));
+        GQ_CUDA(cudaMemcpyAsync(hostio.p, (double2*)scratch.p + nblocks, sizeof(double2), cudaMemcpyDeviceToHost,
+                                stream));
+        GQ_CUDA(cudaStreamSynchronize(stream));
+        double2 v = *(double2*)hostio.p;
+        if (re) *re = v.x;
+        if (im) *im = v.y;
+        stats.kernel_launches += 2;
+        return GQ_OK;
+    }
+
+    // Groups Pauli terms by x mask; uploads them; returns the group count.
+    int upload_terms(const gq_pauli_term* terms, size_t n_terms, uint64_t qmask, int* ngroups, size_t* o_terms) {
+        std::vector<size_t> order(n_terms);
+        for (size_t i = 0; i < n_terms; ++i) {
+            if ((terms[i].x_mask | terms[i].z_mask) & ~qmask) return fail(GQ_EINVAL, "Pauli term on a qubit out of range");
+            order[i] = i;
+        }
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t a, size_t b) { return terms[a].x_mask < terms[b].x_mask; });
+        std::vector<DGroup> groups;
+        std::vector<DTerm> dt;
+        for (size_t k = 0; k < n_terms; ++k) {
+            const gq_pauli_term& t = terms[order[k]];
+            if (groups.empty() || groups.back().x != t.x_mask) groups.push_back({t.x_mask, (int32_t)k, (int32_t)k});
+            groups.back().t1 = (int32_t)k + 1;
+            const int ny = __builtin_popcountll(t.x_mask & t.z_mask) & 3;  // iPow (sim/pauli/pauli.go:205-217)
+            double pr = 1, pi = 0;
+            if (ny == 1) pr = 0, pi = 1;
+            if (ny == 2) pr = -1, pi = 0;
+            if (ny == 3) pr = 0, pi = -1;
+            dt.push_back({t.coeff_re * pr - t.coeff_im * pi, t.coeff_re * pi + t.coeff_im * pr, t.z_mask});
+        }
+        const size_t og = 0, ot = align16(sizeof(DGroup) * std::max<size_t>(1, groups.size()));
+        const size_t total = ot + sizeof(DTerm) * std::max<size_t>(1, dt.size());
+        void* hp = nullptr;
+        GQ_TRY(stage(total, &hp));
+        if (!groups.empty()) std::memcpy((char*)hp + og, groups.data(), sizeof(DGroup) * groups.size());
+        if (!dt.empty()) std::memcpy((char*)hp + ot, dt.data(), sizeof(DTerm) * dt.size());
+        GQ_TRY(upload(scratch2, total));
+        *ngroups = (int)groups.size();
+        *o_terms = ot;
+        return GQ_OK;
+    }
+
+    // ---- sampling --------------------------------------------------------
+    template <class P>
+    int sample_impl(P prob, uint64_t n, const double* uniforms, size_t shots, uint64_t* idx_out) {
+        if (shots == 0) return GQ_OK;
+        const int chunk_log = n >= 2048 ? 11 : (int)std::max<uint64_t>(0, (uint64_t)std::log2((double)n));
+        const uint64_t nchunks = (n + (1ull << chunk_log) - 1) >> chunk_log;
+        // scratch: sums | incl | ends ; scratch2 (io): uniforms | out | flags
+        GQ_TRY(scratch.ensure(3 * nchunks * sizeof(double) + 64));
+        double* sums = (double*)scratch.p;
+        double* incl = sums + nchunks;
+        double* ends = incl + nchunks;
+        const size_t o_u = 0, o_out = align16(shots * 8), o_flags = o_out + align16(shots * 8);
+        const size_t io = o_flags + align16(shots * 4);
+        void* hp = nullptr;
+        GQ_TRY(stage(io, &hp));
+        std::memcpy((char*)hp + o_u, uniforms, shots * 8);
+        GQ_TRY(upload(scratch2, io));
+        char* d = (char*)scratch2.p;
+        k_chunk_sums<P><<<(unsigned)nchunks, 256, 0, stream>>>(prob, n, chunk_log, sums);
+        k_scan_chunks<<<1, 1024, 0, stream>>>(sums, nchunks, incl);
+        const unsigned warps_per_block = 8;
+        k_sample<P><<<(unsigned)((shots + warps_per_block - 1) / warps_per_block), 32 * warps_per_block, 0, stream>>>(
+            prob, n, chunk_log, incl, nchunks, (const double*)(d + o_u), shots, (uint64_t*)(d + o_out),
+            (int*)(d + o_flags));
+        GQ_CUDA(cudaGetLastError());
+        stats.kernel_launches += 3;
+        GQ_TRY(hostio.ensure(shots * 4 + 16));
+        GQ_CUDA(cudaMemcpyAsync(hostio.p, d + o_flags, shots * 4, cudaMemcpyDeviceToHost, stream));
+        GQ_CUDA(cudaStreamSynchronize(stream));
+        const int* fl = (const int*)hostio.p;
+        size_t nflag = 0;
+        for (size_t i = 0; i < shots; ++i) nflag += fl[i] != 0;
+        if (nflag) {
+            k_seq_chunk_ends<P><<<1, 1, 0, stream>>>(prob, n, chunk_log, ends);
+            k_sample_exact<P><<<(unsigned)((shots + 255) / 256), 256, 0, stream>>>(
+                prob, n, chunk_log, ends, nchunks, (const double*)(d + o_u), (const int*)(d + o_flags), shots,
+                (uint64_t*)(d + o_out));
+            GQ_CUDA(cudaGetLastError());
+            stats.kernel_launches += 2;
+        }
+        stats.d2h_bytes += (int64_t)(shots * 8 + shots * 4);
+        GQ_CUDA(cudaMemcpyAsync(idx_out, d + o_out, shots * 8, cudaMemcpyDeviceToHost, stream));
+        GQ_CUDA(cudaStreamSynchronize(stream));
+        return GQ_OK;
+    }
+};
+
+bool valid_prec(int p) { return p == GQ_C128 || p == GQ_C64; }
+
+}  // namespace
+
+// ============================================================================
+struct gq_sv {
+    Engine e;
+    int nq = 0;
+};
+
+struct gq_dm {
+    Engine e;
+    int nq = 0;
+};
+
+extern "C" {
+
+int gq_abi_version(void) { return GQ_ABI_VERSION; }
+
+const char* gq_last_error(void) { return g_err.c_str(); }
+
+int gq_device_count(int* count) {
+    if (!count) return fail(GQ_EINVAL, "null count");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    int ok = 0;
+    for (int i = 0; i < n; ++i) {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, i) == cudaSuccess && p.major == 10) ++ok;
+    }
+    *count = ok;
+    return GQ_OK;
+}
+
+// ---- statevector ------------------------------------------------------------
+int gq_sv_create(int num_qubits, int precision, gq_sv** out) {
+    if (!out) return fail(GQ_EINVAL, "null output handle");
+    *out = nullptr;
+    if (num_qubits < 1 || num_qubits > 34)
+        return fail(GQ_EINVAL, "statevector: numQubits " + std::to_string(num_qubits) + " out of range [1, 34]");
+    if (!valid_prec(precision)) return fail(GQ_EINVAL, "unknown precision");
+    gq_sv* h = new gq_sv();
+    h->nq = num_qubits;
+    int rc = h->e.init(std::max(num_qubits, RQ), precision);
+    if (rc != GQ_OK) {
+        h->e.destroy();
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return GQ_OK;
+}
+
+int gq_sv_destroy(gq_sv* sv) {
+    if (!sv) return GQ_OK;
+    sv->e.destroy();
+    delete sv;
+    return GQ_OK;
+}
+
+int gq_sv_num_qubits(const gq_sv* sv, int* out) {
+    if (!sv || !out) return fail(GQ_EINVAL, "null argument");
+    *out = sv->nq;
+    return GQ_OK;
+}
+
+int gq_sv_reset(gq_sv* sv) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    return sv->e.reset_basis(0);
+}
+
+static int sv_apply_impl(gq_sv* sv, const gq_op* ops, size_t n_ops) {
+    if (n_ops && !ops) return fail(GQ_EINVAL, "null ops");
+    std::vector<NGate> gates;
+    std::string err;
+    for (size_t i = 0; i < n_ops; ++i) {
+        if (ops[i].kind == GQ_OP_CHANNEL) return fail(GQ_EINVAL, "op " + std::to_string(i) + ": channel on a statevector");
+        int rc = normalize_op(ops[i], sv->nq, gates, err);
+        if (rc != GQ_OK) return fail(rc, "op " + std::to_string(i) + ": " + err);
+        if (!gates.empty() && gates.back().src < 0) gates.back().src = (int)i;
+    }
+    return sv->e.run_gates(gates);
+}
+
+namespace {
+int sv_apply_timed(gq_sv* sv, const gq_op* ops, size_t n_ops, bool reset) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    sv->e.clear_stats();
+    GQ_TRY(sv->e.time_begin());
+    if (reset) GQ_TRY(sv->e.reset_basis(0));
+    GQ_TRY(sv_apply_impl(sv, ops, n_ops));
+    return sv->e.time_end();
+}
+}  // namespace
+
+int gq_sv_apply(gq_sv* sv, const gq_op* ops, size_t n_ops) { return sv_apply_timed(sv, ops, n_ops, false); }
+
+int gq_sv_evolve(gq_sv* sv, const gq_op* ops, size_t n_ops) { return sv_apply_timed(sv, ops, n_ops, true); }
+
+int gq_sv_get_state(gq_sv* sv, void* host_out, size_t bytes) {
+    if (!sv || !host_out) return fail(GQ_EINVAL, "null argument");
+    const size_t need = (1ull << sv->nq) * sv->e.amp_bytes();
+    if (bytes < need) return fail(GQ_EINVAL, "output buffer too small");
+    GQ_CUDA(cudaMemcpyAsync(host_out, sv->e.state.p, need, cudaMemcpyDeviceToHost, sv->e.stream));
+    GQ_CUDA(cudaStreamSynchronize(sv->e.stream));
+    return GQ_OK;
+}
+
+int gq_sv_set_state(gq_sv* sv, const void* host_in, size_t bytes) {
+    if (!sv || !host_in) return fail(GQ_EINVAL, "null argument");
+    const size_t need = (1ull << sv->nq) * sv->e.amp_bytes();
+    if (bytes != need) return fail(GQ_EINVAL, "state size mismatch");
+    if (sv->nq < RQ) GQ_CUDA(cudaMemsetAsync(sv->e.state.p, 0, sv->e.n_amps * sv->e.amp_bytes(), sv->e.stream));
+    GQ_CUDA(cudaMemcpyAsync(sv->e.state.p, host_in, need, cudaMemcpyHostToDevice, sv->e.stream));
+    GQ_CUDA(cudaStreamSynchronize(sv->e.stream));
+    return GQ_OK;
+}
+
+int gq_sv_probabilities(gq_sv* sv, double* host_out, size_t n) {
+    if (!sv || !host_out) return fail(GQ_EINVAL, "null argument");
+    const uint64_t na = 1ull << sv->nq;
+    if (n < na) return fail(GQ_EINVAL, "output buffer too small");
+    Engine& e = sv->e;
+    GQ_TRY(e.scratch.ensure(na * 8));
+    if (e.prec == GQ_C64)
+        k_probs<float><<<e.reduce_grid(), 256, 0, e.stream>>>((const cplx<float>*)e.state.p, na, (double*)e.scratch.p);
+    else
+        k_probs<double><<<e.reduce_grid(), 256, 0, e.stream>>>((const cplx<double>*)e.state.p, na, (double*)e.scratch.p);
+    GQ_CUDA(cudaGetLastError());
+    GQ_CUDA(cudaMemcpyAsync(host_out, e.scratch.p, na * 8, cudaMemcpyDeviceToHost, e.stream));
+    GQ_CUDA(cudaStreamSynchronize(e.stream));
+    return GQ_OK;
+}
+
+int gq_sv_sample(gq_sv* sv, const double* uniforms, size_t shots, uint64_t* idx_out) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    if (shots && (!uniforms || !idx_out)) return fail(GQ_EINVAL, "null argument");
+    for (size_t i = 0; i < shots; ++i)
+        if (!(uniforms[i] >= 0.0 && uniforms[i] < 1.0)) return fail(GQ_EINVAL, "uniform outside [0, 1)");
+    const uint64_t na = 1ull << sv->nq;
+    Engine& e = sv->e;
+    if (e.prec == GQ_C64) return e.sample_impl(ProbState<float>{(const cplx<float>*)e.state.p}, na, uniforms, shots, idx_out);
+    return e.sample_impl(ProbState<double>{(const cplx<double>*)e.state.p}, na, uniforms, shots, idx_out);
+}
+
+int gq_sv_run(gq_sv* sv, const gq_op* ops, size_t n_ops, const double* uniforms, size_t shots, uint64_t* idx_out) {
+    GQ_TRY(gq_sv_evolve(sv, ops, n_ops));  // resets the counters of this call
+    return gq_sv_sample(sv, uniforms, shots, idx_out);
+}
+
+int gq_sv_expect_pauli_sum(gq_sv* sv, const gq_pauli_term* terms, size_t n_terms, double* out_re, double* out_im) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    if (n_terms && !terms) return fail(GQ_EINVAL, "null terms");
+    Engine& e = sv->e;
+    int ng = 0;
+    size_t ot = 0;
+    GQ_TRY(e.upload_terms(terms, n_terms, (sv->nq >= 64) ? ~0ull : ((1ull << sv->nq) - 1), &ng, &ot));
+    const int nb = e.reduce_grid();
+    GQ_TRY(e.scratch.ensure((nb + 1) * sizeof(double2)));
+    const char* d = (const char*)e.scratch2.p;
+    const uint64_t na = 1ull << sv->nq;
+    if (e.prec == GQ_C64)
+        k_expect<float><<<nb, 256, 0, e.stream>>>((const cplx<float>*)e.state.p, na, (const DGroup*)d, ng,
+                                                  (const DTerm*)(d + ot), (double2*)e.scratch.p);
+    else
+        k_expect<double><<<nb, 256, 0, e.stream>>>((const cplx<double>*)e.state.p, na, (const DGroup*)d, ng,
+                                                   (const DTerm*)(d + ot), (double2*)e.scratch.p);
+    GQ_CUDA(cudaGetLastError());
+    return e.finish_reduce(nb, out_re, out_im);
+}
+
+int gq_sv_expect_z_mask(gq_sv* sv, uint64_t mask, double* out) {
+    gq_pauli_term t{1.0, 0.0, 0, mask};
+    return gq_sv_expect_pauli_sum(sv, &t, 1, out, nullptr);
+}
+
+int gq_sv_stats(const gq_sv* sv, gq_stats* out) {
+    if (!sv || !out) return fail(GQ_EINVAL, "null argument");
+    *out = sv->e.stats;
+    return GQ_OK;
+}
+
+int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    Engine& e = sv->e;
+    switch (key) {
+        case GQ_OPT_TILE_QUBITS:
+            if (value < RQ || value > e.max_tile())
+                return fail(GQ_EINVAL, "tile qubits out of range [4, " + std::to_string(e.max_tile()) + "]");
+            e.opt.tile_qubits = (int)value;
+            return GQ_OK;
+        case GQ_OPT_PASS_BUDGET:
+            if (value < 0) return fail(GQ_EINVAL, "negative budget");
+            e.opt.budget = value == 0 ? 96 : (int)value;
+            return GQ_OK;
+        case GQ_OPT_LOW_QUBITS:
+            if (value < 0 || value > 6) return fail(GQ_EINVAL, "low qubits out of range [0, 6]");
+            e.opt.low_qubits = (int)value;
+            return GQ_OK;
+        case GQ_OPT_TIMING:
+            e.timing = value != 0;
+            return GQ_OK;
+        default:
+            return fail(GQ_EINVAL, "unknown option");
+    }
+}
+
+int gq_sv_adjoint_gradient(gq_sv*, const gq_op*, size_t, const gq_pauli_term*, size_t, size_t, double*, double*) {
+    return fail(GQ_EUNSUPPORTED, "adjoint gradient not built yet");
+}
+
+// ---- density matrix -----------------------------------------------------------
+
+int gq_dm_create(int num_qubits, gq_dm** out) {
+    if (!out) return fail(GQ_EINVAL, "null output handle");
+    *out = nullptr;
+    if (num_qubits < 1 || num_qubits > 15)
+        return fail(GQ_EINVAL, "densitymatrix: numQubits " + std::to_string(num_qubits) + " out of range [1, 15]");
+    gq_dm* h = new gq_dm();
+    h->nq = num_qubits;
+    int rc = h->e.init(std::max(2 * num_qubits, RQ), GQ_C128);
+    if (rc != GQ_OK) {
+        h->e.destroy();
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return GQ_OK;
+}
+
+int gq_dm_destroy(gq_dm* dm) {
+    if (!dm) return GQ_OK;
+    dm->e.destroy();
+    delete dm;
+    return GQ_OK;
+}
+
+int gq_dm_reset(gq_dm* dm) {
+    if (!dm) return fail(GQ_EINVAL, "null handle");
+    return dm->e.reset_basis(0);
+}
+
+static int dm_apply_impl(gq_dm* dm, const gq_op* ops, size_t n_ops) {
+    if (n_ops && !ops) return fail(GQ_EINVAL, "null ops");
+    std::vector<NGate> gates;
+    {
+        std::string err;
+        int rc = dm_gates(dm->nq, ops, n_ops, gates, err);
+        if (rc != GQ_OK) return fail(rc, err);
+    }
+    return dm->e.run_gates(gates);
+}
+
+static int dm_apply_timed(gq_dm* dm, const gq_op* ops, size_t n_ops, bool reset) {
+    if (!dm) return fail(GQ_EINVAL, "null handle");
+    dm->e.clear_stats();
+    GQ_TRY(dm->e.time_begin());
+    if (reset) GQ_TRY(dm->e.reset_basis(0));
+    GQ_TRY(dm_apply_impl(dm, ops, n_ops));
+    return dm->e.time_end();
+}
+
+int gq_dm_apply(gq_dm* dm, const gq_op* ops, size_t n_ops) { return dm_apply_timed(dm, ops, n_ops, false); }
+
+int gq_dm_evolve(gq_dm* dm, const gq_op* ops, size_t n_ops) { return dm_apply_timed(dm, ops, n_ops, true); }
+
+int gq_dm_set_option(gq_dm* dm, int key, int64_t value) {
+    if (!dm) return fail(GQ_EINVAL, "null handle");
+    if (key == GQ_OPT_TIMING) {
+        dm->e.timing = value != 0;
+        return GQ_OK;
+    }
+    if (key == GQ_OPT_PASS_BUDGET) {
+        if (value < 0) return fail(GQ_EINVAL, "negative budget");
+        dm->e.opt.budget = value == 0 ? 96 : (int)value;
+        return GQ_OK;
+    }
+    if (key == GQ_OPT_TILE_QUBITS) {
+        if (value < RQ || value > dm->e.max_tile()) return fail(GQ_EINVAL, "tile qubits out of range");
+        dm->e.opt.tile_qubits = (int)value;
+        return GQ_OK;
+    }
+    return fail(GQ_EINVAL, "unknown option");
+}
+
+int gq_dm_get(gq_dm* dm, double* host_out, size_t bytes) {
+    if (!dm || !host_out) return fail(GQ_EINVAL, "null argument");
+    const size_t need = (1ull << (2 * dm->nq)) * 16;
+    if (bytes < need) return fail(GQ_EINVAL, "output buffer too small");
+    GQ_CUDA(cudaMemcpyAsync(host_out, dm->e.state.p, need, cudaMemcpyDeviceToHost, dm->e.stream));
+    GQ_CUDA(cudaStreamSynchronize(dm->e.stream));
+    return GQ_OK;
+}
+
+int gq_dm_set(gq_dm* dm, const double* host_in, size_t bytes) {
+    if (!dm || !host_in) return fail(GQ_EINVAL, "null argument");
+    const size_t need = (1ull << (2 * dm->nq)) * 16;
+    if (bytes != need) return fail(GQ_EINVAL, "size mismatch");
+    if (2 * dm->nq < RQ) GQ_CUDA(cudaMemsetAsync(dm->e.state.p, 0, dm->e.n_amps * 16, dm->e.stream));
+    GQ_CUDA(cudaMemcpyAsync(dm->e.state.p, host_in, need, cudaMemcpyHostToDevice, dm->e.stream));
+    GQ_CUDA(cudaStreamSynchronize(dm->e.stream));
+    return GQ_OK;
+}
+
+int gq_dm_diagonal_probs(gq_dm* dm, double* host_out, size_t n) {
+    if (!dm || !host_out) return fail(GQ_EINVAL, "null argument");
+    const uint64_t dim = 1ull << dm->nq;
+    if (n < dim) return fail(GQ_EINVAL, "output buffer too small");
+    Engine& e = dm->e;
+    GQ_TRY(e.scratch.ensure(dim * 8));
+    k_dm_diag_probs<<<e.reduce_grid(), 256, 0, e.stream>>>((const cplx<double>*)e.state.p, dim, (double*)e.scratch.p);
+    GQ_CUDA(cudaGetLastError());
+    GQ_CUDA(cudaMemcpyAsync(host_out, e.scratch.p, dim * 8, cudaMemcpyDeviceToHost, e.stream));
+    GQ_CUDA(cudaStreamSynchronize(e.stream));
+    return GQ_OK;
+}
+
+int gq_dm_expect_pauli_sum(gq_dm* dm, const gq_pauli_term* terms, size_t n_terms, double* out_re, double* out_im) {
+    if (!dm) return fail(GQ_EINVAL, "null handle");
+    if (n_terms && !terms) return fail(GQ_EINVAL, "null terms");
+    Engine& e = dm->e;
+    int ng = 0;
+    size_t ot = 0;
+    GQ_TRY(e.upload_terms(terms, n_terms, (1ull << dm->nq) - 1, &ng, &ot));
+    const int nb = e.reduce_grid();
+    GQ_TRY(e.scratch.ensure((nb + 1) * sizeof(double2)));
+    const char* d = (const char*)e.scratch2.p;
+    k_dm_expect<<<nb, 256, 0, e.stream>>>((const cplx<double>*)e.state.p, 1ull << dm->nq, (const DGroup*)d, ng,
+                                          (const DTerm*)(d + ot), (double2*)e.scratch.p);
+    GQ_CUDA(cudaGetLastError());
+    return e.finish_reduce(nb, out_re, out_im);
+}
+
+int gq_dm_trace(gq_dm* dm, double* out_re, double* out_im) {
+    gq_pauli_term t{1.0, 0.0, 0, 0};
+    return gq_dm_expect_pauli_sum(dm, &t, 1, out_re, out_im);
+}
+
+int gq_dm_purity(gq_dm* dm, double* out) {
+    if (!dm || !out) return fail(GQ_EINVAL, "null argument");
+    Engine& e = dm->e;
+    const int nb = e.reduce_grid();
+    GQ_TRY(e.scratch.ensure((nb + 1) * sizeof(double2)));
+    k_dm_purity<<<nb, 256, 0, e.stream>>>((const cplx<double>*)e.state.p, 1ull << dm->nq, (double2*)e.scratch.p);
+    GQ_CUDA(cudaGetLastError());
+    double re = 0;
+    GQ_TRY(e.finish_reduce(nb, &re, nullptr));
+    *out = std::fabs(re);
+    return GQ_OK;
+}
+
+int gq_dm_fidelity(gq_dm* dm, const double* psi, size_t n, double* out) {
+    if (!dm || !psi || !out) return fail(GQ_EINVAL, "null argument");
+    const uint64_t dim = 1ull << dm->nq;
+    if (n != dim) return fail(GQ_EINVAL, "densitymatrix: pure state length mismatch");
+    Engine& e = dm->e;
+    void* hp = nullptr;
+    GQ_TRY(e.stage(dim * 16, &hp));
+    std::memcpy(hp, psi, dim * 16);
+    GQ_TRY(e.upload(e.scratch2, dim * 16));
+    const int nb = e.reduce_grid();
+    GQ_TRY(e.scratch.ensure((nb + 1) * sizeof(double2)));
+    k_dm_fidelity<<<nb, 256, 0, e.stream>>>((const cplx<double>*)e.state.p, dim, (const cplx<double>*)e.scratch2.p,
+                                            (double2*)e.scratch.p);
+    GQ_CUDA(cudaGetLastError());
+    double re = 0;
+    GQ_TRY(e.finish_reduce(nb, &re, nullptr));
+    *out = std::fabs(re);
+    return GQ_OK;
+}
+
+int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* uniforms, size_t shots,
+                 uint64_t* idx_out) {
+    if (!dm) return fail(GQ_EINVAL, "null handle");
+    if (shots && (!uniforms || !idx_out)) return fail(GQ_EINVAL, "null argument");
+    for (size_t i = 0; i < shots; ++i)
+        if (!(uniforms[i] >= 0.0 && uniforms[i] < 1.0)) return fail(GQ_EINVAL, "uniform outside [0, 1)");
+    Engine& e = dm->e;
+    const uint64_t dim = 1ull << dm->nq;
+    // probs live in `aux`; the sampler uses scratch / scratch2.
+    GQ_TRY(e.aux.ensure(2 * dim * 8));
+    double* a = (double*)e.aux.p;
+    double* b = a + dim;
+    k_dm_diag_probs<<<e.reduce_grid(), 256, 0, e.stream>>>((const cplx<double>*)e.state.p, dim, a);
+    if (p01 && p10)
+        for (int q = 0; q < dm->nq; ++q) {
+            if (p01[q] < 0) continue;
+            k_readout_qubit<<<e.reduce_grid(), 256, 0, e.stream>>>(a, b, dim, 1ull << q, p01[q], p10[q]);
+            std::swap(a, b);
+        }
+    GQ_CUDA(cudaGetLastError());
+    return e.sample_impl(ProbArray{a}, dim, uniforms, shots, idx_out);
+}
+
+int gq_dm_stats(const gq_dm* dm, gq_stats* out) {
+    if (!dm || !out) return fail(GQ_EINVAL, "null argument");
+    *out = dm->e.stats;
+    return GQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,496 @@
+// sm_100a kernels of the engine: the tile pass, probability / sampling
+// kernels and FP64 reductions (expectations, density-matrix traces).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tile_core.cuh"
+
+namespace gq {
+
+// ---------------------------------------------------------------------------
+// Tile pass: one CTA per tile, 2^(m-4) threads, 2^m amplitudes of shared memory.
+// The CTA stages its tile (16 coalesced loads per thread), runs the pass's
+// phases with a barrier between them, and writes the tile back in place.
+// Launch shape per precision: complex128 tiles of up to 2^11 amplitudes with
+// 128 threads (up to 168 registers, three CTAs per SM); complex64 tiles of up
+// to 2^12 amplitudes with 256 threads (two CTAs per SM).
+template <class T>
+struct TileShape;
+template <>
+struct TileShape<double> {
+    static constexpr int kMaxTile = 11, kThreads = 128, kMinBlocks = 3;
+};
+template <>
+struct TileShape<float> {
+    static constexpr int kMaxTile = 12, kThreads = 256, kMinBlocks = 2;
+};
+
+template <class T>
+__global__ void __launch_bounds__(TileShape<T>::kThreads, TileShape<T>::kMinBlocks)
+    k_tile_pass(cplx<T>* __restrict__ st, const PassDesc* __restrict__ pdp,
+                                                   const PhaseDesc* __restrict__ phases,
+                                                   const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    const PassDesc& pd = *pdp;
+    const int m = pd.m;
+    const int tbits = m - RQ;
+    const uint32_t t = threadIdx.x;
+    const uint64_t base = cta_base(pd, blockIdx.x);
+
+    // Linear staging index lin = it * 2^tbits + t: thread bits are tile bits
+    // [0, tbits), `it` supplies tile bits [tbits, m).
+    uint64_t gt = 0;
+    uint32_t stt = 0;
+    for (int b = 0; b < tbits; ++b)
+        if ((t >> b) & 1u) {
+            gt |= 1ull << pd.tile_q[b];
+            stt ^= pd.acol[b];
+        }
+    uint64_t gq[RQ];
+    uint32_t sq[RQ];
+#pragma unroll
+    for (int k = 0; k < RQ; ++k) {
+        gq[k] = 1ull << pd.tile_q[tbits + k];
+        sq[k] = pd.acol[tbits + k];
+    }
+    {
+        cplx<T> v[NREG];
+#pragma unroll
+        for (int it = 0; it < NREG; ++it) {
+            uint64_t g = base | gt;
+#pragma unroll
+            for (int k = 0; k < RQ; ++k)
+                if ((it >> k) & 1) g |= gq[k];
+            v[it] = st[g];
+        }
+#pragma unroll
+        for (int it = 0; it < NREG; ++it) {
+            uint32_t s = stt;
+#pragma unroll
+            for (int k = 0; k < RQ; ++k)
+                if ((it >> k) & 1) s ^= sq[k];
+            sm[s] = v[it];
+        }
+    }
+    __syncthreads();
+    const int nph = pd.n_phases;
+    for (int p = 0; p < nph; ++p) {
+        run_phase<T>(sm, phases[pd.phase0 + p], ops, pool, t, tbits, base);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int k = 0; k < RQ; ++k) {
+        gq[k] = 1ull << pd.tile_q[tbits + k];
+        sq[k] = pd.acol[tbits + k];
+    }
+    {
+        cplx<T> v[NREG];
+#pragma unroll
+        for (int it = 0; it < NREG; ++it) {
+            uint32_t s = stt;
+#pragma unroll
+            for (int k = 0; k < RQ; ++k)
+                if ((it >> k) & 1) s ^= sq[k];
+            v[it] = sm[s];
+        }
+#pragma unroll
+        for (int it = 0; it < NREG; ++it) {
+            uint64_t g = base | gt;
+#pragma unroll
+            for (int k = 0; k < RQ; ++k)
+                if ((it >> k) & 1) g |= gq[k];
+            st[g] = v[it];
+        }
+    }
+}
+
+template <class T>
+__global__ void k_set_amp(cplx<T>* st, uint64_t idx, T re, T im) {
+    st[idx] = {re, im};
+}
+
+// ---------------------------------------------------------------------------
+// Probabilities. p = re*re + im*im with each product and the sum rounded
+// separately (no FMA contraction), the arithmetic of goqu's probabilities()
+// (sim/statevector/sim.go:274-280) compiled by Go on amd64.
+__device__ __forceinline__ double prob_of(cplx<double> a) {
+    return __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
+}
+__device__ __forceinline__ double prob_of(cplx<float> a) {
+    const double x = a.x, y = a.y;
+    return __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+}
+
+template <class T>
+struct ProbState {
+    const cplx<T>* st;
+    __device__ __forceinline__ double operator()(uint64_t i) const { return prob_of(st[i]); }
+};
+struct ProbArray {
+    const double* p;
+    __device__ __forceinline__ double operator()(uint64_t i) const { return p[i]; }
+};
+
+template <class T>
+__global__ void k_probs(const cplx<T>* __restrict__ st, uint64_t n, double* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = prob_of(st[i]);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Per-chunk probability sums (chunk = 2^chunk_log entries, one CTA each).
+template <class P>
+__global__ void k_chunk_sums(P prob, uint64_t n, int chunk_log, double* __restrict__ sums) {
+    const uint64_t c0 = (uint64_t)blockIdx.x << chunk_log;
+    const uint64_t len = (uint64_t)1 << chunk_log;
+    double s = 0.0;
+    for (uint64_t j = threadIdx.x; j < len; j += blockDim.x)
+        if (c0 + j < n) s += prob(c0 + j);
+    s = warp_sum(s);
+    __shared__ double ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) sums[blockIdx.x] = v;
+    }
+}
+
+// Inclusive prefix of the chunk sums (single CTA of 1024 threads).
+__global__ void k_scan_chunks(const double* __restrict__ sums, uint64_t nchunks, double* __restrict__ incl) {
+    __shared__ double part[1024];
+    const uint64_t per = (nchunks + blockDim.x - 1) / blockDim.x;
+    const uint64_t b = threadIdx.x * per, e = b + per < nchunks ? b + per : nchunks;
+    double s = 0.0;
+    for (uint64_t c = b; c < e; ++c) s += sums[c];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {  // 1024 sequential adds, negligible
+        double acc = 0.0;
+        for (unsigned i = 0; i < blockDim.x; ++i) {
+            const double v = part[i];
+            part[i] = acc;
+            acc += v;
+        }
+    }
+    __syncthreads();
+    double acc = part[threadIdx.x];
+    for (uint64_t c = b; c < e; ++c) {
+        acc += sums[c];
+        incl[c] = acc;
+    }
+}
+
+// Inverse-CDF search, one warp per shot. The FP64 prefix S_j computed here
+// differs from goqu's sequential running sum s_j (sampleIndex,
+// sim/statevector/sim.go:288-298) by at most bound(j) = (j + 1 + 4096) *
+// 2^-52 * S_j: every step of the sequential sum rounds by at most 2^-53 s_j
+// and this kernel's summation tree is at most a few thousand additions deep.
+// A shot whose uniform lies within that bound of S_{idx-1} or S_idx is
+// flagged and resolved exactly by k_sample_exact.
+__device__ __forceinline__ double seq_bound(uint64_t j, double s) {
+    return ((double)j + 4097.0) * 2.220446049250313e-16 * (s + 1e-300);
+}
+
+template <class P>
+__global__ void k_sample(P prob, uint64_t n, int chunk_log, const double* __restrict__ incl, uint64_t nchunks,
+                         const double* __restrict__ uniforms, uint64_t shots, uint64_t* __restrict__ out,
+                         int* __restrict__ flags) {
+    const uint64_t shot = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (shot >= shots) return;
+    const double r = uniforms[shot];
+    // First chunk with r < incl[c] (binary search).
+    uint64_t lo = 0, hi = nchunks;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (r < incl[mid])
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    int flag = 0;
+    uint64_t idx = n - 1;
+    if (lo == nchunks) {
+        // r beyond the total: goqu falls back to the last index.
+        const double tot = nchunks ? incl[nchunks - 1] : 0.0;
+        if (r - tot < seq_bound(n - 1, tot)) flag = 1;
+    } else {
+        const uint64_t c = lo;
+        const uint64_t c0 = c << chunk_log;
+        const uint64_t len = ((uint64_t)1 << chunk_log) < n - c0 ? ((uint64_t)1 << chunk_log) : n - c0;
+        const uint64_t seg = (len + 31) / 32;
+        const uint64_t b = c0 + lane * seg;
+        const uint64_t e = (b + seg < c0 + len) ? b + seg : c0 + len;
+        double s = 0.0;
+        for (uint64_t j = b; j < e; ++j) s += prob(j);
+        // exclusive scan over lanes
+        double x = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        const double excl_c = c ? incl[c - 1] : 0.0;
+        double run = excl_c + (x - s);
+        double prev = run;
+        uint64_t hit = ~0ull;
+        double s_hit = 0.0, s_prev = 0.0;
+        for (uint64_t j = b; j < e; ++j) {
+            prev = run;
+            run += prob(j);
+            if (r < run) {
+                hit = j;
+                s_hit = run;
+                s_prev = prev;
+                break;
+            }
+        }
+        const unsigned found = __ballot_sync(0xffffffffu, hit != ~0ull);
+        if (found == 0) {
+            flag = 1;  // the chunk-level and lane-level sums disagreed
+        } else {
+            const int src = __ffs(found) - 1;
+            idx = __shfl_sync(0xffffffffu, hit, src);
+            const double sh = __shfl_sync(0xffffffffu, s_hit, src);
+            const double sp = __shfl_sync(0xffffffffu, s_prev, src);
+            if (sh - r <= seq_bound(idx, sh)) flag = 1;
+            if (idx > 0 && r - sp < seq_bound(idx - 1, sp + (sh - sp))) flag = 1;
+        }
+    }
+    if (lane == 0) {
+        out[shot] = idx;
+        flags[shot] = flag;
+    }
+}
+
+// Exact sequential running sums at every chunk end, in goqu's order (one
+// thread; used only when a shot was flagged).
+template <class P>
+__global__ void k_seq_chunk_ends(P prob, uint64_t n, int chunk_log, double* __restrict__ ends) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double cum = 0.0;
+    const uint64_t len = (uint64_t)1 << chunk_log;
+    for (uint64_t j = 0; j < n; ++j) {
+        cum = __dadd_rn(cum, prob(j));
+        if ((j & (len - 1)) == len - 1 || j == n - 1) ends[j >> chunk_log] = cum;
+    }
+}
+
+// Exact resolution of flagged shots from the exact chunk-end sums.
+template <class P>
+__global__ void k_sample_exact(P prob, uint64_t n, int chunk_log, const double* __restrict__ ends,
+                               uint64_t nchunks, const double* __restrict__ uniforms, const int* __restrict__ flags,
+                               uint64_t shots, uint64_t* __restrict__ out) {
+    const uint64_t shot = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (shot >= shots || !flags[shot]) return;
+    const double r = uniforms[shot];
+    uint64_t lo = 0, hi = nchunks;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (r < ends[mid])
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    uint64_t idx = n - 1;
+    if (lo < nchunks) {
+        double cum = lo ? ends[lo - 1] : 0.0;
+        const uint64_t c0 = lo << chunk_log;
+        const uint64_t e = (c0 + ((uint64_t)1 << chunk_log)) < n ? c0 + ((uint64_t)1 << chunk_log) : n;
+        for (uint64_t j = c0; j < e; ++j) {
+            cum = __dadd_rn(cum, prob(j));
+            if (r < cum) {
+                idx = j;
+                break;
+            }
+        }
+    }
+    out[shot] = idx;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 reductions.
+struct DTerm {
+    double wre, wim;  // coeff * i^(number of Y)
+    uint64_t z;
+};
+struct DGroup {
+    uint64_t x;
+    int32_t t0, t1;
+};
+
+__device__ __forceinline__ void block_reduce_store(double re, double im, double2* __restrict__ partial) {
+    re = warp_sum(re);
+    im = warp_sum(im);
+    __shared__ double sre[32], sim[32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sre[w] = re;
+        sim[w] = im;
+    }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        re = l < nw ? sre[l] : 0.0;
+        im = l < nw ? sim[l] : 0.0;
+        re = warp_sum(re);
+        im = warp_sum(im);
+        if (l == 0) partial[blockIdx.x] = make_double2(re, im);
+    }
+}
+
+// sum_t coeff_t <psi|P_t|psi>: for each amplitude i and each group of terms
+// sharing an x mask, conj(psi[i^x]) psi[i] times sum_t w_t (-1)^popcount(i&z_t)
+// (the formula of pauli.Expect, sim/pauli/expect_sv.go:21-47).
+template <class T>
+__global__ void k_expect(const cplx<T>* __restrict__ st, uint64_t n, const DGroup* __restrict__ groups, int ngroups,
+                         const DTerm* __restrict__ terms, double2* __restrict__ partial) {
+    double are = 0.0, aim = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const cplx<T> ai = st[i];
+        const double xr = (double)ai.x, xi = (double)ai.y;
+        for (int g = 0; g < ngroups; ++g) {
+            const DGroup gr = groups[g];
+            const cplx<T> aj = st[i ^ gr.x];
+            const double yr = (double)aj.x, yi = (double)aj.y;
+            // conj(a_j) * a_i
+            const double pr = yr * xr + yi * xi, pi = yr * xi - yi * xr;
+            double fr = 0.0, fi = 0.0;
+            for (int k = gr.t0; k < gr.t1; ++k) {
+                const DTerm tm = terms[k];
+                const double sg = (__popcll(i & tm.z) & 1) ? -1.0 : 1.0;
+                fr += sg * tm.wre;
+                fi += sg * tm.wim;
+            }
+            are += fr * pr - fi * pi;
+            aim += fr * pi + fi * pr;
+        }
+    }
+    block_reduce_store(are, aim, partial);
+}
+
+// Tr(rho P) for a row-major rho of dimension dim = 2^nq: sum_i rho[i, i^x]
+// times the same term factors (pauli.ExpectDM, sim/pauli/expect_dm.go:9-21).
+__global__ void k_dm_expect(const cplx<double>* __restrict__ rho, uint64_t dim, const DGroup* __restrict__ groups,
+                            int ngroups, const DTerm* __restrict__ terms, double2* __restrict__ partial) {
+    double are = 0.0, aim = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+        for (int g = 0; g < ngroups; ++g) {
+            const DGroup gr = groups[g];
+            const cplx<double> v = rho[i * dim + (i ^ gr.x)];
+            double fr = 0.0, fi = 0.0;
+            for (int k = gr.t0; k < gr.t1; ++k) {
+                const DTerm tm = terms[k];
+                const double sg = (__popcll(i & tm.z) & 1) ? -1.0 : 1.0;
+                fr += sg * tm.wre;
+                fi += sg * tm.wim;
+            }
+            are += fr * v.x - fi * v.y;
+            aim += fr * v.y + fi * v.x;
+        }
+    }
+    block_reduce_store(are, aim, partial);
+}
+
+// sum_{i,j} rho_ij conj(rho_ji): the sum goqu's Purity takes
+// (sim/densitymatrix/sim.go:265-276). 32x32 tiles through shared memory.
+__global__ void k_dm_purity(const cplx<double>* __restrict__ rho, uint64_t dim, double2* __restrict__ partial) {
+    __shared__ cplx<double> tile[32][33];
+    const uint64_t ntile = dim >= 32 ? dim / 32 : 1;
+    const uint64_t tdim = dim >= 32 ? 32 : dim;
+    double are = 0.0, aim = 0.0;
+    for (uint64_t tb = blockIdx.x; tb < ntile * ntile; tb += gridDim.x) {
+        const uint64_t bi = tb / ntile, bj = tb % ntile;
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+        __syncthreads();
+        for (int yy = ty; yy < 32; yy += 8)
+            if ((uint64_t)yy < tdim && (uint64_t)tx < tdim)
+                tile[yy][tx] = rho[(bj * 32 + yy) * dim + bi * 32 + tx];  // block (j, i)
+        __syncthreads();
+        for (int yy = ty; yy < 32; yy += 8) {
+            if ((uint64_t)yy >= tdim || (uint64_t)tx >= tdim) continue;
+            const cplx<double> a = rho[(bi * 32 + yy) * dim + bj * 32 + tx];  // rho_ij
+            const cplx<double> b = tile[tx][yy];                              // rho_ji
+            are += a.x * b.x + a.y * b.y;  // a * conj(b)
+            aim += a.y * b.x - a.x * b.y;
+        }
+    }
+    block_reduce_store(are, aim, partial);
+}
+
+// sum_i conj(psi_i) sum_j rho_ij psi_j (Fidelity, sim/densitymatrix/sim.go:280-291).
+__global__ void k_dm_fidelity(const cplx<double>* __restrict__ rho, uint64_t dim, const cplx<double>* __restrict__ psi,
+                              double2* __restrict__ partial) {
+    double are = 0.0, aim = 0.0;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    const int lane = threadIdx.x & 31;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < dim; i += warps) {
+        double rr = 0.0, ri = 0.0;
+        for (uint64_t j = lane; j < dim; j += 32) {
+            const cplx<double> a = rho[i * dim + j], p = psi[j];
+            rr += a.x * p.x - a.y * p.y;
+            ri += a.x * p.y + a.y * p.x;
+        }
+        const cplx<double> q = psi[i];
+        // conj(q) * (rr + i ri), accumulated by every lane's partial row sum
+        are += q.x * rr + q.y * ri;
+        aim += q.x * ri - q.y * rr;
+    }
+    block_reduce_store(are, aim, partial);
+}
+
+__global__ void k_dm_diag_probs(const cplx<double>* __restrict__ rho, uint64_t dim, double* __restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double v = rho[i * dim + i].x;
+        out[i] = v < 0 ? 0.0 : v;
+    }
+}
+
+// One qubit of ApplyReadoutError (sim/densitymatrix/measure.go:29-71):
+// out[k] = in[k]*(1-P) + in[k^m]*P' with the reference's rounding.
+__global__ void k_readout_qubit(const double* __restrict__ in, double* __restrict__ out, uint64_t dim, uint64_t mask,
+                                double p01, double p10) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < dim; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t f = k ^ mask;
+        // contribution of i = k (stays) and of i = f (flips into k)
+        const double a = (k & mask) ? __dmul_rn(in[k], __dsub_rn(1.0, p10)) : __dmul_rn(in[k], __dsub_rn(1.0, p01));
+        const double b = (f & mask) ? __dmul_rn(in[f], p10) : __dmul_rn(in[f], p01);
+        out[k] = __dadd_rn(a, b);
+    }
+}
+
+__global__ void k_final_reduce(const double2* __restrict__ partial, int n, double2* __restrict__ out) {
+    double re = 0.0, im = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        re += partial[i].x;
+        im += partial[i].y;
+    }
+    re = warp_sum(re);
+    im = warp_sum(im);
+    __shared__ double sre[32], sim[32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sre[w] = re;
+        sim[w] = im;
+    }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        re = l < nw ? sre[l] : 0.0;
+        im = l < nw ? sim[l] : 0.0;
+        re = warp_sum(re);
+        im = warp_sum(im);
+        if (l == 0) *out = make_double2(re, im);
+    }
+}
+
+}  // namespace gq

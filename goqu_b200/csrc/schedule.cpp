@@ -511,4 +511,127 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
     }
 }
 
+// ---- density matrix ----------------------------------------------------
+namespace {
+
+
+// Superoperator sum_k E_k (x) conj(E_k) of a Kraus set on k qubits, as a
+// matrix on the 2k vectorised qubits (row qubits first, then column qubits).
+std::vector<Z> superop(const Z* kraus, int nk, int k) {
+    const int d = 1 << k, D = d * d;
+    std::vector<Z> s(D * D, Z{0, 0});
+    for (int e = 0; e < nk; ++e) {
+        const Z* E = kraus + e * d * d;
+        for (int r = 0; r < d; ++r)
+            for (int c = 0; c < d; ++c)
+                for (int r2 = 0; r2 < d; ++r2)
+                    for (int c2 = 0; c2 < d; ++c2) {
+                        const Z a = E[r * d + r2], b = E[c * d + c2];  // E[r,r'] * conj(E[c,c'])
+                        Z& o = s[(r * d + c) * D + (r2 * d + c2)];
+                        o.re += a.re * b.re + a.im * b.im;
+                        o.im += a.im * b.re - a.re * b.im;
+                    }
+    }
+    return s;
+}
+
+std::vector<Z> matmul(const std::vector<Z>& a, const std::vector<Z>& b, int D) {
+    std::vector<Z> c(D * D, Z{0, 0});
+    for (int i = 0; i < D; ++i)
+        for (int k = 0; k < D; ++k) {
+            const Z x = a[i * D + k];
+            if (x.re == 0 && x.im == 0) continue;
+            for (int j = 0; j < D; ++j) {
+                const Z y = b[k * D + j];
+                c[i * D + j].re += x.re * y.re - x.im * y.im;
+                c[i * D + j].im += x.re * y.im + x.im * y.re;
+            }
+        }
+    return c;
+}
+
+// U (x) conj(U) on (row qubits, column qubits), local index row bits high.
+std::vector<Z> unitary_superop(const std::vector<Z>& u, int k) {
+    return superop(u.data(), 1, k);
+}
+
+std::vector<Z> full_controlled(const gq_op& op) {
+    const int tot = op.num_qubits, nt = op.num_qubits - op.num_controls;
+    const int dim = 1 << tot, inner = 1 << nt, start = dim - inner;
+    std::vector<Z> f(dim * dim, Z{0, 0});
+    for (int i = 0; i < start; ++i) f[i * dim + i] = Z{1, 0};
+    const Z* m = (const Z*)op.matrix;
+    for (int r = 0; r < inner; ++r)
+        for (int c = 0; c < inner; ++c) f[(start + r) * dim + start + c] = m[r * inner + c];
+    return f;
+}
+
+}  // namespace
+
+int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, std::string& err) {
+    auto vec_qubits = [&](const gq_op& op) {
+        std::vector<int> q;
+        for (int i = 0; i < op.num_qubits; ++i) q.push_back(op.qubits[i] + nq);  // row qubits
+        for (int i = 0; i < op.num_qubits; ++i) q.push_back(op.qubits[i]);       // column qubits
+        return q;
+    };
+    for (size_t i = 0; i < n_ops; ++i) {
+        const gq_op& op = ops[i];
+        if (op.kind == GQ_OP_BARRIER) continue;
+        if (op.num_qubits < 1 || op.num_qubits > 8) { err = "op " + std::to_string(i) + ": bad qubit count"; return GQ_EINVAL; }
+        for (int j = 0; j < op.num_qubits; ++j)
+            if (op.qubits[j] < 0 || op.qubits[j] >= nq) { err = "op " + std::to_string(i) + ": qubit out of range"; return GQ_EINVAL; }
+        const int k = op.num_qubits;
+        const int d = 1 << k;
+        if (op.kind == GQ_OP_RESET) {
+            // sim/densitymatrix/sim.go:195-217: rho[r,c] += rho[r|m, c|m] on the
+            // (0,0) block, everything with the bit set cleared.
+            std::vector<Z> s(16, Z{0, 0});
+            s[0 * 4 + 0] = Z{1, 0};
+            s[0 * 4 + 3] = Z{1, 0};
+            int rc = analyze_matrix(s, {op.qubits[0] + nq, op.qubits[0]}, 0, (int)i, gates, err);
+            if (rc != GQ_OK) return rc;
+            continue;
+        }
+        if (!op.matrix) { err = "op " + std::to_string(i) + ": no matrix"; return GQ_EINVAL; }
+        std::vector<Z> sop;
+        if (op.kind == GQ_OP_CHANNEL) {
+            if (op.num_kraus < 1) { err = "channel without Kraus operators"; return GQ_EINVAL; }
+            sop = superop((const Z*)op.matrix, op.num_kraus, k);
+        } else {
+            std::vector<Z> u;
+            if (op.kind == GQ_OP_CONTROLLED)
+                u = full_controlled(op);
+            else
+                u.assign((const Z*)op.matrix, (const Z*)op.matrix + d * d);
+            const bool fold = k <= 2 && i + 1 < n_ops && ops[i + 1].kind == GQ_OP_CHANNEL &&
+                              ops[i + 1].num_qubits == k && std::equal(ops[i + 1].qubits, ops[i + 1].qubits + k, op.qubits) &&
+                              ops[i + 1].matrix && ops[i + 1].num_kraus >= 1;
+            if (fold) {
+                // The channel that follows on the same qubits folds into one
+                // superoperator S * (U (x) conj(U)).
+                sop = matmul(superop((const Z*)ops[i + 1].matrix, ops[i + 1].num_kraus, k), unitary_superop(u, k), d * d);
+                ++i;
+            } else {
+                // U on the row qubits, conj(U) on the column qubits.
+                std::vector<int> rq, cq;
+                for (int j = 0; j < k; ++j) {
+                    rq.push_back(op.qubits[j] + nq);
+                    cq.push_back(op.qubits[j]);
+                }
+                std::vector<Z> uc(u);
+                for (auto& z : uc) z.im = -z.im;
+                int rc = analyze_matrix(u, rq, 0, (int)i, gates, err);
+                if (rc == GQ_OK) rc = analyze_matrix(uc, cq, 0, (int)i, gates, err);
+                if (rc != GQ_OK) { err = "op " + std::to_string(i) + ": " + err; return rc; }
+                continue;
+            }
+        }
+        int rc = analyze_matrix(sop, vec_qubits(op), 0, (int)i, gates, err);
+        if (rc != GQ_OK) { err = "op " + std::to_string(i) + ": " + err; return rc; }
+    }
+    return GQ_OK;
+}
+
+
 }  // namespace gq

@@ -61,5 +61,10 @@ int normalize_op(const gq_op& op, int nphys, std::vector<NGate>& out, std::strin
 int analyze_matrix(const std::vector<Z>& m, const std::vector<int>& qubits, uint64_t ctrl, int src,
                    std::vector<NGate>& out, std::string& err);
 void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& opt, Program& prog);
+// Density matrix ops -> NGates on the 2n-qubit vectorised rho (row qubit q is
+// vector bit q+n, column qubit q is bit q): U on rows and conj(U) on columns,
+// channels as sum_k E_k (x) conj(E_k), a gate and the channel that follows it
+// on the same qubits folded into one superoperator.
+int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, std::string& err);
 
 }  // namespace gq

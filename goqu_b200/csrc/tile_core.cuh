@@ -91,10 +91,41 @@ struct PassDesc {
     int32_t outer_q[MAX_QUBITS]; // global qubit of CTA-index bit k
 };
 
-template <class T>
-GQ_HD cplx<T> ldc(const cplx<T>* p, uint32_t i) {
+// Read-only load of a complex constant (all threads of a CTA read the same
+// program data, so these are broadcasts through the L1 cache).
+GQ_HD cplx<double> ldc(const cplx<double>* p, uint32_t i) {
 #if defined(__CUDA_ARCH__)
-    return __ldg(p + i);
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p + i));
+    return {v.x, v.y};
+#else
+    return p[i];
+#endif
+}
+GQ_HD cplx<float> ldc(const cplx<float>* p, uint32_t i) {
+#if defined(__CUDA_ARCH__)
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p + i));
+    return {v.x, v.y};
+#else
+    return p[i];
+#endif
+}
+
+// Same load, but not merged or hoisted by the compiler: used where a matrix
+// is too large to keep in registers across the unrolled amplitude groups.
+GQ_HD cplx<double> ldc_v(const cplx<double>* p, uint32_t i) {
+#if defined(__CUDA_ARCH__)
+    double x, y;
+    asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "l"(p + i));
+    return {x, y};
+#else
+    return p[i];
+#endif
+}
+GQ_HD cplx<float> ldc_v(const cplx<float>* p, uint32_t i) {
+#if defined(__CUDA_ARCH__)
+    float x, y;
+    asm volatile("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(x), "=f"(y) : "l"(p + i));
+    return {x, y};
 #else
     return p[i];
 #endif
@@ -173,24 +204,26 @@ GQ_HD void k_u3(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
         for (int r = 0; r < 8; ++r) {
             cplx<T> o = {T(0), T(0)};
 #pragma unroll
-            for (int c = 0; c < 8; ++c) o = cfma(ldc(m, r * 8 + c), v[c], o);
+            for (int c = 0; c < 8; ++c) o = cfma(ldc_v(m, r * 8 + c), v[c], o);
             a[idx[r]] = o;
         }
     }
 }
 
+// 16x16 on all register bits. The outputs go straight to the thread's own
+// shared-memory slots (so only the 16 inputs stay live in registers) and are
+// read back afterwards; no other thread touches those slots in this phase.
 template <class T>
-GQ_HD void k_u4(cplx<T> (&a)[NREG], const cplx<T>* m) {
-    cplx<T> v[NREG];
-#pragma unroll
-    for (int c = 0; c < NREG; ++c) v[c] = a[c];
-#pragma unroll
+GQ_HD void k_u4(cplx<T> (&a)[NREG], const cplx<T>* m, cplx<T>* sm, uint32_t sbase, const uint32_t* rslot) {
+#pragma unroll 1
     for (int r = 0; r < NREG; ++r) {
         cplx<T> o = {T(0), T(0)};
 #pragma unroll
-        for (int c = 0; c < NREG; ++c) o = cfma(ldc(m, r * NREG + c), v[c], o);
-        a[r] = o;
+        for (int c = 0; c < NREG; ++c) o = cfma(ldc_v(m, r * NREG + c), a[c], o);
+        sm[sbase ^ rslot[r]] = o;
     }
+#pragma unroll
+    for (int r = 0; r < NREG; ++r) a[r] = sm[sbase ^ rslot[r]];
 }
 
 template <class T, int S>
@@ -277,7 +310,8 @@ GQ_HD void k_phase(cplx<T> (&a)[NREG], const cplx<T> s, uint32_t creg) {
 // Applies one op to the thread's 16 amplitudes. g0 is the global index of the
 // thread's register slot 0 (its thread bits and the CTA's base).
 template <class T>
-GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint64_t g0) {
+GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint64_t g0, cplx<T>* sm,
+                    uint32_t sbase, const uint32_t* rslot) {
     if ((g0 & op.cmask) != op.cmask) return;
     const cplx<T>* m = pool + op.mat;
     const uint32_t creg = op.creg;
@@ -309,7 +343,7 @@ GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint
             }
             break;
         case K_U4:
-            k_u4<T>(a, m);
+            k_u4<T>(a, m, sm, sbase, rslot);
             break;
         case K_X: {
             const bool pure = op.flags & 1;
@@ -387,7 +421,7 @@ GQ_HD void run_phase(cplx<T>* sm, const PhaseDesc& ph, const KOp* ops, const cpl
     cplx<T> a[NREG];
 #pragma unroll
     for (int j = 0; j < NREG; ++j) a[j] = sm[sbase ^ ph.rslot[j]];
-    for (int o = ph.op_begin; o < ph.op_end; ++o) apply_op<T>(a, ops[o], pool, g0);
+    for (int o = ph.op_begin; o < ph.op_end; ++o) apply_op<T>(a, ops[o], pool, g0, sm, sbase, ph.rslot);
 #pragma unroll
     for (int j = 0; j < NREG; ++j) sm[sbase ^ ph.rslot[j]] = a[j];
 }

@@ -110,7 +110,11 @@ typedef struct gq_stats {
     int64_t kernel_launches; /* kernels of this library launched                  */
     int64_t phases;          /* register phases summed over all passes            */
     int64_t state_bytes;     /* bytes of one state (2^n * amplitude size)          */
-    double last_ms;          /* device time of the last apply (CUDA events)        */
+    double last_ms;          /* device time of the last apply/evolve call, CUDA events
+                                on the handle's stream (GQ_OPT_TIMING only)           */
+    double pass_ms;          /* device time of its tile passes alone                */
+    int64_t h2d_bytes;       /* host->device bytes the last call copied (program, inputs) */
+    int64_t d2h_bytes;       /* device->host bytes the last call copied (results)   */
 } gq_stats;
 
 /* ---- library ------------------------------------------------------------- */
@@ -203,6 +207,7 @@ int gq_dm_fidelity(gq_dm* dm, const double* psi, size_t n, double* out);
 int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* uniforms,
                  size_t shots, uint64_t* idx_out);
 int gq_dm_stats(const gq_dm* dm, gq_stats* out);
+int gq_dm_set_option(gq_dm* dm, int key, int64_t value);
 
 #ifdef __cplusplus
 }

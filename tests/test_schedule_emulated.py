@@ -87,3 +87,37 @@ def test_emulated_qft_and_brickwork(emu):
     got, passes, _ = run_emu(emu, ops, tile=10)
     np.testing.assert_allclose(got, want, atol=1e-12, rtol=0)
     assert passes < len(ops)  # gates were fused into passes
+
+
+def _emu_dm(emu, stream, tile=0, budget=0):
+    n = stream.num_qubits
+    rho = np.zeros(1 << (2 * n), dtype=np.complex128)
+    rho[0] = 1
+    emu.gqx_emulate_dm.restype = ctypes.c_int
+    emu.gqx_emulate_dm.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_abi.gq_op),
+                                   ctypes.c_size_t, ctypes.c_int, ctypes.c_int]
+    rc = emu.gqx_emulate_dm(n, rho.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            stream.ptr(), len(stream), tile, budget)
+    assert rc == 0, emu.gqx_last_error()
+    return rho
+
+
+@pytest.mark.parametrize("n,seed,tile", [(1, 1, 0), (2, 2, 0), (3, 3, 0), (4, 4, 6), (5, 5, 8), (6, 6, 0)])
+def test_emulated_density_matrix_matches_oracle(emu, n, seed, tile):
+    from goqu_b200 import noise as N
+    c = random_circuit(n, 30, seed, allow_3q=False, allow_ctrl=False, allow_reset=True)
+    nm = N.New()
+    nm.AddDefaultError(1, N.Depolarizing1Q(0.05))
+    nm.AddDefaultError(2, N.Depolarizing2Q(0.05))
+    nm.AddGateError("H", N.AmplitudeDamping(0.1))
+    ops = encode.density_ops(c, nm)
+    want = orc.dm_evolve(ops)
+    got = _emu_dm(emu, ops, tile=tile)
+    np.testing.assert_allclose(got, want, atol=1e-12, rtol=0)
+
+
+def test_emulated_noisy_brickwork(emu):
+    from goqu_b200 import workloads
+    c, nm = workloads.noisy_brickwork(5, layers=4, seed=1)
+    ops = encode.density_ops(c, nm)
+    np.testing.assert_allclose(_emu_dm(emu, ops), orc.dm_evolve(ops), atol=1e-12, rtol=0)
