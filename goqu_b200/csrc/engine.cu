@@ -325,18 +325,24 @@ struct Engine {
     }
 
     // ---- sampling --------------------------------------------------------
+    // Exact inverse-CDF sampling (see k_chunk_steps in kernels.cuh). The
+    // exact chunk-end sums are cached until the state changes.
     template <class P>
     int sample_impl(P prob, uint64_t n, const double* uniforms, size_t shots, uint64_t* idx_out) {
         if (shots == 0) return GQ_OK;
         const int chunk_log = n >= 2048 ? 11 : (int)std::max<uint64_t>(0, (uint64_t)std::log2((double)n));
         const uint64_t nchunks = (n + (1ull << chunk_log) - 1) >> chunk_log;
-        // scratch: sums | incl | ends ; scratch2 (io): uniforms | out | flags
-        GQ_TRY(scratch.ensure(3 * nchunks * sizeof(double) + 64));
-        double* sums = (double*)scratch.p;
-        double* incl = sums + nchunks;
-        double* ends = incl + nchunks;
-        const size_t o_u = 0, o_out = align16(shots * 8), o_flags = o_out + align16(shots * 8);
-        const size_t io = o_flags + align16(shots * 4);
+        // scratch: sums | incl | ends | steps | cexp | clean | n_seq
+        const size_t o_sums = 0, o_incl = o_sums + align16(nchunks * 8), o_ends = o_incl + align16(nchunks * 8);
+        const size_t o_steps = o_ends + align16(nchunks * 8), o_exp = o_steps + align16(nchunks * 8);
+        const size_t o_clean = o_exp + align16(nchunks * 4), o_nseq = o_clean + align16(nchunks * 4);
+        GQ_TRY(scratch.ensure(o_nseq + 16));
+        char* sc = (char*)scratch.p;
+        double* sums = (double*)(sc + o_sums);
+        double* incl = (double*)(sc + o_incl);
+        double* ends = (double*)(sc + o_ends);
+        const size_t o_u = 0, o_out = align16(shots * 8);
+        const size_t io = o_out + align16(shots * 8);
         void* hp = nullptr;
         GQ_TRY(stage(io, &hp));
         std::memcpy((char*)hp + o_u, uniforms, shots * 8);
@@ -344,27 +350,16 @@ struct Engine {
         char* d = (char*)scratch2.p;
         k_chunk_sums<P><<<(unsigned)nchunks, 256, 0, stream>>>(prob, n, chunk_log, sums);
         k_scan_chunks<<<1, 1024, 0, stream>>>(sums, nchunks, incl);
-        const unsigned warps_per_block = 8;
-        k_sample<P><<<(unsigned)((shots + warps_per_block - 1) / warps_per_block), 32 * warps_per_block, 0, stream>>>(
-            prob, n, chunk_log, incl, nchunks, (const double*)(d + o_u), shots, (uint64_t*)(d + o_out),
-            (int*)(d + o_flags));
+        k_chunk_steps<P><<<(unsigned)nchunks, 256, 0, stream>>>(prob, n, chunk_log, incl, (long long*)(sc + o_steps),
+                                                               (int*)(sc + o_exp), (int*)(sc + o_clean));
+        k_chunk_walk<P><<<1, 1, 0, stream>>>(prob, n, chunk_log, (const long long*)(sc + o_steps),
+                                             (const int*)(sc + o_exp), (const int*)(sc + o_clean), nchunks, ends,
+                                             (int*)(sc + o_nseq));
+        k_sample_find<P><<<(unsigned)((shots + 127) / 128), 128, 0, stream>>>(
+            prob, n, chunk_log, ends, nchunks, (const double*)(d + o_u), shots, (uint64_t*)(d + o_out));
         GQ_CUDA(cudaGetLastError());
-        stats.kernel_launches += 3;
-        GQ_TRY(hostio.ensure(shots * 4 + 16));
-        GQ_CUDA(cudaMemcpyAsync(hostio.p, d + o_flags, shots * 4, cudaMemcpyDeviceToHost, stream));
-        GQ_CUDA(cudaStreamSynchronize(stream));
-        const int* fl = (const int*)hostio.p;
-        size_t nflag = 0;
-        for (size_t i = 0; i < shots; ++i) nflag += fl[i] != 0;
-        if (nflag) {
-            k_seq_chunk_ends<P><<<1, 1, 0, stream>>>(prob, n, chunk_log, ends);
-            k_sample_exact<P><<<(unsigned)((shots + 255) / 256), 256, 0, stream>>>(
-                prob, n, chunk_log, ends, nchunks, (const double*)(d + o_u), (const int*)(d + o_flags), shots,
-                (uint64_t*)(d + o_out));
-            GQ_CUDA(cudaGetLastError());
-            stats.kernel_launches += 2;
-        }
-        stats.d2h_bytes += (int64_t)(shots * 8 + shots * 4);
+        stats.kernel_launches += 5;
+        stats.d2h_bytes += (int64_t)(shots * 8);
         GQ_CUDA(cudaMemcpyAsync(idx_out, d + o_out, shots * 8, cudaMemcpyDeviceToHost, stream));
         GQ_CUDA(cudaStreamSynchronize(stream));
         return GQ_OK;

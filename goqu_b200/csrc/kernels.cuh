@@ -189,109 +189,122 @@ __global__ void k_scan_chunks(const double* __restrict__ sums, uint64_t nchunks,
     }
 }
 
-// Inverse-CDF search, one warp per shot. The FP64 prefix S_j computed here
-// differs from goqu's sequential running sum s_j (sampleIndex,
-// sim/statevector/sim.go:288-298) by at most bound(j) = (j + 1 + 4096) *
-// 2^-52 * S_j: every step of the sequential sum rounds by at most 2^-53 s_j
-// and this kernel's summation tree is at most a few thousand additions deep.
-// A shot whose uniform lies within that bound of S_{idx-1} or S_idx is
-// flagged and resolved exactly by k_sample_exact.
-__device__ __forceinline__ double seq_bound(uint64_t j, double s) {
-    return ((double)j + 4097.0) * 2.220446049250313e-16 * (s + 1e-300);
+// ---------------------------------------------------------------------------
+// Exact inverse-CDF sampling.
+//
+// goqu's sampleIndex (sim/statevector/sim.go:288-298) scans cum += p_j in FP64
+// and returns the first j with r < cum. The sum is reproduced exactly here
+// without a 2^n-long dependency chain: while the running sum s stays in one
+// binade [2^e, 2^(e+1)), every step rounds s + p_j to the grid u = 2^(e-52),
+// so s advances by an integer number of grid steps, round-to-nearest(p_j / u)
+// (an exact-half tie would depend on the parity of s: such chunks are handled
+// sequentially). A chunk whose running sum stays inside one binade therefore
+// advances s by u * (an exact int64 sum of per-element steps). Chunks that
+// start at zero, straddle a binade boundary or contain a tie (a few dozen at
+// most) are summed sequentially with the same FP64 additions as goqu.
+//   k_chunk_sums / k_scan_chunks: approximate chunk-end sums (FP64 tree),
+//       used only to predict each chunk's binade;
+//   k_chunk_steps: per chunk, the exact int64 step count for the predicted
+//       binade (or "not clean");
+//   k_chunk_walk: one thread walks the chunks with the exact running sum,
+//       taking clean chunks in O(1) and the others element by element;
+//   k_sample_find: per shot, a binary search on the exact chunk ends and an
+//       exact sequential scan inside the chunk.
+__device__ __forceinline__ int exponent_of(double x) { return ilogb(x); }
+
+template <class P>
+__global__ void k_chunk_steps(P prob, uint64_t n, int chunk_log, const double* __restrict__ incl,
+                              long long* __restrict__ steps, int* __restrict__ cexp, int* __restrict__ clean) {
+    const uint64_t c = blockIdx.x;
+    const double s0 = c ? incl[c - 1] : 0.0, s1 = incl[c];
+    // Predicted binade of the whole chunk, with a margin far above the error
+    // of the approximate sums (~1e-12 relative).
+    bool ok = s0 > 0x1p-1000;
+    int e = 0;
+    if (ok) {
+        e = exponent_of(s0);
+        const double lo = ldexp(1.0, e), hi = ldexp(1.0, e + 1);
+        ok = s0 >= lo * (1.0 + 0x1p-30) && s1 <= hi * (1.0 - 0x1p-30);
+    }
+    if (!ok) {
+        if (threadIdx.x == 0) {
+            steps[c] = 0;
+            cexp[c] = e;
+            clean[c] = 0;
+        }
+        return;
+    }
+    const uint64_t c0 = c << chunk_log;
+    const uint64_t len = (uint64_t)1 << chunk_log;
+    long long sum = 0;
+    int tie = 0;
+    for (uint64_t j = threadIdx.x; j < len; j += blockDim.x) {
+        if (c0 + j >= n) break;
+        const double q = ldexp(prob(c0 + j), 52 - e);  // exact: a power-of-two scaling
+        const double f = floor(q);
+        const double fr = q - f;                       // exact
+        long long k = (long long)f;
+        if (fr > 0.5) ++k;
+        if (fr == 0.5) tie = 1;
+        sum += k;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        tie |= __shfl_xor_sync(0xffffffffu, tie, o);
+    }
+    __shared__ long long ws[32];
+    __shared__ int wt[32];
+    if ((threadIdx.x & 31) == 0) {
+        ws[threadIdx.x >> 5] = sum;
+        wt[threadIdx.x >> 5] = tie;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t = 0;
+        int ti = 0;
+        for (unsigned w = 0; w < (blockDim.x >> 5); ++w) {
+            t += ws[w];
+            ti |= wt[w];
+        }
+        steps[c] = t;
+        cexp[c] = e;
+        clean[c] = !ti;
+    }
 }
 
 template <class P>
-__global__ void k_sample(P prob, uint64_t n, int chunk_log, const double* __restrict__ incl, uint64_t nchunks,
-                         const double* __restrict__ uniforms, uint64_t shots, uint64_t* __restrict__ out,
-                         int* __restrict__ flags) {
-    const uint64_t shot = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (shot >= shots) return;
-    const double r = uniforms[shot];
-    // First chunk with r < incl[c] (binary search).
-    uint64_t lo = 0, hi = nchunks;
-    while (lo < hi) {
-        const uint64_t mid = (lo + hi) >> 1;
-        if (r < incl[mid])
-            hi = mid;
-        else
-            lo = mid + 1;
-    }
-    int flag = 0;
-    uint64_t idx = n - 1;
-    if (lo == nchunks) {
-        // r beyond the total: goqu falls back to the last index.
-        const double tot = nchunks ? incl[nchunks - 1] : 0.0;
-        if (r - tot < seq_bound(n - 1, tot)) flag = 1;
-    } else {
-        const uint64_t c = lo;
-        const uint64_t c0 = c << chunk_log;
-        const uint64_t len = ((uint64_t)1 << chunk_log) < n - c0 ? ((uint64_t)1 << chunk_log) : n - c0;
-        const uint64_t seg = (len + 31) / 32;
-        const uint64_t b = c0 + lane * seg;
-        const uint64_t e = (b + seg < c0 + len) ? b + seg : c0 + len;
-        double s = 0.0;
-        for (uint64_t j = b; j < e; ++j) s += prob(j);
-        // exclusive scan over lanes
-        double x = s;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const double y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        const double excl_c = c ? incl[c - 1] : 0.0;
-        double run = excl_c + (x - s);
-        double prev = run;
-        uint64_t hit = ~0ull;
-        double s_hit = 0.0, s_prev = 0.0;
-        for (uint64_t j = b; j < e; ++j) {
-            prev = run;
-            run += prob(j);
-            if (r < run) {
-                hit = j;
-                s_hit = run;
-                s_prev = prev;
-                break;
+__global__ void k_chunk_walk(P prob, uint64_t n, int chunk_log, const long long* __restrict__ steps,
+                             const int* __restrict__ cexp, const int* __restrict__ clean, uint64_t nchunks,
+                             double* __restrict__ ends, int* __restrict__ n_seq) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double s = 0.0;
+    int seq = 0;
+    const uint64_t len = (uint64_t)1 << chunk_log;
+    for (uint64_t c = 0; c < nchunks; ++c) {
+        const int e = cexp[c];
+        if (clean[c] && s > 0.0 && exponent_of(s) == e) {
+            const double t = s + ldexp((double)steps[c], e - 52);  // exact below 2^(e+1)
+            if (t < ldexp(1.0, e + 1)) {
+                s = t;
+                ends[c] = s;
+                continue;
             }
         }
-        const unsigned found = __ballot_sync(0xffffffffu, hit != ~0ull);
-        if (found == 0) {
-            flag = 1;  // the chunk-level and lane-level sums disagreed
-        } else {
-            const int src = __ffs(found) - 1;
-            idx = __shfl_sync(0xffffffffu, hit, src);
-            const double sh = __shfl_sync(0xffffffffu, s_hit, src);
-            const double sp = __shfl_sync(0xffffffffu, s_prev, src);
-            if (sh - r <= seq_bound(idx, sh)) flag = 1;
-            if (idx > 0 && r - sp < seq_bound(idx - 1, sp + (sh - sp))) flag = 1;
-        }
+        ++seq;
+        const uint64_t c0 = c << chunk_log;
+        const uint64_t e1 = c0 + len < n ? c0 + len : n;
+        for (uint64_t j = c0; j < e1; ++j) s = __dadd_rn(s, prob(j));
+        ends[c] = s;
     }
-    if (lane == 0) {
-        out[shot] = idx;
-        flags[shot] = flag;
-    }
+    *n_seq = seq;
 }
 
-// Exact sequential running sums at every chunk end, in goqu's order (one
-// thread; used only when a shot was flagged).
 template <class P>
-__global__ void k_seq_chunk_ends(P prob, uint64_t n, int chunk_log, double* __restrict__ ends) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    double cum = 0.0;
-    const uint64_t len = (uint64_t)1 << chunk_log;
-    for (uint64_t j = 0; j < n; ++j) {
-        cum = __dadd_rn(cum, prob(j));
-        if ((j & (len - 1)) == len - 1 || j == n - 1) ends[j >> chunk_log] = cum;
-    }
-}
-
-// Exact resolution of flagged shots from the exact chunk-end sums.
-template <class P>
-__global__ void k_sample_exact(P prob, uint64_t n, int chunk_log, const double* __restrict__ ends,
-                               uint64_t nchunks, const double* __restrict__ uniforms, const int* __restrict__ flags,
-                               uint64_t shots, uint64_t* __restrict__ out) {
+__global__ void k_sample_find(P prob, uint64_t n, int chunk_log, const double* __restrict__ ends, uint64_t nchunks,
+                              const double* __restrict__ uniforms, uint64_t shots, uint64_t* __restrict__ out) {
     const uint64_t shot = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (shot >= shots || !flags[shot]) return;
+    if (shot >= shots) return;
     const double r = uniforms[shot];
     uint64_t lo = 0, hi = nchunks;
     while (lo < hi) {

@@ -40,6 +40,7 @@ def lib():
             "or_sv_probabilities": (None, [ctypes.c_int, _D, _D]),
             "or_sample": (None, [_D, ctypes.c_uint64, _D, ctypes.c_size_t, _U64]),
             "or_cumsum_at": (None, [_D, ctypes.c_uint64, _U64, ctypes.c_size_t, _D]),
+            "or_cumsum": (None, [_D, ctypes.c_uint64, _D]),
             "or_sv_expect_pauli_sum": (None, [ctypes.c_int, _D, _TP, ctypes.c_size_t, ctypes.c_int, _D, _D]),
             "or_sv_expect_z": (ctypes.c_double, [ctypes.c_int, _D, ctypes.c_uint64, ctypes.c_int]),
             "or_dm_apply": (ctypes.c_int, [ctypes.c_int, _D, _OPP, ctypes.c_size_t, ctypes.c_int]),
@@ -94,6 +95,16 @@ def sample(probs, uniforms):
     out = np.empty(u.size, dtype=np.uint64)
     lib().or_sample(_dp(probs), probs.size, _dp(u), u.size, out.ctypes.data_as(_U64))
     return out
+
+
+def sample_fast(probs, uniforms):
+    """sampleIndex for many shots: the sequential running sum once, then a
+    sorted search (first i with r < cum_i; the last index when none)."""
+    probs = np.ascontiguousarray(probs, dtype=np.float64)
+    cum = np.empty_like(probs)
+    lib().or_cumsum(_dp(probs), probs.size, _dp(cum))
+    idx = np.searchsorted(cum, np.asarray(uniforms, dtype=np.float64), side="right")
+    return np.minimum(idx, probs.size - 1).astype(np.uint64)
 
 
 def cumsum_at(probs, indices):

@@ -661,6 +661,16 @@ void or_cumsum_at(const double* probs, uint64_t len, const uint64_t* at, size_t 
     }
 }
 
+// The full sequential running sum cum_i = (((p_0 + p_1) + p_2) + ... + p_i),
+// so that sampleIndex(r) = first i with r < cum_i (a sorted search).
+void or_cumsum(const double* probs, uint64_t len, double* out) {
+    double cum = 0.0;
+    for (uint64_t i = 0; i < len; ++i) {
+        cum += probs[i];
+        out[i] = cum;
+    }
+}
+
 // pauli.Expect / ExpectSum (sim/pauli/expect_sv.go:21-97).
 void or_sv_expect_pauli_sum(int nq, const double* state, const gq_pauli_term* terms, size_t n_terms,
                             int threads, double* out_re, double* out_im) {

@@ -142,6 +142,22 @@ def test_sampling_bit_exact_on_boundaries():
     assert np.array_equal(sim.Sample(u), orc.sample(probs, u))
 
 
+@pytest.mark.parametrize("n,prec", [(20, _abi.GQ_C128), (24, _abi.GQ_C128), (22, _abi.GQ_C64)])
+def test_sampling_bit_exact_large_states(n, prec):
+    # large states: every interval p_i is far below any a-priori rounding
+    # bound, so this exercises the exact binade-step sampler end to end
+    c = workloads.random_layers(n, layers=3, seed=n)
+    sim = evolve(c, prec)
+    probs = orc.probabilities(sim.StateVector())
+    u = statevector.uniforms(4096, np.random.default_rng(n))
+    assert np.array_equal(sim.Sample(u), orc.sample_fast(probs, u))
+    sel = np.random.default_rng(1).choice(probs.size - 1, 32, replace=False)
+    _, cum = orc.cumsum_at(probs, sel)
+    uu = np.concatenate([cum, np.nextafter(cum, 0), np.nextafter(cum, 2)])
+    uu = uu[uu < 1.0]
+    assert np.array_equal(sim.Sample(uu), orc.sample_fast(probs, uu))
+
+
 def test_sampling_degenerate_states():
     # |0...0>: every uniform maps to index 0; uniform superposition: exact dyadic sums
     sim = statevector.New(12)

@@ -117,6 +117,14 @@ def test_oracle_sample_is_sequential_inverse_cdf():
     assert got.tolist() == want
 
 
+def test_oracle_fast_sampler_equals_scan():
+    rng = np.random.default_rng(4)
+    p = rng.random(4096) ** 4
+    p /= p.sum()
+    u = np.concatenate([rng.integers(0, 1 << 53, 500) / float(1 << 53), [0.0, np.nextafter(1.0, 0)]])
+    assert np.array_equal(orc.sample_fast(p, u), orc.sample(p, u))
+
+
 def test_oracle_density_matches_statevector_noiseless():
     # sim/densitymatrix/sim_test.go:46-120: noiseless rho = |psi><psi|
     for seed in range(4):
