@@ -46,6 +46,7 @@ GQ_OPT_TILE_QUBITS = 1
 GQ_OPT_PASS_BUDGET = 2
 GQ_OPT_LOW_QUBITS = 3
 GQ_OPT_TIMING = 4
+GQ_OPT_KERNEL_VARIANT = 5
 
 _DBL_P = ctypes.POINTER(ctypes.c_double)
 

@@ -36,7 +36,7 @@ void run_program(std::vector<gq::cplx<T>>& st, const gq::Program& prog) {
             for (int p = 0; p < pd.n_phases; ++p) {
                 const gq::PhaseDesc& ph = prog.phases[pd.phase0 + p];
                 for (uint32_t t = 0; t < tpb; ++t)
-                    gq::run_phase<T>(sm.data(), ph, prog.ops.data(), pool.data(), t, m - gq::RQ, base);
+                    gq::run_phase<T>(sm.data(), ph, prog.ops.data(), pool.data(), t, base);
             }
             for (uint32_t lin = 0; lin < (1u << m); ++lin) {
                 uint64_t goff;

@@ -100,13 +100,53 @@ struct PinnedBuf {
 
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// FMA-per-amplitude budget of a pass: the measured optimum of the 28-qubit
+// layered benchmark (larger budgets trade passes for compute per pass).
+constexpr int kDefaultBudget = 256;
+
+// Tile-pass kernel instantiations (see kVariants* in kernels.cuh).
+using TileKernelD = void (*)(cplx<double>*, const PassDesc*, const PhaseDesc*, const KOp*, const cplx<double>*);
+using TileKernelF = void (*)(cplx<float>*, const PassDesc*, const PhaseDesc*, const KOp*, const cplx<float>*);
+const TileKernelD kTileD[kNumVariants] = {
+    k_tile_pass<double, kVariantsC128[0].threads, kVariantsC128[0].min_blocks>,
+    k_tile_pass<double, kVariantsC128[1].threads, kVariantsC128[1].min_blocks>,
+    k_tile_pass<double, kVariantsC128[2].threads, kVariantsC128[2].min_blocks>,
+    k_tile_pass<double, kVariantsC128[3].threads, kVariantsC128[3].min_blocks>};
+const TileKernelF kTileF[kNumVariants] = {
+    k_tile_pass<float, kVariantsC64[0].threads, kVariantsC64[0].min_blocks>,
+    k_tile_pass<float, kVariantsC64[1].threads, kVariantsC64[1].min_blocks>,
+    k_tile_pass<float, kVariantsC64[2].threads, kVariantsC64[2].min_blocks>,
+    k_tile_pass<float, kVariantsC64[3].threads, kVariantsC64[3].min_blocks>};
+
+template <class T>
+struct TileTable;
+template <>
+struct TileTable<double> {
+    static TileKernelD get(int v) { return kTileD[v]; }
+    static int threads(int v) { return kVariantsC128[v].threads; }
+};
+template <>
+struct TileTable<float> {
+    static TileKernelF get(int v) { return kTileF[v]; }
+    static int threads(int v) { return kVariantsC64[v].threads; }
+};
+
+int log2i(int x) {
+    int r = 0;
+    while ((1 << (r + 1)) <= x) ++r;
+    return r;
+}
+
 template <class T>
 int set_smem_attr() {
     static std::once_flag once;
     static cudaError_t err = cudaSuccess;
     std::call_once(once, [] {
-        err = cudaFuncSetAttribute(k_tile_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(sizeof(cplx<T>) << TileShape<T>::kMaxTile));
+        for (int v = 0; v < kNumVariants && err == cudaSuccess; ++v) {
+            const int m = log2i(TileTable<T>::threads(v)) + RQ;
+            err = cudaFuncSetAttribute(TileTable<T>::get(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(cplx<T>) << m));
+        }
     });
     if (err != cudaSuccess) return fail(GQ_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
     return GQ_OK;
@@ -128,8 +168,11 @@ struct Engine {
     bool timing = false;
     gq_stats stats{};
 
+    int variant = 0;
     size_t amp_bytes() const { return prec == GQ_C64 ? 8 : 16; }
-    int max_tile() const { return prec == GQ_C64 ? TileShape<float>::kMaxTile : TileShape<double>::kMaxTile; }
+    int max_tile() const {
+        return RQ + log2i(prec == GQ_C64 ? kVariantsC64[variant].threads : kVariantsC128[variant].threads);
+    }
 
     int init(int nphys_, int prec_) {
         GQ_TRY(check_device(&device));
@@ -143,10 +186,11 @@ struct Engine {
         GQ_CUDA(cudaEventCreate(&ev_pass0));
         GQ_CUDA(cudaEventCreate(&ev_pass1));
         GQ_TRY(state.ensure(n_amps * amp_bytes()));
-        opt.tile_qubits = max_tile();
         opt.low_qubits = prec == GQ_C64 ? 4 : 3;
         opt.swizzle_width = prec == GQ_C64 ? 4 : 3;
-        opt.budget = 96;
+        variant = prec == GQ_C64 ? 1 : 0;
+        opt.tile_qubits = max_tile();
+        opt.budget = kDefaultBudget;
         stats.state_bytes = (int64_t)(n_amps * amp_bytes());
         GQ_TRY(prec == GQ_C64 ? set_smem_attr<float>() : set_smem_attr<double>());
         return reset_basis(0);
@@ -224,9 +268,9 @@ struct Engine {
             const unsigned threads = 1u << (pd.m - RQ);
             const size_t smem = sizeof(cplx<T>) << pd.m;
             const unsigned grid = 1u << pd.n_outer;
-            k_tile_pass<T><<<grid, threads, smem, stream>>>((cplx<T>*)state.p, (const PassDesc*)(d + o_pass) + i,
-                                                            (const PhaseDesc*)(d + o_phase), (const KOp*)(d + o_ops),
-                                                            (const cplx<T>*)(d + o_pool));
+            TileTable<T>::get(variant)<<<grid, threads, smem, stream>>>(
+                (cplx<T>*)state.p, (const PassDesc*)(d + o_pass) + i, (const PhaseDesc*)(d + o_phase),
+                (const KOp*)(d + o_ops), (const cplx<T>*)(d + o_pool));
         }
         GQ_CUDA(cudaGetLastError());
         if (timing) {
@@ -352,7 +396,7 @@ struct Engine {
         k_scan_chunks<<<1, 1024, 0, stream>>>(sums, nchunks, incl);
         k_chunk_steps<P><<<(unsigned)nchunks, 256, 0, stream>>>(prob, n, chunk_log, incl, (long long*)(sc + o_steps),
                                                                (int*)(sc + o_exp), (int*)(sc + o_clean));
-        k_chunk_walk<P><<<1, 1, 0, stream>>>(prob, n, chunk_log, (const long long*)(sc + o_steps),
+        k_chunk_walk<P><<<1, 32, 0, stream>>>(prob, n, chunk_log, (const long long*)(sc + o_steps),
                                              (const int*)(sc + o_exp), (const int*)(sc + o_clean), nchunks, ends,
                                              (int*)(sc + o_nseq));
         k_sample_find<P><<<(unsigned)((shots + 127) / 128), 128, 0, stream>>>(
@@ -562,7 +606,7 @@ int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
             return GQ_OK;
         case GQ_OPT_PASS_BUDGET:
             if (value < 0) return fail(GQ_EINVAL, "negative budget");
-            e.opt.budget = value == 0 ? 96 : (int)value;
+            e.opt.budget = value == 0 ? kDefaultBudget : (int)value;
             return GQ_OK;
         case GQ_OPT_LOW_QUBITS:
             if (value < 0 || value > 6) return fail(GQ_EINVAL, "low qubits out of range [0, 6]");
@@ -570,6 +614,11 @@ int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
             return GQ_OK;
         case GQ_OPT_TIMING:
             e.timing = value != 0;
+            return GQ_OK;
+        case GQ_OPT_KERNEL_VARIANT:
+            if (value < 0 || value >= kNumVariants) return fail(GQ_EINVAL, "kernel variant out of range");
+            e.variant = (int)value;
+            e.opt.tile_qubits = e.max_tile();
             return GQ_OK;
         default:
             return fail(GQ_EINVAL, "unknown option");
@@ -643,12 +692,18 @@ int gq_dm_set_option(gq_dm* dm, int key, int64_t value) {
     }
     if (key == GQ_OPT_PASS_BUDGET) {
         if (value < 0) return fail(GQ_EINVAL, "negative budget");
-        dm->e.opt.budget = value == 0 ? 96 : (int)value;
+        dm->e.opt.budget = value == 0 ? kDefaultBudget : (int)value;
         return GQ_OK;
     }
     if (key == GQ_OPT_TILE_QUBITS) {
         if (value < RQ || value > dm->e.max_tile()) return fail(GQ_EINVAL, "tile qubits out of range");
         dm->e.opt.tile_qubits = (int)value;
+        return GQ_OK;
+    }
+    if (key == GQ_OPT_KERNEL_VARIANT) {
+        if (value < 0 || value >= kNumVariants) return fail(GQ_EINVAL, "kernel variant out of range");
+        dm->e.variant = (int)value;
+        dm->e.opt.tile_qubits = dm->e.max_tile();
         return GQ_OK;
     }
     return fail(GQ_EINVAL, "unknown option");

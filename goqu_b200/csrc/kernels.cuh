@@ -12,22 +12,18 @@ namespace gq {
 // Tile pass: one CTA per tile, 2^(m-4) threads, 2^m amplitudes of shared memory.
 // The CTA stages its tile (16 coalesced loads per thread), runs the pass's
 // phases with a barrier between them, and writes the tile back in place.
-// Launch shape per precision: complex128 tiles of up to 2^11 amplitudes with
-// 128 threads (up to 168 registers, three CTAs per SM); complex64 tiles of up
-// to 2^12 amplitudes with 256 threads (two CTAs per SM).
-template <class T>
-struct TileShape;
-template <>
-struct TileShape<double> {
-    static constexpr int kMaxTile = 11, kThreads = 128, kMinBlocks = 3;
+// Launch shapes. THREADS = 2^(m-4) bounds the tile size of a variant; MINB is
+// the CTAs per SM the register allocation is sized for (65536 / (THREADS *
+// MINB) registers per thread).
+struct TileVariant {
+    int threads, min_blocks;
 };
-template <>
-struct TileShape<float> {
-    static constexpr int kMaxTile = 12, kThreads = 256, kMinBlocks = 2;
-};
+constexpr TileVariant kVariantsC128[] = {{128, 3}, {128, 4}, {256, 2}, {64, 6}};
+constexpr TileVariant kVariantsC64[] = {{256, 2}, {128, 4}, {512, 1}, {128, 3}};
+constexpr int kNumVariants = 4;
 
-template <class T>
-__global__ void __launch_bounds__(TileShape<T>::kThreads, TileShape<T>::kMinBlocks)
+template <class T, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
     k_tile_pass(cplx<T>* __restrict__ st, const PassDesc* __restrict__ pdp,
                                                    const PhaseDesc* __restrict__ phases,
                                                    const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool) {
@@ -77,7 +73,7 @@ __global__ void __launch_bounds__(TileShape<T>::kThreads, TileShape<T>::kMinBloc
     __syncthreads();
     const int nph = pd.n_phases;
     for (int p = 0; p < nph; ++p) {
-        run_phase<T>(sm, phases[pd.phase0 + p], ops, pool, t, tbits, base);
+        run_phase<T>(sm, phases[pd.phase0 + p], ops, pool, t, base);
         __syncthreads();
     }
 #pragma unroll
@@ -273,31 +269,64 @@ __global__ void k_chunk_steps(P prob, uint64_t n, int chunk_log, const double* _
     }
 }
 
+// One warp walks the chunks 32 at a time. When the running sum s and all 32
+// chunks of a group are clean in s's binade, their ends are s plus u times
+// the group's int64 inclusive prefix (exact while below 2^(e+1)); otherwise
+// the group is walked chunk by chunk, non-clean chunks element by element.
 template <class P>
 __global__ void k_chunk_walk(P prob, uint64_t n, int chunk_log, const long long* __restrict__ steps,
                              const int* __restrict__ cexp, const int* __restrict__ clean, uint64_t nchunks,
                              double* __restrict__ ends, int* __restrict__ n_seq) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
     double s = 0.0;
     int seq = 0;
     const uint64_t len = (uint64_t)1 << chunk_log;
-    for (uint64_t c = 0; c < nchunks; ++c) {
-        const int e = cexp[c];
-        if (clean[c] && s > 0.0 && exponent_of(s) == e) {
-            const double t = s + ldexp((double)steps[c], e - 52);  // exact below 2^(e+1)
-            if (t < ldexp(1.0, e + 1)) {
-                s = t;
-                ends[c] = s;
-                continue;
+    for (uint64_t g = 0; g < nchunks; g += 32) {
+        const uint64_t c = g + lane;
+        const bool in = c < nchunks;
+        const long long st = in ? steps[c] : 0;
+        const int e = in ? cexp[c] : 0;
+        const int cl = in ? clean[c] : 1;
+        // inclusive int64 prefix over the lanes
+        long long pre = st;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += y;
+        }
+        const int se = s > 0.0 ? exponent_of(s) : -100000;
+        const bool lane_ok = !in || (cl && e == se);
+        const long long total = __shfl_sync(0xffffffffu, pre, 31);
+        bool fast = __all_sync(0xffffffffu, lane_ok) && s > 0.0;
+        if (fast) fast = s + ldexp((double)total, se - 52) < ldexp(1.0, se + 1);
+        if (fast) {
+            if (in) ends[c] = s + ldexp((double)pre, se - 52);
+            s = s + ldexp((double)total, se - 52);
+            continue;
+        }
+        // slow group: lane 0 walks it, the other lanes wait at the shuffle
+        if (lane == 0) {
+            for (uint64_t cc = g; cc < g + 32 && cc < nchunks; ++cc) {
+                const int ec = cexp[cc];
+                if (clean[cc] && s > 0.0 && exponent_of(s) == ec) {
+                    const double t = s + ldexp((double)steps[cc], ec - 52);
+                    if (t < ldexp(1.0, ec + 1)) {
+                        s = t;
+                        ends[cc] = s;
+                        continue;
+                    }
+                }
+                ++seq;
+                const uint64_t c0 = cc << chunk_log;
+                const uint64_t e1 = c0 + len < n ? c0 + len : n;
+                for (uint64_t jj = c0; jj < e1; ++jj) s = __dadd_rn(s, prob(jj));
+                ends[cc] = s;
             }
         }
-        ++seq;
-        const uint64_t c0 = c << chunk_log;
-        const uint64_t e1 = c0 + len < n ? c0 + len : n;
-        for (uint64_t j = c0; j < e1; ++j) s = __dadd_rn(s, prob(j));
-        ends[c] = s;
+        s = __shfl_sync(0xffffffffu, s, 0);
     }
-    *n_seq = seq;
+    if (lane == 0) *n_seq = seq;
 }
 
 template <class P>

@@ -411,23 +411,42 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                     rtb[nr] = b;
                     ++nr;
                 }
+            uint32_t tslot[MAX_TILE];
+            uint64_t tglob[MAX_TILE];
             int nb = 0;
             for (int b = 0; b < m; ++b)
                 if (!(R & (1ull << tile_q[b]))) {
-                    ph.tslot[nb] = pd.acol[b];
-                    ph.tq[nb] = tile_q[b];
+                    tslot[nb] = pd.acol[b];
+                    tglob[nb] = 1ull << tile_q[b];
                     ++nb;
                 }
+            for (int v = 0; v < TLO; ++v) {
+                uint32_t sv = 0;
+                uint64_t gv = 0;
+                for (int b = 0; b < 4 && b < nb; ++b)
+                    if ((v >> b) & 1) {
+                        sv ^= tslot[b];
+                        gv |= tglob[b];
+                    }
+                ph.tlo_slot[v] = sv;
+                ph.tlo_glob[v] = gv;
+            }
+            for (int v = 0; v < THI; ++v) {
+                uint32_t sv = 0;
+                uint64_t gv = 0;
+                for (int b = 0; b < 5 && b + 4 < nb; ++b)
+                    if ((v >> b) & 1) {
+                        sv ^= tslot[b + 4];
+                        gv |= tglob[b + 4];
+                    }
+                ph.thi_slot[v] = sv;
+                ph.thi_glob[v] = gv;
+            }
             for (int j = 0; j < NREG; ++j) {
                 uint32_t s = 0;
-                uint64_t g = 0;
                 for (int k = 0; k < RQ; ++k)
-                    if ((j >> k) & 1) {
-                        s ^= pd.acol[rtb[k]];
-                        g |= 1ull << rq[k];
-                    }
+                    if ((j >> k) & 1) s ^= pd.acol[rtb[k]];
                 ph.rslot[j] = s;
-                ph.rglob[j] = g;
             }
             auto kbit = [&](int q) {
                 for (int k = 0; k < RQ; ++k)

@@ -73,12 +73,17 @@ struct KOp {
     uint64_t ridx;       // K_DIAG: 4-bit register part of the index for each slot j
 };
 
+// Thread bits of a phase: thread t's shared-memory base and global-index base
+// are XOR / OR of per-bit columns, tabulated for the low 4 and high 5 bits of t.
+constexpr int TLO = 16, THI = 32;
+
 struct PhaseDesc {
     int32_t op_begin, op_end;
     uint32_t rslot[NREG];      // shared-memory slot offset of register slot j
-    uint64_t rglob[NREG];      // global index offset of register slot j
-    uint32_t tslot[MAX_TILE];  // shared-memory slot column of thread bit b
-    int32_t tq[MAX_TILE];      // global qubit of thread bit b
+    uint32_t tlo_slot[TLO];    // slot base of thread bits 0..3
+    uint32_t thi_slot[THI];    // slot base of thread bits 4..8
+    uint64_t tlo_glob[TLO];    // global index base of thread bits 0..3
+    uint64_t thi_glob[THI];    // global index base of thread bits 4..8
 };
 
 struct PassDesc {
@@ -149,13 +154,13 @@ GQ_HD uint64_t pext64(uint64_t v, uint64_t mask) {
 
 // ---- register-level gate bodies (S* are register bits, compile-time) -------
 
-template <class T, int S>
+template <class T, int S, bool C>
 GQ_HD void k_u1(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
     const cplx<T> m0 = ldc(m, 0), m1 = ldc(m, 1), m2 = ldc(m, 2), m3 = ldc(m, 3);
 #pragma unroll
     for (int j = 0; j < NREG; ++j) {
         if (j & (1 << S)) continue;
-        if ((j & creg) != creg) continue;
+        if (C && (j & creg) != creg) continue;
         const cplx<T> a0 = a[j], a1 = a[j | (1 << S)];
         cplx<T> o0 = {T(0), T(0)}, o1 = {T(0), T(0)};
         o0 = cfma(m0, a0, o0);
@@ -167,12 +172,12 @@ GQ_HD void k_u1(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
     }
 }
 
-template <class T, int S0, int S1>
+template <class T, int S0, int S1, bool C>
 GQ_HD void k_u2(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
 #pragma unroll
     for (int j = 0; j < NREG; ++j) {
         if (j & ((1 << S0) | (1 << S1))) continue;
-        if ((j & creg) != creg) continue;
+        if (C && (j & creg) != creg) continue;
         const int idx[4] = {j, j | (1 << S0), j | (1 << S1), j | (1 << S0) | (1 << S1)};
         cplx<T> v[4];
 #pragma unroll
@@ -181,7 +186,7 @@ GQ_HD void k_u2(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
         for (int r = 0; r < 4; ++r) {
             cplx<T> o = {T(0), T(0)};
 #pragma unroll
-            for (int c = 0; c < 4; ++c) o = cfma(ldc(m, r * 4 + c), v[c], o);
+            for (int c = 0; c < 4; ++c) o = cfma(ldc_v(m, r * 4 + c), v[c], o);
             a[idx[r]] = o;
         }
     }
@@ -226,13 +231,13 @@ GQ_HD void k_u4(cplx<T> (&a)[NREG], const cplx<T>* m, cplx<T>* sm, uint32_t sbas
     for (int r = 0; r < NREG; ++r) a[r] = sm[sbase ^ rslot[r]];
 }
 
-template <class T, int S>
+template <class T, int S, bool C>
 GQ_HD void k_x(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg, bool pure) {
     if (pure) {
 #pragma unroll
         for (int j = 0; j < NREG; ++j) {
             if (j & (1 << S)) continue;
-            if ((j & creg) != creg) continue;
+            if (C && (j & creg) != creg) continue;
             const cplx<T> t = a[j];
             a[j] = a[j | (1 << S)];
             a[j | (1 << S)] = t;
@@ -243,7 +248,7 @@ GQ_HD void k_x(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg, bool pure) {
 #pragma unroll
     for (int j = 0; j < NREG; ++j) {
         if (j & (1 << S)) continue;
-        if ((j & creg) != creg) continue;
+        if (C && (j & creg) != creg) continue;
         const cplx<T> a0 = a[j], a1 = a[j | (1 << S)];
         a[j] = cmul(p0, a1);
         a[j | (1 << S)] = cmul(p1, a0);
@@ -317,21 +322,41 @@ GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint
     const uint32_t creg = op.creg;
     switch (op.type) {
         case K_U1:
-            switch (op.t0) {
-                case 0: k_u1<T, 0>(a, m, creg); break;
-                case 1: k_u1<T, 1>(a, m, creg); break;
-                case 2: k_u1<T, 2>(a, m, creg); break;
-                default: k_u1<T, 3>(a, m, creg); break;
+            if (creg == 0) {
+                switch (op.t0) {
+                    case 0: k_u1<T, 0, false>(a, m, 0); break;
+                    case 1: k_u1<T, 1, false>(a, m, 0); break;
+                    case 2: k_u1<T, 2, false>(a, m, 0); break;
+                    default: k_u1<T, 3, false>(a, m, 0); break;
+                }
+            } else {
+                switch (op.t0) {
+                    case 0: k_u1<T, 0, true>(a, m, creg); break;
+                    case 1: k_u1<T, 1, true>(a, m, creg); break;
+                    case 2: k_u1<T, 2, true>(a, m, creg); break;
+                    default: k_u1<T, 3, true>(a, m, creg); break;
+                }
             }
             break;
         case K_U2:
-            switch (op.t0 * 4 + op.t1) {
-                case 1: k_u2<T, 0, 1>(a, m, creg); break;
-                case 2: k_u2<T, 0, 2>(a, m, creg); break;
-                case 3: k_u2<T, 0, 3>(a, m, creg); break;
-                case 6: k_u2<T, 1, 2>(a, m, creg); break;
-                case 7: k_u2<T, 1, 3>(a, m, creg); break;
-                default: k_u2<T, 2, 3>(a, m, creg); break;
+            if (creg == 0) {
+                switch (op.t0 * 4 + op.t1) {
+                    case 1: k_u2<T, 0, 1, false>(a, m, 0); break;
+                    case 2: k_u2<T, 0, 2, false>(a, m, 0); break;
+                    case 3: k_u2<T, 0, 3, false>(a, m, 0); break;
+                    case 6: k_u2<T, 1, 2, false>(a, m, 0); break;
+                    case 7: k_u2<T, 1, 3, false>(a, m, 0); break;
+                    default: k_u2<T, 2, 3, false>(a, m, 0); break;
+                }
+            } else {
+                switch (op.t0 * 4 + op.t1) {
+                    case 1: k_u2<T, 0, 1, true>(a, m, creg); break;
+                    case 2: k_u2<T, 0, 2, true>(a, m, creg); break;
+                    case 3: k_u2<T, 0, 3, true>(a, m, creg); break;
+                    case 6: k_u2<T, 1, 2, true>(a, m, creg); break;
+                    case 7: k_u2<T, 1, 3, true>(a, m, creg); break;
+                    default: k_u2<T, 2, 3, true>(a, m, creg); break;
+                }
             }
             break;
         case K_U3:
@@ -347,11 +372,20 @@ GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint
             break;
         case K_X: {
             const bool pure = op.flags & 1;
-            switch (op.t0) {
-                case 0: k_x<T, 0>(a, m, creg, pure); break;
-                case 1: k_x<T, 1>(a, m, creg, pure); break;
-                case 2: k_x<T, 2>(a, m, creg, pure); break;
-                default: k_x<T, 3>(a, m, creg, pure); break;
+            if (creg == 0) {
+                switch (op.t0) {
+                    case 0: k_x<T, 0, false>(a, m, 0, pure); break;
+                    case 1: k_x<T, 1, false>(a, m, 0, pure); break;
+                    case 2: k_x<T, 2, false>(a, m, 0, pure); break;
+                    default: k_x<T, 3, false>(a, m, 0, pure); break;
+                }
+            } else {
+                switch (op.t0) {
+                    case 0: k_x<T, 0, true>(a, m, creg, pure); break;
+                    case 1: k_x<T, 1, true>(a, m, creg, pure); break;
+                    case 2: k_x<T, 2, true>(a, m, creg, pure); break;
+                    default: k_x<T, 3, true>(a, m, creg, pure); break;
+                }
             }
             break;
         }
@@ -410,18 +444,14 @@ GQ_HD void linear_slot(const PassDesc& p, uint32_t lin, uint64_t& goff, uint32_t
 // slots, so phases only need a barrier between them.
 template <class T>
 GQ_HD void run_phase(cplx<T>* sm, const PhaseDesc& ph, const KOp* ops, const cplx<T>* pool, uint32_t t,
-                     int thread_bits, uint64_t base) {
-    uint32_t sbase = 0;
-    uint64_t g0 = base;
-    for (int b = 0; b < thread_bits; ++b)
-        if ((t >> b) & 1u) {
-            sbase ^= ph.tslot[b];
-            g0 |= 1ull << ph.tq[b];
-        }
+                     uint64_t base) {
+    const uint32_t sbase = ph.tlo_slot[t & (TLO - 1)] ^ ph.thi_slot[(t >> 4) & (THI - 1)];
+    const uint64_t g0 = base | ph.tlo_glob[t & (TLO - 1)] | ph.thi_glob[(t >> 4) & (THI - 1)];
     cplx<T> a[NREG];
 #pragma unroll
     for (int j = 0; j < NREG; ++j) a[j] = sm[sbase ^ ph.rslot[j]];
-    for (int o = ph.op_begin; o < ph.op_end; ++o) apply_op<T>(a, ops[o], pool, g0, sm, sbase, ph.rslot);
+    const int ob = ph.op_begin, oe = ph.op_end;
+    for (int o = ob; o < oe; ++o) apply_op<T>(a, ops[o], pool, g0, sm, sbase, ph.rslot);
 #pragma unroll
     for (int j = 0; j < NREG; ++j) sm[sbase ^ ph.rslot[j]] = a[j];
 }

@@ -170,10 +170,11 @@ int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops,
 int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 
 /* Engine options (per handle). */
-#define GQ_OPT_TILE_QUBITS 1    /* qubits staged per CTA tile (4..12, default auto) */
+#define GQ_OPT_TILE_QUBITS 1    /* qubits staged per CTA tile (4..13, bounded by the variant) */
 #define GQ_OPT_PASS_BUDGET 2    /* FMA-per-amplitude budget of one pass (0 = auto) */
 #define GQ_OPT_LOW_QUBITS 3     /* lowest qubits always in a tile (coalescing)      */
 #define GQ_OPT_TIMING 4         /* 1: record CUDA events around every apply        */
+#define GQ_OPT_KERNEL_VARIANT 5 /* tile-pass launch shape (0..3); sets the tile size */
 int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
 
 /* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */
