@@ -47,6 +47,7 @@ GQ_OPT_PASS_BUDGET = 2
 GQ_OPT_LOW_QUBITS = 3
 GQ_OPT_TIMING = 4
 GQ_OPT_KERNEL_VARIANT = 5
+GQ_OPT_ADJOINT_SEGMENTS = 6
 
 _DBL_P = ctypes.POINTER(ctypes.c_double)
 

@@ -112,4 +112,79 @@ int gqx_emulate_dm(int nq, double* rho, const gq_op* ops, size_t n_ops, int tile
     return GQ_OK;
 }
 
+// Adjoint gradient on the host through the same reverse program and dual
+// tile code as the device: psi forward, lambda = sum_t Re(c_t) P_t psi, then
+// the reverse passes accumulating 2 Re <lambda| G |psi> per parameter.
+int gqx_emulate_adjoint(int nq, const gq_op* ops, size_t n_ops, const gq_pauli_term* terms, size_t n_terms,
+                        size_t n_params, int tile_qubits, int budget, double* grad_out, double* energy_out) {
+    const int nphys = nq < gq::RQ ? gq::RQ : nq;
+    std::vector<gq::NGate> fwd, rev;
+    std::vector<int> fo, ro;
+    int rc = gq::adjoint_gates(nq, ops, n_ops, n_params, fwd, rev, fo, ro, g_err);
+    if (rc != GQ_OK) return rc;
+    gq::SchedOptions opt;
+    if (tile_qubits > 0) opt.tile_qubits = tile_qubits;
+    if (budget > 0) opt.budget = budget;
+    gq::Program pf, pr;
+    gq::schedule(fwd, nphys, opt, pf);
+    gq::schedule(rev, nphys, opt, pr);
+    const uint64_t n = 1ull << nphys;
+    std::vector<gq::cplx<double>> psi(n, {0.0, 0.0}), lam(n, {0.0, 0.0});
+    psi[0] = {1.0, 0.0};
+    run_program<double>(psi, pf);
+    double energy = 0.0;
+    for (size_t t = 0; t < n_terms; ++t) {
+        const uint64_t x = terms[t].x_mask, z = terms[t].z_mask;
+        const int ny = __builtin_popcountll(x & z) & 3;
+        const double c = terms[t].coeff_re;
+        double wr = c, wi = 0;
+        if (ny == 1) wr = 0, wi = c;
+        if (ny == 2) wr = -c, wi = 0;
+        if (ny == 3) wr = 0, wi = -c;
+        for (uint64_t i = 0; i < (1ull << nq); ++i) {
+            const uint64_t j = i ^ x;
+            const double sg = (__builtin_popcountll(j & z) & 1) ? -1.0 : 1.0;
+            const gq::cplx<double> v = psi[j];
+            lam[i].x += sg * (wr * v.x - wi * v.y);
+            lam[i].y += sg * (wr * v.y + wi * v.x);
+        }
+    }
+    for (uint64_t i = 0; i < n; ++i) energy += psi[i].x * lam[i].x + psi[i].y * lam[i].y;
+    std::vector<double> grad(n_params, 0.0);
+    std::vector<gq::cplx<double>> pool(pr.pool.size());
+    for (size_t i = 0; i < pool.size(); ++i) pool[i] = {pr.pool[i].re, pr.pool[i].im};
+    for (size_t pi = 0; pi < pr.passes.size(); ++pi) {
+        const gq::PassDesc& pd = pr.passes[pi];
+        const int m = pd.m;
+        const uint32_t tpb = 1u << (m - gq::RQ);
+        std::vector<gq::cplx<double>> sa(1u << m), sb(1u << m);
+        std::vector<double> slots(gq::MAX_GRAD_SLOTS, 0.0);
+        for (uint64_t cta = 0; cta < (1ull << pd.n_outer); ++cta) {
+            const uint64_t base = gq::cta_base(pd, cta);
+            for (uint32_t lin = 0; lin < (1u << m); ++lin) {
+                uint64_t goff;
+                uint32_t slot;
+                gq::linear_slot(pd, lin, goff, slot);
+                sa[slot] = psi[base | goff];
+                sb[slot] = lam[base | goff];
+            }
+            for (int p = 0; p < pd.n_phases; ++p)
+                for (uint32_t t = 0; t < tpb; ++t)
+                    gq::run_phase_dual<double>(sa.data(), sb.data(), pr.phases[pd.phase0 + p], pr.ops.data(), pool.data(),
+                                               t, base, [&](uint32_t s, double v) { slots[s] += v; });
+            for (uint32_t lin = 0; lin < (1u << m); ++lin) {
+                uint64_t goff;
+                uint32_t slot;
+                gq::linear_slot(pd, lin, goff, slot);
+                psi[base | goff] = sa[slot];
+                lam[base | goff] = sb[slot];
+            }
+        }
+        for (size_t sl = 0; sl < pr.pass_params[pi].size(); ++sl) grad[pr.pass_params[pi][sl]] += 2.0 * slots[sl];
+    }
+    for (size_t i = 0; i < n_params; ++i) grad_out[i] = grad[i];
+    if (energy_out) *energy_out = energy;
+    return GQ_OK;
+}
+
 }  // extern "C"

@@ -118,6 +118,26 @@ const TileKernelF kTileF[kNumVariants] = {
     k_tile_pass<float, kVariantsC64[2].threads, kVariantsC64[2].min_blocks>,
     k_tile_pass<float, kVariantsC64[3].threads, kVariantsC64[3].min_blocks>};
 
+// Adjoint (two-state) pass: 128 threads (tiles of up to 2^11 amplitudes).
+using AdjKernelD = void (*)(cplx<double>*, cplx<double>*, const PassDesc*, const PhaseDesc*, const KOp*,
+                            const cplx<double>*, double*, int);
+using AdjKernelF = void (*)(cplx<float>*, cplx<float>*, const PassDesc*, const PhaseDesc*, const KOp*,
+                            const cplx<float>*, double*, int);
+constexpr int kAdjThreads = 128;
+const AdjKernelD kAdjD = k_adjoint_pass<double, kAdjThreads, 2>;
+const AdjKernelF kAdjF = k_adjoint_pass<float, kAdjThreads, 3>;
+template <class T>
+struct AdjTable;
+template <>
+struct AdjTable<double> {
+    static AdjKernelD get() { return kAdjD; }
+};
+template <>
+struct AdjTable<float> {
+    static AdjKernelF get() { return kAdjF; }
+};
+size_t adj_smem(size_t amp, int m) { return 2 * (amp << m) + (kAdjThreads / 32) * MAX_GRAD_SLOTS * sizeof(double); }
+
 template <class T>
 struct TileTable;
 template <>
@@ -147,6 +167,9 @@ int set_smem_attr() {
             err = cudaFuncSetAttribute(TileTable<T>::get(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(sizeof(cplx<T>) << m));
         }
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(AdjTable<T>::get(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)adj_smem(sizeof(cplx<T>), log2i(kAdjThreads) + RQ));
     });
     if (err != cudaSuccess) return fail(GQ_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
     return GQ_OK;
@@ -160,6 +183,8 @@ struct Engine {
     uint64_t n_amps = 0;
     cudaStream_t stream = nullptr;
     DevBuf state, prog, scratch, scratch2, aux;
+    DevBuf lam, ckpt, adj_partial, adj_grad;  // adjoint differentiation
+    int adj_segments = 0;                     // forward checkpoints (0: automatic)
     PinnedBuf staging, hostio;
     cudaEvent_t staged = nullptr, ev0 = nullptr, ev1 = nullptr, ev_pass0 = nullptr, ev_pass1 = nullptr;
     bool pass_timed = false;
@@ -203,6 +228,10 @@ struct Engine {
         scratch.release();
         scratch2.release();
         aux.release();
+        lam.release();
+        ckpt.release();
+        adj_partial.release();
+        adj_grad.release();
         staging.release();
         hostio.release();
         if (staged) cudaEventDestroy(staged);
@@ -281,6 +310,68 @@ struct Engine {
         stats.kernel_launches += (int64_t)pr.passes.size();
         stats.phases += (int64_t)pr.phases.size();
         return GQ_OK;
+    }
+
+    // Reverse sweep of an adjoint gradient: two-state tile passes, then the
+    // per-pass gradient reduction into adj_grad.
+    template <class T>
+    int run_adjoint_t(const Program& pr) {
+        if (pr.passes.empty()) return GQ_OK;
+        size_t nslot_total = 0;
+        for (const auto& v : pr.pass_params) nslot_total += v.size();
+        const size_t o_pass = 0;
+        const size_t o_phase = align16(o_pass + sizeof(PassDesc) * pr.passes.size());
+        const size_t o_ops = align16(o_phase + sizeof(PhaseDesc) * pr.phases.size());
+        const size_t o_pool = align16(o_ops + sizeof(KOp) * pr.ops.size());
+        const size_t o_slots = align16(o_pool + sizeof(cplx<T>) * std::max<size_t>(1, pr.pool.size()));
+        const size_t total = align16(o_slots + sizeof(int) * std::max<size_t>(1, nslot_total));
+        void* hp = nullptr;
+        GQ_TRY(stage(total, &hp));
+        char* h = (char*)hp;
+        std::memcpy(h + o_pass, pr.passes.data(), sizeof(PassDesc) * pr.passes.size());
+        std::memcpy(h + o_phase, pr.phases.data(), sizeof(PhaseDesc) * pr.phases.size());
+        if (!pr.ops.empty()) std::memcpy(h + o_ops, pr.ops.data(), sizeof(KOp) * pr.ops.size());
+        cplx<T>* pool = (cplx<T>*)(h + o_pool);
+        for (size_t i = 0; i < pr.pool.size(); ++i) pool[i] = {(T)pr.pool[i].re, (T)pr.pool[i].im};
+        int* slots = (int*)(h + o_slots);
+        size_t k = 0;
+        uint64_t max_part = 1;
+        for (size_t i = 0; i < pr.passes.size(); ++i) {
+            for (int v : pr.pass_params[i]) slots[k++] = v;
+            max_part = std::max<uint64_t>(max_part, (1ull << pr.passes[i].n_outer) * pr.pass_params[i].size());
+        }
+        GQ_TRY(upload(prog, total));
+        GQ_TRY(adj_partial.ensure(max_part * sizeof(double)));
+        char* d = (char*)prog.p;
+        size_t slot_off = 0;
+        for (size_t i = 0; i < pr.passes.size(); ++i) {
+            const PassDesc& pd = pr.passes[i];
+            const int nslots = (int)pr.pass_params[i].size();
+            const unsigned threads = 1u << (pd.m - RQ);
+            const unsigned grid = 1u << pd.n_outer;
+            AdjTable<T>::get()<<<grid, threads, adj_smem(sizeof(cplx<T>), pd.m), stream>>>(
+                (cplx<T>*)state.p, (cplx<T>*)lam.p, (const PassDesc*)(d + o_pass) + i, (const PhaseDesc*)(d + o_phase),
+                (const KOp*)(d + o_ops), (const cplx<T>*)(d + o_pool), (double*)adj_partial.p, nslots);
+            ++stats.kernel_launches;
+            if (nslots > 0) {
+                k_grad_reduce<<<1, 1024, 0, stream>>>((const double*)adj_partial.p, grid, nslots,
+                                                      (const int*)(d + o_slots) + slot_off, (double*)adj_grad.p);
+                ++stats.kernel_launches;
+            }
+            slot_off += nslots;
+        }
+        GQ_CUDA(cudaGetLastError());
+        stats.passes += (int64_t)pr.passes.size();
+        stats.phases += (int64_t)pr.phases.size();
+        return GQ_OK;
+    }
+
+    int run_adjoint(const std::vector<NGate>& gates) {
+        SchedOptions o = opt;
+        o.tile_qubits = std::min(o.tile_qubits, log2i(kAdjThreads) + RQ);
+        Program pr;
+        schedule(gates, nphys, o, pr);
+        return prec == GQ_C64 ? run_adjoint_t<float>(pr) : run_adjoint_t<double>(pr);
     }
 
     int run_gates(const std::vector<NGate>& gates) {
@@ -620,13 +711,95 @@ int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
             e.variant = (int)value;
             e.opt.tile_qubits = e.max_tile();
             return GQ_OK;
+        case GQ_OPT_ADJOINT_SEGMENTS:
+            if (value < 0 || value > 4096) return fail(GQ_EINVAL, "adjoint segments out of range [0, 4096]");
+            e.adj_segments = (int)value;
+            return GQ_OK;
         default:
             return fail(GQ_EINVAL, "unknown option");
     }
 }
 
-int gq_sv_adjoint_gradient(gq_sv*, const gq_op*, size_t, const gq_pauli_term*, size_t, size_t, double*, double*) {
-    return fail(GQ_EUNSUPPORTED, "adjoint gradient not built yet");
+int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_pauli_term* terms, size_t n_terms,
+                           size_t n_params, double* grad_out, double* energy_out) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    if ((n_ops && !ops) || (n_terms && !terms) || (n_params && !grad_out)) return fail(GQ_EINVAL, "null argument");
+    Engine& e = sv->e;
+    std::vector<NGate> fwd, rev;
+    std::vector<int> fo, ro;
+    {
+        std::string err;
+        int rc = adjoint_gates(sv->nq, ops, n_ops, n_params, fwd, rev, fo, ro, err);
+        if (rc != GQ_OK) return fail(rc, err);
+    }
+    e.clear_stats();
+    GQ_TRY(e.time_begin());
+    const size_t sbytes = e.n_amps * e.amp_bytes();
+    GQ_TRY(e.lam.ensure(sbytes));
+    GQ_TRY(e.adj_grad.ensure(std::max<size_t>(1, n_params) * sizeof(double)));
+    // Forward segments (checkpoints bound the drift of un-applying gates).
+    int segs = e.adj_segments;
+    if (segs <= 0) segs = (e.prec == GQ_C64 && n_ops > 256) ? (int)std::min<size_t>(8, n_ops / 128) : 1;
+    segs = std::max(1, std::min<int>(segs, (int)std::max<size_t>(1, n_ops)));
+    std::vector<size_t> bound(segs + 1);
+    for (int j = 0; j <= segs; ++j) bound[j] = n_ops * (size_t)j / (size_t)segs;
+    if (segs > 1) GQ_TRY(e.ckpt.ensure(sbytes * (segs - 1)));
+    auto seg_of = [&](int op_index) {
+        int j = 0;
+        while (j + 1 < segs && (size_t)op_index >= bound[j + 1]) ++j;
+        return j;
+    };
+    GQ_TRY(e.reset_basis(0));
+    for (int j = 0; j < segs; ++j) {
+        std::vector<NGate> part;
+        for (size_t k = 0; k < fwd.size(); ++k)
+            if (seg_of(fo[k]) == j) part.push_back(fwd[k]);
+        GQ_TRY(e.run_gates(part));
+        if (j + 1 < segs)
+            GQ_CUDA(cudaMemcpyAsync((char*)e.ckpt.p + sbytes * j, e.state.p, sbytes, cudaMemcpyDeviceToDevice, e.stream));
+    }
+    // lambda = Re(H) psi and the energy
+    std::vector<gq_pauli_term> rt(terms, terms + n_terms);
+    for (auto& t : rt) t.coeff_im = 0.0;
+    int ng = 0;
+    size_t ot = 0;
+    GQ_TRY(e.upload_terms(rt.data(), rt.size(), (1ull << sv->nq) - 1, &ng, &ot));
+    const int nb = e.reduce_grid();
+    GQ_TRY(e.scratch.ensure((nb + 1) * sizeof(double2)));
+    {
+        const char* d = (const char*)e.scratch2.p;
+        const uint64_t na = 1ull << sv->nq;
+        if (sv->nq < RQ) GQ_CUDA(cudaMemsetAsync(e.lam.p, 0, sbytes, e.stream));
+        if (e.prec == GQ_C64)
+            k_apply_terms<float><<<nb, 256, 0, e.stream>>>((const cplx<float>*)e.state.p, (cplx<float>*)e.lam.p, na,
+                                                           (const DGroup*)d, ng, (const DTerm*)(d + ot),
+                                                           (double2*)e.scratch.p);
+        else
+            k_apply_terms<double><<<nb, 256, 0, e.stream>>>((const cplx<double>*)e.state.p, (cplx<double>*)e.lam.p,
+                                                            na, (const DGroup*)d, ng, (const DTerm*)(d + ot),
+                                                            (double2*)e.scratch.p);
+        GQ_CUDA(cudaGetLastError());
+        double en = 0.0;
+        GQ_TRY(e.finish_reduce(nb, &en, nullptr));
+        if (energy_out) *energy_out = en;
+        ++e.stats.kernel_launches;
+    }
+    // reverse sweep
+    GQ_CUDA(cudaMemsetAsync(e.adj_grad.p, 0, std::max<size_t>(1, n_params) * sizeof(double), e.stream));
+    for (int j = segs - 1; j >= 0; --j) {
+        if (j + 1 < segs)
+            GQ_CUDA(cudaMemcpyAsync(e.state.p, (char*)e.ckpt.p + sbytes * j, sbytes, cudaMemcpyDeviceToDevice, e.stream));
+        std::vector<NGate> part;
+        for (size_t k = 0; k < rev.size(); ++k)
+            if (seg_of(ro[k]) == j) part.push_back(rev[k]);
+        GQ_TRY(e.run_adjoint(part));
+    }
+    if (n_params) {
+        GQ_CUDA(cudaMemcpyAsync(grad_out, e.adj_grad.p, n_params * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        e.stats.d2h_bytes += (int64_t)(n_params * sizeof(double));
+    }
+    GQ_CUDA(cudaStreamSynchronize(e.stream));
+    return e.time_end();
 }
 
 // ---- density matrix -----------------------------------------------------------

@@ -102,6 +102,93 @@ __global__ void __launch_bounds__(THREADS, MINB)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint reverse pass: the tile pass on two states (psi, lambda) at once,
+// with gradient ops. Each warp writes its sum for every gradient slot once
+// per pass into shared memory; the CTA's per-slot totals go to
+// partial[cta * nslots + slot] (summed per slot by k_grad_reduce).
+template <class T, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_adjoint_pass(cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam, const PassDesc* __restrict__ pdp,
+                   const PhaseDesc* __restrict__ phases, const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool,
+                   double* __restrict__ partial, int nslots) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const PassDesc& pd = *pdp;
+    const int m = pd.m;
+    const int tbits = m - RQ;
+    cplx<T>* sa = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* sb = sa + (1u << m);
+    double* gsm = reinterpret_cast<double*>(sb + (1u << m));  // [warps][MAX_GRAD_SLOTS]
+    const uint32_t t = threadIdx.x;
+    const uint64_t base = cta_base(pd, blockIdx.x);
+    uint64_t gt = 0;
+    uint32_t stt = 0;
+    for (int b = 0; b < tbits; ++b)
+        if ((t >> b) & 1u) {
+            gt |= 1ull << pd.tile_q[b];
+            stt ^= pd.acol[b];
+        }
+    for (int it = 0; it < NREG; ++it) {
+        uint64_t g = base | gt;
+        uint32_t s = stt;
+        for (int k = 0; k < RQ; ++k)
+            if ((it >> k) & 1) {
+                g |= 1ull << pd.tile_q[tbits + k];
+                s ^= pd.acol[tbits + k];
+            }
+        sa[s] = psi[g];
+        sb[s] = lam[g];
+    }
+    __syncthreads();
+    const int warp = t >> 5, lane = t & 31;
+    auto grad = [&](uint32_t slot, double v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) gsm[warp * MAX_GRAD_SLOTS + slot] = v;
+    };
+    for (int p = 0; p < pd.n_phases; ++p) {
+        run_phase_dual<T>(sa, sb, phases[pd.phase0 + p], ops, pool, t, base, grad);
+        __syncthreads();
+    }
+    for (int it = 0; it < NREG; ++it) {
+        uint64_t g = base | gt;
+        uint32_t s = stt;
+        for (int k = 0; k < RQ; ++k)
+            if ((it >> k) & 1) {
+                g |= 1ull << pd.tile_q[tbits + k];
+                s ^= pd.acol[tbits + k];
+            }
+        psi[g] = sa[s];
+        lam[g] = sb[s];
+    }
+    if ((int)t < nslots) {
+        double acc = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += gsm[w * MAX_GRAD_SLOTS + t];
+        partial[(uint64_t)blockIdx.x * nslots + t] = acc;
+    }
+}
+
+// grad[slot_param[s]] += 2 * sum over CTAs of partial[cta][s], slots in order
+// (single CTA of 1024 threads: deterministic).
+__global__ void k_grad_reduce(const double* __restrict__ partial, uint64_t nctas, int nslots,
+                              const int* __restrict__ slot_param, double* __restrict__ grad) {
+    __shared__ double red[32];
+    for (int s = 0; s < nslots; ++s) {
+        double v = 0.0;
+        for (uint64_t c = threadIdx.x; c < nctas; c += blockDim.x) v += partial[c * nslots + s];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (unsigned w = 0; w < (blockDim.x >> 5); ++w) tot += red[w];
+            grad[slot_param[s]] += 2.0 * tot;
+        }
+        __syncthreads();
+    }
+}
+
 template <class T>
 __global__ void k_set_amp(cplx<T>* st, uint64_t idx, T re, T im) {
     st[idx] = {re, im};
@@ -533,6 +620,36 @@ __global__ void k_final_reduce(const double2* __restrict__ partial, int n, doubl
         im = warp_sum(im);
         if (l == 0) *out = make_double2(re, im);
     }
+}
+
+// lambda = sum_t Re(c_t) P_t psi, with (P psi)_i = i^nY (-1)^popcount((i^x)&z)
+// psi[i^x]; also accumulates Re <psi|lambda> = E into partial (per block).
+template <class T>
+__global__ void k_apply_terms(const cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam, uint64_t n,
+                              const DGroup* __restrict__ groups, int ngroups, const DTerm* __restrict__ terms,
+                              double2* __restrict__ partial) {
+    double e = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        double lr = 0.0, li = 0.0;
+        for (int g = 0; g < ngroups; ++g) {
+            const DGroup gr = groups[g];
+            const uint64_t j = i ^ gr.x;
+            const cplx<T> v = psi[j];
+            double fr = 0.0, fi = 0.0;
+            for (int k = gr.t0; k < gr.t1; ++k) {
+                const DTerm tm = terms[k];
+                const double sg = (__popcll(j & tm.z) & 1) ? -1.0 : 1.0;
+                fr += sg * tm.wre;
+                fi += sg * tm.wim;
+            }
+            lr += fr * (double)v.x - fi * (double)v.y;
+            li += fr * (double)v.y + fi * (double)v.x;
+        }
+        lam[i] = {(T)lr, (T)li};
+        const cplx<T> a = psi[i];
+        e += (double)a.x * lr + (double)a.y * li;
+    }
+    block_reduce_store(e, 0.0, partial);
 }
 
 }  // namespace gq

@@ -47,6 +47,7 @@ std::vector<Z> restrict_to_one(const std::vector<Z>& m, int k, int p) {
 
 int cost_of(KType t) {
     switch (t) {
+        case K_GRAD: return 16;
         case K_U1: return 8;
         case K_U2: return 16;
         case K_U3: return 32;
@@ -65,12 +66,13 @@ constexpr uint64_t kGlobalBit = 1ull << 63;
 void finish(NGate& g) {
     g.nd_mask = 0;
     g.d_mask = g.ctrl | kGlobalBit;
-    if (g.type == K_DIAG) {
+    const KType kind = g.type == K_GRAD ? g.grad_kind : g.type;
+    if (kind == K_DIAG) {
         for (int q : g.targets) g.d_mask |= 1ull << q;
-    } else if (g.type != K_PHASE) {
+    } else if (kind != K_PHASE) {
         for (int q : g.targets) g.nd_mask |= 1ull << q;
     }
-    g.cost = cost_of(g.type);
+    g.cost = cost_of(kind) + (g.type == K_GRAD ? cost_of(K_GRAD) : 0);
 }
 
 }  // namespace
@@ -306,15 +308,17 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
         {
             std::vector<int> take, rest;
             uint64_t T = low_mask, bnd = 0, bd = 0;
-            int used = 0;
+            int used = 0, ngrad = 0;
             for (size_t i = 0; i < remaining.size(); ++i) {
                 const NGate& g = gates[remaining[i]];
                 const bool free =
                     !(g.nd_mask & (bnd | bd)) && !(g.d_mask & bnd) && (!g.barrier || (bnd | bd) == 0);
                 const uint64_t nt = T | g.nd_mask;
-                if (free && popc(nt) <= m && (used + g.cost <= opt.budget || take.empty())) {
+                const bool grad_ok = g.type != K_GRAD || ngrad < MAX_GRAD_SLOTS;
+                if (free && grad_ok && popc(nt) <= m && (used + g.cost <= opt.budget || take.empty())) {
                     T = nt;
                     used += g.cost;
+                    ngrad += g.type == K_GRAD;
                     take.push_back(remaining[i]);
                     continue;
                 }
@@ -400,6 +404,7 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
         }
         for (int b = 0; b < m; ++b) pd.acol[b] = (1u << b) ^ S[b];
 
+        std::vector<int> slot_params;
         for (size_t p = 0; p < groups.size(); ++p) {
             PhaseDesc ph;
             std::memset(&ph, 0, sizeof(ph));
@@ -459,12 +464,17 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                 KOp op;
                 std::memset(&op, 0, sizeof(op));
                 op.type = g.type;
+                const KType kind = g.type == K_GRAD ? g.grad_kind : g.type;
+                if (g.type == K_GRAD) {
+                    op.slot = (uint32_t)slot_params.size();
+                    slot_params.push_back(g.param);
+                }
                 for (int k = 0; k < RQ; ++k)
                     if (g.ctrl & (1ull << rq[k])) op.creg |= (uint8_t)(1u << k);
                 op.cmask = g.ctrl & ~R;
                 op.mat = (uint32_t)prog.pool.size();
                 const int t = (int)g.targets.size();
-                if (g.type >= K_U1 && g.type <= K_U4) {
+                if (kind >= K_U1 && kind <= K_U4) {
                     // order[p] = target index whose register bit is the p-th smallest
                     std::vector<int> order(t);
                     for (int i = 0; i < t; ++i) order[i] = i;
@@ -484,17 +494,17 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                     };
                     for (int r = 0; r < dim; ++r)
                         for (int c = 0; c < dim; ++c) prog.pool.push_back(g.data[mapidx(r) * dim + mapidx(c)]);
-                } else if (g.type == K_X || g.type == K_RESET) {
+                } else if (kind == K_X || kind == K_RESET) {
                     op.t0 = (uint8_t)kbit(g.targets[0]);
                     op.flags = g.pure ? 1 : 0;
                     prog.pool.insert(prog.pool.end(), g.data.begin(), g.data.end());
-                } else if (g.type == K_SWAP) {
+                } else if (kind == K_SWAP) {
                     int a = kbit(g.targets[0]), b = kbit(g.targets[1]);
                     op.t0 = (uint8_t)std::min(a, b);
                     op.t1 = (uint8_t)std::max(a, b);
-                } else if (g.type == K_PHASE) {
+                } else if (kind == K_PHASE) {
                     prog.pool.push_back(g.data[0]);
-                } else if (g.type == K_DIAG) {
+                } else if (kind == K_DIAG) {
                     // Index layout: register targets (ascending register bit)
                     // in the low bits, the others (ascending qubit) above.
                     std::vector<int> reg_t, oth_t;  // target positions
@@ -520,6 +530,7 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                         op.ridx |= ri << (4 * j);
                     }
                 }
+                if (g.type == K_GRAD) op.flags = (uint8_t)kind;
                 prog.ops.push_back(op);
             }
             ph.op_end = (int32_t)prog.ops.size();
@@ -527,6 +538,7 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
         }
         (void)tb_of;
         prog.passes.push_back(pd);
+        prog.pass_params.push_back(slot_params);
     }
 }
 
@@ -652,5 +664,141 @@ int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, 
     return GQ_OK;
 }
 
+
+// ---- adjoint differentiation ---------------------------------------------
+namespace {
+
+std::vector<Z> dagger(const std::vector<Z>& m, int dim) {
+    std::vector<Z> o(dim * dim);
+    for (int r = 0; r < dim; ++r)
+        for (int c = 0; c < dim; ++c) o[r * dim + c] = Z{m[c * dim + r].re, -m[c * dim + r].im};
+    return o;
+}
+
+std::vector<Z> mul(const std::vector<Z>& a, const std::vector<Z>& b, int dim) {
+    std::vector<Z> c(dim * dim, Z{0, 0});
+    for (int i = 0; i < dim; ++i)
+        for (int k = 0; k < dim; ++k) {
+            const Z x = a[i * dim + k];
+            for (int j = 0; j < dim; ++j) {
+                const Z y = b[k * dim + j];
+                c[i * dim + j].re += x.re * y.re - x.im * y.im;
+                c[i * dim + j].im += x.re * y.im + x.im * y.re;
+            }
+        }
+    return c;
+}
+
+bool zero_control(const std::vector<Z>& m, int k, int p) {
+    const int dim = 1 << k, bit = 1 << (k - 1 - p);
+    for (int r = 0; r < dim; ++r)
+        for (int c = 0; c < dim; ++c) {
+            if ((r & bit) && (c & bit)) continue;
+            const Z v = m[r * dim + c];
+            if (v.re != 0.0 || v.im != 0.0) return false;
+        }
+    return true;
+}
+
+// G as a K_GRAD gate: qubits on whose |0> rows and columns G vanishes become
+// controls; the rest is a phase, a diagonal or a dense matrix on <= 4 qubits.
+int grad_gate(std::vector<Z> m, std::vector<int> qubits, uint64_t ctrl, int param, std::vector<NGate>& out,
+              std::string& err) {
+    for (bool found = true; found && !qubits.empty();) {
+        found = false;
+        const int k = (int)qubits.size();
+        for (int p = 0; p < k; ++p)
+            if (zero_control(m, k, p)) {
+                ctrl |= 1ull << qubits[p];
+                m = restrict_to_one(m, k, p);
+                qubits.erase(qubits.begin() + p);
+                found = true;
+                break;
+            }
+    }
+    const int t = (int)qubits.size(), dim = 1 << t;
+    NGate g;
+    g.type = K_GRAD;
+    g.param = param;
+    g.ctrl = ctrl;
+    g.targets = qubits;
+    bool diag = true;
+    for (int r = 0; r < dim && diag; ++r)
+        for (int c = 0; c < dim; ++c)
+            if (r != c && (m[r * dim + c].re != 0.0 || m[r * dim + c].im != 0.0)) {
+                diag = false;
+                break;
+            }
+    if (t == 0) {
+        g.grad_kind = K_PHASE;
+        g.data = {m[0]};
+    } else if (diag) {
+        g.grad_kind = K_DIAG;
+        g.data.resize(dim);
+        for (int i = 0; i < dim; ++i) g.data[i] = m[i * dim + i];
+    } else if (t <= RQ) {
+        g.grad_kind = (KType)(K_U1 + (t - 1));
+        g.data = m;
+    } else {
+        err = "derivative acts densely on more than 4 qubits";
+        return GQ_EUNSUPPORTED;
+    }
+    finish(g);
+    out.push_back(g);
+    return GQ_OK;
+}
+
+}  // namespace
+
+int adjoint_gates(int nq, const gq_op* ops, size_t n_ops, size_t n_params, std::vector<NGate>& forward,
+                  std::vector<NGate>& reverse, std::vector<int>& fwd_op, std::vector<int>& rev_op, std::string& err) {
+    for (size_t i = 0; i < n_ops; ++i) {
+        const size_t before = forward.size();
+        const gq_op& op = ops[i];
+        if (op.kind == GQ_OP_RESET || op.kind == GQ_OP_CHANNEL) {
+            err = "op " + std::to_string(i) + ": adjoint differentiation needs a unitary circuit";
+            return GQ_EUNSUPPORTED;
+        }
+        int rc = normalize_op(op, nq, forward, err);
+        if (rc != GQ_OK) {
+            err = "op " + std::to_string(i) + ": " + err;
+            return rc;
+        }
+        for (size_t k = before; k < forward.size(); ++k) fwd_op.push_back((int)i);
+    }
+    for (size_t ii = n_ops; ii-- > 0;) {
+        const gq_op& op = ops[ii];
+        if (op.kind == GQ_OP_BARRIER) continue;
+        const int nc = op.kind == GQ_OP_CONTROLLED ? op.num_controls : 0;
+        const int k = op.num_qubits - nc, dim = 1 << k;
+        uint64_t ctrl = 0;
+        for (int c = 0; c < nc; ++c) ctrl |= 1ull << op.qubits[c];
+        std::vector<int> qs(op.qubits + nc, op.qubits + op.num_qubits);
+        std::vector<Z> u((const Z*)op.matrix, (const Z*)op.matrix + dim * dim);
+        const std::vector<Z> ud = dagger(u, dim);
+        const size_t before = reverse.size();
+        for (int p = 0; p < GQ_MAX_OP_PARAMS; ++p) {
+            const int pi = op.param_index[p];
+            if (pi < 0) continue;
+            if ((size_t)pi >= n_params || !op.dmatrix[p]) {
+                err = "op " + std::to_string(ii) + ": parameter index out of range or missing derivative";
+                return GQ_EINVAL;
+            }
+            std::vector<Z> du((const Z*)op.dmatrix[p], (const Z*)op.dmatrix[p] + dim * dim);
+            int rc = grad_gate(mul(du, ud, dim), qs, ctrl, pi, reverse, err);
+            if (rc != GQ_OK) {
+                err = "op " + std::to_string(ii) + ": " + err;
+                return rc;
+            }
+        }
+        int rc = analyze_matrix(ud, qs, ctrl, (int)ii, reverse, err);
+        if (rc != GQ_OK) {
+            err = "op " + std::to_string(ii) + ": " + err;
+            return rc;
+        }
+        for (size_t kk = before; kk < reverse.size(); ++kk) rev_op.push_back((int)ii);
+    }
+    return GQ_OK;
+}
 
 }  // namespace gq

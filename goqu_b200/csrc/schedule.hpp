@@ -33,6 +33,8 @@ struct NGate {
     uint64_t nd_mask = 0;      // qubits acted on non-diagonally (must be in registers)
     uint64_t d_mask = 0;       // qubits acted on diagonally (controls, diagonal targets)
     bool barrier = false;      // reset: nonlinear, commutes with nothing
+    KType grad_kind = K_NONE;  // K_GRAD: structure of G (dense K_U*, K_DIAG or K_PHASE)
+    int param = -1;            // K_GRAD: circuit parameter the slot accumulates into
     int cost = 0;              // FMA per amplitude, for the pass budget
     int src = -1;              // index of the gq_op it came from
 };
@@ -51,6 +53,7 @@ struct Program {
     std::vector<Z> pool;
     int64_t gates = 0;
     int64_t conflict_phases = 0;  // phases whose lane groups could not be made conflict free
+    std::vector<std::vector<int>> pass_params;  // K_GRAD: parameter of each slot, per pass
 };
 
 // Appends the NGates of one op (0 when it is an identity or a barrier).
@@ -66,5 +69,12 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
 // channels as sum_k E_k (x) conj(E_k), a gate and the channel that follows it
 // on the same qubits folded into one superoperator.
 int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, std::string& err);
+// Adjoint differentiation: `forward` are the gates of `ops`; `reverse` is the
+// reverse sweep: for each op from last to first, one K_GRAD gate per
+// parameter it depends on (G = dU/dtheta * U^dagger, zero where its controls
+// are unset), then the inverse of the op. Ops must be unitary. `seg_ends`
+// receives, per forward gate, the op index it came from (for checkpoints).
+int adjoint_gates(int nq, const gq_op* ops, size_t n_ops, size_t n_params, std::vector<NGate>& forward,
+                  std::vector<NGate>& reverse, std::vector<int>& fwd_op, std::vector<int>& rev_op, std::string& err);
 
 }  // namespace gq

@@ -56,7 +56,11 @@ enum KType : uint8_t {
     K_DIAG = 7,  // diagonal factor d[index]; index = pext(g, dmask) << nreg | ridx[j]
     K_PHASE = 8, // scalar factor when all controls are set
     K_RESET = 9, // deterministic reset of register bit t0 (sim/statevector/sim.go:168-186)
+    K_GRAD = 10, // adjoint: Re <lambda| G |psi> into gradient slot `slot`; flags = the
+                 // structure of G (K_U1..K_U4 dense on t0.., K_DIAG, K_PHASE)
 };
+
+constexpr int MAX_GRAD_SLOTS = 64;  // gradient ops per pass
 
 // One op as placed in a phase (40 bytes).
 struct KOp {
@@ -67,7 +71,7 @@ struct KOp {
     uint8_t flags;
     uint8_t pad;
     uint32_t mat;        // offset into the complex pool
-    uint32_t pad2;
+    uint32_t slot;       // K_GRAD: gradient slot of the pass
     uint64_t cmask;      // controls outside the registers (global mask)
     uint64_t dmask;      // K_DIAG: diagonal qubits outside the registers (global mask)
     uint64_t ridx;       // K_DIAG: 4-bit register part of the index for each slot j
@@ -454,6 +458,110 @@ GQ_HD void run_phase(cplx<T>* sm, const PhaseDesc& ph, const KOp* ops, const cpl
     for (int o = ob; o < oe; ++o) apply_op<T>(a, ops[o], pool, g0, sm, sbase, ph.rslot);
 #pragma unroll
     for (int j = 0; j < NREG; ++j) sm[sbase ^ ph.rslot[j]] = a[j];
+}
+
+// ---- adjoint differentiation ----------------------------------------------
+
+template <class T>
+GQ_HD double cdot_re(cplx<T> b, cplx<T> v) {  // Re(conj(b) * v) in FP64
+    return (double)b.x * (double)v.x + (double)b.y * (double)v.y;
+}
+
+// Re sum_j conj(lambda_j) (G psi)_j over the thread's amplitudes, G being the
+// op's matrix restricted to the amplitudes whose controls are set (zero
+// elsewhere). a = psi, b = lambda; neither is modified.
+template <class T>
+GQ_HD double grad_partial(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const KOp& op, const cplx<T>* pool,
+                          uint64_t g0) {
+    if ((g0 & op.cmask) != op.cmask) return 0.0;
+    const cplx<T>* m = pool + op.mat;
+    const uint32_t creg = op.creg;
+    double acc = 0.0;
+    switch (op.flags) {
+        case K_PHASE: {
+            const cplx<T> sc = ldc(m, 0);
+#pragma unroll
+            for (int j = 0; j < NREG; ++j)
+                if ((j & creg) == creg) acc += cdot_re(b[j], cmul(sc, a[j]));
+            return acc;
+        }
+        case K_DIAG: {
+            const uint32_t hi = (uint32_t)(pext64(g0, op.dmask) << op.nreg);
+#pragma unroll
+            for (int j = 0; j < NREG; ++j) {
+                if ((j & creg) != creg) continue;
+                const uint32_t idx = hi | (uint32_t)((op.ridx >> (4 * j)) & 15u);
+                acc += cdot_re(b[j], cmul(ldc(m, idx), a[j]));
+            }
+            return acc;
+        }
+        default: {
+            // dense G on the target register bits: apply it to a copy of psi
+            // (the amplitudes whose controls are unset keep psi's values and
+            // are excluded from the sum)
+            return 0.0;
+        }
+    }
+}
+
+template <class T>
+GQ_HD double grad_partial_dense(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const KOp& op,
+                                const cplx<T>* pool, uint64_t g0, cplx<T>* sm, uint32_t sbase, const uint32_t* rslot) {
+    if ((g0 & op.cmask) != op.cmask) return 0.0;
+    KOp d = op;
+    d.type = op.flags;
+    d.cmask = 0;
+    cplx<T> v[NREG];
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) v[j] = a[j];
+    apply_op<T>(v, d, pool, g0, sm, sbase, rslot);
+    double acc = 0.0;
+    const uint32_t creg = op.creg;
+#pragma unroll
+    for (int j = 0; j < NREG; ++j)
+        if ((j & creg) == creg) acc += cdot_re(b[j], v[j]);
+    return acc;
+}
+
+template <class T>
+GQ_HD void load_regs(cplx<T> (&a)[NREG], const cplx<T>* sm, uint32_t sbase, const uint32_t* rslot) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) a[j] = sm[sbase ^ rslot[j]];
+}
+template <class T>
+GQ_HD void store_regs(const cplx<T> (&a)[NREG], cplx<T>* sm, uint32_t sbase, const uint32_t* rslot) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) sm[sbase ^ rslot[j]] = a[j];
+}
+
+// One thread's work in one phase of an adjoint (reverse) pass: the same ops
+// are applied to psi (tile sm_a) and lambda (tile sm_b); gradient ops return
+// their partial sums through `grad(slot, value)`.
+template <class T, class Grad>
+GQ_HD void run_phase_dual(cplx<T>* sm_a, cplx<T>* sm_b, const PhaseDesc& ph, const KOp* ops, const cplx<T>* pool,
+                          uint32_t t, uint64_t base, Grad grad) {
+    const uint32_t sbase = ph.tlo_slot[t & (TLO - 1)] ^ ph.thi_slot[(t >> 4) & (THI - 1)];
+    const uint64_t g0 = base | ph.tlo_glob[t & (TLO - 1)] | ph.thi_glob[(t >> 4) & (THI - 1)];
+    cplx<T> a[NREG], b[NREG];
+    load_regs(a, sm_a, sbase, ph.rslot);
+    load_regs(b, sm_b, sbase, ph.rslot);
+    const int ob = ph.op_begin, oe = ph.op_end;
+    for (int o = ob; o < oe; ++o) {
+        const KOp& op = ops[o];
+        if (op.type == K_GRAD) {
+            const double v = (op.flags == K_PHASE || op.flags == K_DIAG)
+                                 ? grad_partial<T>(a, b, op, pool, g0)
+                                 : grad_partial_dense<T>(a, b, op, pool, g0, sm_a, sbase, ph.rslot);
+            grad(op.slot, v);
+            continue;
+        }
+        // U4 spills through the thread's own slots: keep the two states'
+        // slots apart by applying to psi and lambda with their own tiles.
+        apply_op<T>(a, op, pool, g0, sm_a, sbase, ph.rslot);
+        apply_op<T>(b, op, pool, g0, sm_b, sbase, ph.rslot);
+    }
+    store_regs(a, sm_a, sbase, ph.rslot);
+    store_regs(b, sm_b, sbase, ph.rslot);
 }
 
 }  // namespace gq

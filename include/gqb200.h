@@ -175,6 +175,7 @@ int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 #define GQ_OPT_LOW_QUBITS 3     /* lowest qubits always in a tile (coalescing)      */
 #define GQ_OPT_TIMING 4         /* 1: record CUDA events around every apply        */
 #define GQ_OPT_KERNEL_VARIANT 5 /* tile-pass launch shape (0..3); sets the tile size */
+#define GQ_OPT_ADJOINT_SEGMENTS 6 /* adjoint: forward checkpoints (0 = automatic, 1 = none) */
 int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
 
 /* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */

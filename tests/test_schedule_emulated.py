@@ -121,3 +121,77 @@ def test_emulated_noisy_brickwork(emu):
     c, nm = workloads.noisy_brickwork(5, layers=4, seed=1)
     ops = encode.density_ops(c, nm)
     np.testing.assert_allclose(_emu_dm(emu, ops), orc.dm_evolve(ops), atol=1e-12, rtol=0)
+
+
+def _emu_adjoint(emu, circuit, names, x, h, tile=0, budget=0):
+    from goqu_b200 import pauli as P
+    bindings = {nm: float(x[i]) for i, nm in enumerate(names)}
+    stream = encode.statevector_ops(circuit, bindings, names)
+    terms = P.to_terms(h)
+    grad = np.zeros(len(names))
+    energy = ctypes.c_double()
+    emu.gqx_emulate_adjoint.restype = ctypes.c_int
+    emu.gqx_emulate_adjoint.argtypes = [ctypes.c_int, ctypes.POINTER(_abi.gq_op), ctypes.c_size_t,
+                                        ctypes.POINTER(_abi.gq_pauli_term), ctypes.c_size_t, ctypes.c_size_t,
+                                        ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_double)]
+    rc = emu.gqx_emulate_adjoint(circuit.NumQubits(), stream.ptr(), len(stream),
+                                 ctypes.cast(terms, ctypes.POINTER(_abi.gq_pauli_term)), len(terms), len(names),
+                                 tile, budget, grad.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                 ctypes.byref(energy))
+    assert rc == 0, emu.gqx_last_error()
+    return energy.value, grad
+
+
+def _oracle_energy(circuit, names, x, h):
+    from goqu_b200 import circuit as ir, pauli as P
+    bound = ir.Bind(circuit, {nm: float(x[i]) for i, nm in enumerate(names)})
+    st = orc.sv_evolve(encode.statevector_ops(bound))
+    return orc.expect_pauli_sum(st, P.to_terms(h)).real
+
+
+def _oracle_param_shift(circuit, names, x, h):
+    import math
+    g = np.zeros(len(names))
+    for i in range(len(names)):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += math.pi / 2
+        xm[i] -= math.pi / 2
+        g[i] = (_oracle_energy(circuit, names, xp, h) - _oracle_energy(circuit, names, xm, h)) / 2
+    return g
+
+
+@pytest.mark.parametrize("n,layers,tile", [(4, 2, 0), (6, 2, 0), (7, 3, 5), (9, 2, 6)])
+def test_emulated_adjoint_matches_parameter_shift(emu, n, layers, tile):
+    from goqu_b200 import workloads
+    c, names = workloads.hardware_efficient_ansatz(n, layers)
+    h = workloads.ising_hamiltonian(n)
+    x = np.random.default_rng(n).uniform(0, 2 * np.pi, len(names))
+    e, g = _emu_adjoint(emu, c, names, x, h, tile=tile)
+    assert abs(e - _oracle_energy(c, names, x, h)) < 1e-12
+    np.testing.assert_allclose(g, _oracle_param_shift(c, names, x, h), atol=1e-10, rtol=0)
+
+
+def test_emulated_adjoint_general_gates(emu):
+    # U3 / CP / RXX / RZZ / RX with expressions (chain rule) and shared parameters
+    from goqu_b200 import circuit as ir, param as prm, pauli as P
+    th = prm.NewVector("t", 5)
+    b = ir.Builder("g", 5)
+    b.H(0).H(1).H(2)
+    b.SymU3(th.At(0), prm.Mul(2.0, th.At(1)), th.At(2), 3)
+    b.SymCP(th.At(3), 0, 4).SymRXX(prm.Add(th.At(4), 0.3), 1, 2).SymRZZ(th.At(0), 2, 3)
+    b.SymRX(prm.Neg(th.At(1)), 4).CNOT(3, 0).SymRY(th.At(2), 1)
+    c = b.Build()
+    names = ir.FreeParameters(c)
+    h = P.NewPauliSum([P.NewPauliString(0.7, {0: P.Z, 3: P.X}, 5), P.NewPauliString(-0.4, {1: P.Y, 2: P.Y}, 5),
+                       P.NewPauliString(0.25, {4: P.X}, 5)])
+    x = np.random.default_rng(3).uniform(0, 2 * np.pi, len(names))
+    e, g = _emu_adjoint(emu, c, names, x, h)
+    fd = np.zeros(len(names))
+    for i in range(len(names)):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += 1e-5
+        xm[i] -= 1e-5
+        fd[i] = (_oracle_energy(c, names, xp, h) - _oracle_energy(c, names, xm, h)) / 2e-5
+    assert abs(e - _oracle_energy(c, names, x, h)) < 1e-12
+    np.testing.assert_allclose(g, fd, atol=1e-7, rtol=0)
