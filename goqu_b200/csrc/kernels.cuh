@@ -141,9 +141,15 @@ __global__ void __launch_bounds__(THREADS, MINB)
     }
     __syncthreads();
     const int warp = t >> 5, lane = t & 31;
+    // Tiles below 2^9 amplitudes have fewer than 32 threads: reduce over the
+    // lanes that exist (the mask of a shuffle must name only live lanes).
+    const unsigned nlanes = blockDim.x < 32 ? blockDim.x : 32u;
+    const unsigned lanes = nlanes == 32 ? 0xffffffffu : ((1u << nlanes) - 1u);
     auto grad = [&](uint32_t slot, double v) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        for (unsigned o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(lanes, v, o);
+            if ((lane ^ o) < (int)nlanes) v += y;
+        }
         if (lane == 0) gsm[warp * MAX_GRAD_SLOTS + slot] = v;
     };
     for (int p = 0; p < pd.n_phases; ++p) {

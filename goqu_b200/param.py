@@ -7,6 +7,8 @@ themselves, which the adjoint gradient uses for the chain rule.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 from . import gate as _gate
@@ -213,8 +215,8 @@ class SymbolicGate(_gate.Gate):
         return None
 
     def Inverse(self):
-        return SymbolicGate(self.base_name + "†", self._n, [Neg(e) for e in self.exprs],
-                            lambda vals, c=self.constructor: c(vals).Inverse())
+        # param/gate.go:37-49: negate the expressions, keep the constructor
+        return SymbolicGate(self.base_name + "†", self._n, [Neg(e) for e in self.exprs], self.constructor)
 
     def Bind(self, bindings):
         vals = [e.Eval(bindings) for e in self.exprs]
@@ -232,22 +234,40 @@ class SymbolicGate(_gate.Gate):
     def IsBound(self):
         return all(e.IsNumeric() for e in self.exprs)
 
+    # exp(-i theta/2 G) with G^2 = I: dU/dtheta = U(theta + pi) / 2
+    _SHIFT = {"RX", "RY", "RZ", "RXX", "RYY", "RZZ"}
+    # diag(1, ..., 1, e^(i phi)): dU/dphi = i (U - I)
+    _PHASE = {"P", "CP", "U1"}
+
+    def _dmatrix(self, k, vals):
+        base = self.base_name.rstrip("†")
+        if len(vals) == 1 and base in self._SHIFT:
+            return self.constructor([vals[0] + math.pi]).Matrix() / 2
+        if len(vals) == 1 and base in self._PHASE:
+            u = self.constructor(vals).Matrix()
+            dim = int(round(math.sqrt(u.size)))
+            return 1j * (u - np.eye(dim, dtype=np.complex128).reshape(-1))
+        if len(vals) == 1 and base == "GlobalPhase":
+            return 1j * self.constructor(vals).Matrix()
+
+        def m(v):
+            vv = list(vals)
+            vv[k] = v
+            return self.constructor(vv).Matrix()
+
+        x = vals[k]
+        return (-m(x + 2 * _H) + 8 * m(x + _H) - 8 * m(x - _H) + m(x - 2 * _H)) / (12 * _H)
+
     def MatrixDerivative(self, name, bindings):
-        """d(bound matrix)/d(parameter `name`) with the chain rule applied."""
+        """d(bound matrix)/d(parameter `name`) with the chain rule applied:
+        closed forms for rotation and phase gates, a 5-point stencil otherwise."""
         vals = [e.Eval(bindings) for e in self.exprs]
         total = None
         for k, e in enumerate(self.exprs):
             de = e.Deriv(name, bindings)
             if de == 0.0:
                 continue
-
-            def m(v, k=k):
-                vv = list(vals)
-                vv[k] = v
-                return self.constructor(vv).Matrix()
-
-            x = vals[k]
-            dm = (-m(x + 2 * _H) + 8 * m(x + _H) - 8 * m(x - _H) + m(x - 2 * _H)) / (12 * _H)
+            dm = self._dmatrix(k, vals)
             total = dm * de if total is None else total + dm * de
         if total is None:
             total = np.zeros_like(self.constructor(vals).Matrix())
