@@ -48,6 +48,7 @@ GQ_OPT_LOW_QUBITS = 3
 GQ_OPT_TIMING = 4
 GQ_OPT_KERNEL_VARIANT = 5
 GQ_OPT_ADJOINT_SEGMENTS = 6
+GQ_OPT_USE_GRAPH = 7
 
 _DBL_P = ctypes.POINTER(ctypes.c_double)
 
@@ -86,6 +87,18 @@ class gq_stats(ctypes.Structure):
         ("pass_ms", ctypes.c_double),
         ("h2d_bytes", ctypes.c_int64),
         ("d2h_bytes", ctypes.c_int64),
+    ]
+
+
+class gq_batch_item(ctypes.Structure):
+    _fields_ = [
+        ("num_qubits", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("ops", ctypes.POINTER(gq_op)),
+        ("n_ops", ctypes.c_size_t),
+        ("terms", ctypes.POINTER(gq_pauli_term)),
+        ("n_terms", ctypes.c_size_t),
+        ("n_params", ctypes.c_size_t),
     ]
 
 
@@ -145,6 +158,11 @@ SIGNATURES = {
     "gq_dm_sample": (_I, [_VP, _DBL_P, _DBL_P, _DBL_P, _SZ, _U64P]),
     "gq_dm_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
     "gq_dm_set_option": (_I, [_VP, _I, ctypes.c_int64]),
+    "gq_batch_create": (_I, [_I, ctypes.POINTER(_VP)]),
+    "gq_batch_destroy": (_I, [_VP]),
+    "gq_batch_run": (_I, [_VP, ctypes.POINTER(gq_batch_item), _SZ, _I, _DBL_P, _DBL_P]),
+    "gq_batch_set_option": (_I, [_VP, _I, ctypes.c_int64]),
+    "gq_batch_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
 }
 
 

@@ -998,3 +998,475 @@ int gq_dm_stats(const gq_dm* dm, gq_stats* out) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Batches of independent circuits (sweep.RunSim-style parameter batches,
+// sweep/run.go:27-171, and the QAOA / VQE evaluations of algorithm/*): every
+// circuit's forward and reverse programs are concatenated into one device
+// program. Wave w runs pass w of every circuit in one launch per tile size
+// (work items = state, pass, CTA), so no kernel waits on another; lambda,
+// energies and gradients are reduced per circuit in fixed order. The launch
+// sequence is captured in a CUDA graph and replayed while the circuits'
+// structure (not their angles) stays the same.
+namespace {
+
+struct BLaunch {
+    uint32_t item0, count;  // into the item array
+    int m;
+    bool adjoint;
+    uint32_t grp0, ngrp;    // gradient groups reduced after an adjoint launch
+};
+
+struct BatchPlan {
+    Program prog;                  // concatenated passes / phases / ops / pool
+    std::vector<int> pass_nslots;  // gradient slots per pass
+    std::vector<uint32_t> slot_grad;
+    std::vector<uint32_t> pass_slot0;
+    std::vector<BItem> items;
+    std::vector<uint64_t> part_off;
+    std::vector<BLaunch> launches;  // forward waves, then reverse waves
+    size_t n_forward_launches = 0;
+    std::vector<BGradGroup> ggroups;
+    std::vector<uint64_t> state_off;
+    uint64_t total_amps = 0, total_partials = 0;
+    std::vector<DGroup> groups;
+    std::vector<DTerm> terms;
+    std::vector<BCircuit> circ;
+    std::vector<BChunk> chunks;
+    std::vector<uint64_t> chunk_seg;
+    size_t total_params = 0;
+    uint64_t signature = 0;
+};
+
+uint64_t fnv(uint64_t h, const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return h;
+}
+
+void append_program(const Program& src, BatchPlan& P, uint64_t grad_off) {
+    const int phase_base = (int)P.prog.phases.size(), op_base = (int)P.prog.ops.size();
+    const uint32_t pool_base = (uint32_t)P.prog.pool.size();
+    for (size_t i = 0; i < src.passes.size(); ++i) {
+        PassDesc pd = src.passes[i];
+        pd.phase0 += phase_base;
+        P.prog.passes.push_back(pd);
+        P.pass_slot0.push_back((uint32_t)P.slot_grad.size());
+        const std::vector<int> none;
+        const std::vector<int>& sp = i < src.pass_params.size() ? src.pass_params[i] : none;
+        P.pass_nslots.push_back((int)sp.size());
+        for (int v : sp) P.slot_grad.push_back((uint32_t)(grad_off + v));
+    }
+    for (PhaseDesc ph : src.phases) {
+        ph.op_begin += op_base;
+        ph.op_end += op_base;
+        P.prog.phases.push_back(ph);
+    }
+    for (KOp op : src.ops) {
+        op.mat += pool_base;
+        P.prog.ops.push_back(op);
+    }
+    P.prog.pool.insert(P.prog.pool.end(), src.pool.begin(), src.pool.end());
+}
+
+}  // namespace
+
+struct gq_batch {
+    Engine e;
+    BatchPlan plan;
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_sig = 0;
+    int64_t graph_launches = 0;
+    bool use_graph = true;
+    DevBuf states, lams, partials, energies, grads, tables;
+};
+
+namespace {
+
+// Batched tile pass per precision: the same launch shapes as variant 0.
+template <class T>
+struct BatchTile;
+template <>
+struct BatchTile<double> {
+    static constexpr auto kernel = k_tile_pass_batch<double, 128, 3>;
+};
+template <>
+struct BatchTile<float> {
+    static constexpr auto kernel = k_tile_pass_batch<float, 256, 2>;
+};
+
+template <class T>
+int set_batch_attrs() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        const int mt = log2i(TileTable<T>::threads(0)) + RQ;
+        err = cudaFuncSetAttribute(BatchTile<T>::kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(cplx<T>) << mt));
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(k_adjoint_pass_batch<T, kAdjThreads, 2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)adj_smem(sizeof(cplx<T>), log2i(kAdjThreads) + RQ));
+    });
+    if (err != cudaSuccess) return fail(GQ_ECUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
+    return GQ_OK;
+}
+
+// Builds the concatenated program, work items and reduction tables.
+int build_batch_plan(int prec, const gq_batch_item* items, size_t n, bool grads, const SchedOptions& base_opt,
+                     BatchPlan& P) {
+    P = BatchPlan();
+    std::string err;
+    std::vector<std::vector<int>> fwd_passes(n), rev_passes(n);
+    std::vector<uint64_t> grad_off(n);
+    for (size_t c = 0; c < n; ++c) {
+        const gq_batch_item& it = items[c];
+        if (it.num_qubits < 1 || it.num_qubits > 30) return fail(GQ_EINVAL, "batch item " + std::to_string(c) + ": qubits out of range");
+        if ((it.n_ops && !it.ops) || (it.n_terms && !it.terms)) return fail(GQ_EINVAL, "batch item " + std::to_string(c) + ": null ops or terms");
+        const int nphys = std::max(it.num_qubits, RQ);
+        std::vector<NGate> fwd, rev;
+        std::vector<int> fo, ro;
+        int rc;
+        if (grads) {
+            rc = adjoint_gates(it.num_qubits, it.ops, it.n_ops, it.n_params, fwd, rev, fo, ro, err);
+        } else {
+            rc = GQ_OK;
+            for (size_t k = 0; k < it.n_ops && rc == GQ_OK; ++k) rc = normalize_op(it.ops[k], it.num_qubits, fwd, err);
+        }
+        if (rc != GQ_OK) return fail(rc, "batch item " + std::to_string(c) + ": " + err);
+        grad_off[c] = P.total_params;
+        P.total_params += it.n_params;
+        P.state_off.push_back(P.total_amps);
+        P.total_amps += 1ull << nphys;
+        SchedOptions o = base_opt;
+        Program pf;
+        schedule(fwd, nphys, o, pf);
+        const size_t pb = P.prog.passes.size();
+        append_program(pf, P, grad_off[c]);
+        for (size_t i = 0; i < pf.passes.size(); ++i) fwd_passes[c].push_back((int)(pb + i));
+        if (grads) {
+            o.tile_qubits = std::min(o.tile_qubits, log2i(kAdjThreads) + RQ);
+            Program pr;
+            schedule(rev, nphys, o, pr);
+            const size_t rb = P.prog.passes.size();
+            append_program(pr, P, grad_off[c]);
+            for (size_t i = 0; i < pr.passes.size(); ++i) rev_passes[c].push_back((int)(rb + i));
+        }
+        // Pauli terms of this circuit: Re(c_t) only (lambda for the gradient
+        // and Re <psi|H|psi>), grouped by x mask
+        const uint64_t qmask = (1ull << it.num_qubits) - 1;
+        std::vector<size_t> order(it.n_terms);
+        for (size_t i = 0; i < it.n_terms; ++i) {
+            if ((it.terms[i].x_mask | it.terms[i].z_mask) & ~qmask)
+                return fail(GQ_EINVAL, "batch item " + std::to_string(c) + ": Pauli term out of range");
+            order[i] = i;
+        }
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t a, size_t b) { return it.terms[a].x_mask < it.terms[b].x_mask; });
+        BCircuit bc;
+        bc.state = P.state_off[c];
+        bc.n_amps = 1ull << it.num_qubits;
+        bc.group0 = (int32_t)P.groups.size();
+        for (size_t k = 0; k < it.n_terms; ++k) {
+            const gq_pauli_term& t = it.terms[order[k]];
+            if (P.groups.size() == (size_t)bc.group0 || P.groups.back().x != t.x_mask)
+                P.groups.push_back({t.x_mask, (int32_t)P.terms.size(), (int32_t)P.terms.size()});
+            const int ny = __builtin_popcountll(t.x_mask & t.z_mask) & 3;
+            double wr = t.coeff_re, wi = 0.0;
+            if (ny == 1) wr = 0.0, wi = t.coeff_re;
+            if (ny == 2) wr = -t.coeff_re;
+            if (ny == 3) wr = 0.0, wi = -t.coeff_re;
+            P.terms.push_back({wr, wi, t.z_mask});
+            P.groups.back().t1 = (int32_t)P.terms.size();
+        }
+        bc.ngroups = (int32_t)P.groups.size() - bc.group0;
+        P.circ.push_back(bc);
+    }
+    // chunks of the lambda / energy kernel
+    const uint32_t chunk_len = 4096;
+    P.chunk_seg.push_back(0);
+    for (size_t c = 0; c < n; ++c) {
+        for (uint64_t b = 0; b < P.circ[c].n_amps; b += chunk_len) P.chunks.push_back({(uint32_t)c, (uint32_t)b});
+        P.chunk_seg.push_back(P.chunks.size());
+    }
+    // waves
+    auto add_waves = [&](const std::vector<std::vector<int>>& passes, bool adjoint) {
+        size_t W = 0;
+        for (auto& v : passes) W = std::max(W, v.size());
+        for (size_t w = 0; w < W; ++w) {
+            for (int m = RQ; m <= MAX_TILE; ++m) {
+                BLaunch L{(uint32_t)P.items.size(), 0, m, adjoint, (uint32_t)P.ggroups.size(), 0};
+                for (size_t c = 0; c < n; ++c) {
+                    if (w >= passes[c].size()) continue;
+                    const int gp = passes[c][w];
+                    const PassDesc& pd = P.prog.passes[gp];
+                    if (pd.m != m) continue;
+                    const uint32_t first = (uint32_t)P.items.size();
+                    for (uint64_t cta = 0; cta < (1ull << pd.n_outer); ++cta) {
+                        P.items.push_back({P.state_off[c], (uint32_t)gp, (uint32_t)cta});
+                        P.part_off.push_back(P.total_partials);
+                        P.total_partials += P.pass_nslots[gp];
+                    }
+                    if (adjoint && P.pass_nslots[gp] > 0)
+                        P.ggroups.push_back({first, (uint32_t)P.items.size(), P.pass_slot0[gp], (uint32_t)P.pass_nslots[gp]});
+                }
+                L.count = (uint32_t)P.items.size() - L.item0;
+                L.ngrp = (uint32_t)P.ggroups.size() - L.grp0;
+                if (L.count) P.launches.push_back(L);
+            }
+        }
+    };
+    add_waves(fwd_passes, false);
+    P.n_forward_launches = P.launches.size();
+    if (grads) add_waves(rev_passes, true);
+    // structure signature: everything but the matrix values
+    uint64_t h = 1469598103934665603ull;
+    h = fnv(h, P.prog.passes.data(), P.prog.passes.size() * sizeof(PassDesc));
+    h = fnv(h, P.prog.phases.data(), P.prog.phases.size() * sizeof(PhaseDesc));
+    h = fnv(h, P.prog.ops.data(), P.prog.ops.size() * sizeof(KOp));
+    h = fnv(h, P.items.data(), P.items.size() * sizeof(BItem));
+    h = fnv(h, P.groups.data(), P.groups.size() * sizeof(DGroup));
+    const size_t ps = P.prog.pool.size(), nt = P.terms.size();
+    h = fnv(h, &ps, sizeof(ps));
+    h = fnv(h, &nt, sizeof(nt));
+    h = fnv(h, &prec, sizeof(prec));
+    const int g = grads;
+    h = fnv(h, &g, sizeof(g));
+    P.signature = h;
+    return GQ_OK;
+}
+
+template <class T>
+int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* grad_out) {
+    Engine& e = b->e;
+    BatchPlan& P = b->plan;
+    // ---- one upload: program | items | part_off | groups... (tables)
+    struct Off {
+        size_t pass, phase, ops, pool, items, part, nslots, ggroups, slotg, bcirc, chunks, seg, groups, terms, soff, total;
+    } o{};
+    size_t at = 0;
+    auto put = [&](size_t bytes) {
+        const size_t r = at;
+        at = align16(at + std::max<size_t>(bytes, 1));
+        return r;
+    };
+    o.pass = put(P.prog.passes.size() * sizeof(PassDesc));
+    o.phase = put(P.prog.phases.size() * sizeof(PhaseDesc));
+    o.ops = put(P.prog.ops.size() * sizeof(KOp));
+    o.pool = put(P.prog.pool.size() * sizeof(cplx<T>));
+    o.items = put(P.items.size() * sizeof(BItem));
+    o.part = put(P.part_off.size() * sizeof(uint64_t));
+    o.nslots = put(P.pass_nslots.size() * sizeof(int));
+    o.ggroups = put(P.ggroups.size() * sizeof(BGradGroup));
+    o.slotg = put(P.slot_grad.size() * sizeof(uint32_t));
+    o.bcirc = put(P.circ.size() * sizeof(BCircuit));
+    o.chunks = put(P.chunks.size() * sizeof(BChunk));
+    o.seg = put(P.chunk_seg.size() * sizeof(uint64_t));
+    o.groups = put(P.groups.size() * sizeof(DGroup));
+    o.terms = put(P.terms.size() * sizeof(DTerm));
+    o.soff = put(P.state_off.size() * sizeof(uint64_t));
+    o.total = at;
+    void* hp = nullptr;
+    GQ_TRY(e.stage(o.total, &hp));
+    char* h = (char*)hp;
+    auto cp = [&](size_t off, const void* src, size_t bytes) {
+        if (bytes) std::memcpy(h + off, src, bytes);
+    };
+    cp(o.pass, P.prog.passes.data(), P.prog.passes.size() * sizeof(PassDesc));
+    cp(o.phase, P.prog.phases.data(), P.prog.phases.size() * sizeof(PhaseDesc));
+    cp(o.ops, P.prog.ops.data(), P.prog.ops.size() * sizeof(KOp));
+    {
+        cplx<T>* pool = (cplx<T>*)(h + o.pool);
+        for (size_t i = 0; i < P.prog.pool.size(); ++i) pool[i] = {(T)P.prog.pool[i].re, (T)P.prog.pool[i].im};
+    }
+    cp(o.items, P.items.data(), P.items.size() * sizeof(BItem));
+    cp(o.part, P.part_off.data(), P.part_off.size() * sizeof(uint64_t));
+    cp(o.nslots, P.pass_nslots.data(), P.pass_nslots.size() * sizeof(int));
+    cp(o.ggroups, P.ggroups.data(), P.ggroups.size() * sizeof(BGradGroup));
+    cp(o.slotg, P.slot_grad.data(), P.slot_grad.size() * sizeof(uint32_t));
+    cp(o.bcirc, P.circ.data(), P.circ.size() * sizeof(BCircuit));
+    cp(o.chunks, P.chunks.data(), P.chunks.size() * sizeof(BChunk));
+    cp(o.seg, P.chunk_seg.data(), P.chunk_seg.size() * sizeof(uint64_t));
+    cp(o.groups, P.groups.data(), P.groups.size() * sizeof(DGroup));
+    cp(o.terms, P.terms.data(), P.terms.size() * sizeof(DTerm));
+    cp(o.soff, P.state_off.data(), P.state_off.size() * sizeof(uint64_t));
+    const bool resized = o.total > b->tables.cap || P.total_amps * sizeof(cplx<T>) > b->states.cap ||
+                         P.total_amps * sizeof(cplx<T>) > b->lams.cap ||
+                         std::max<uint64_t>(P.total_partials, P.chunks.size()) * sizeof(double) > b->partials.cap ||
+                         (n + 1) * sizeof(double) > b->energies.cap ||
+                         std::max<size_t>(1, P.total_params) * sizeof(double) > b->grads.cap;
+    GQ_TRY(b->states.ensure(P.total_amps * sizeof(cplx<T>)));
+    GQ_TRY(b->lams.ensure(P.total_amps * sizeof(cplx<T>)));
+    GQ_TRY(b->partials.ensure(std::max<uint64_t>(1, std::max<uint64_t>(P.total_partials, P.chunks.size())) * sizeof(double)));
+    GQ_TRY(b->energies.ensure((n + 1) * sizeof(double)));
+    GQ_TRY(b->grads.ensure(std::max<size_t>(1, P.total_params) * sizeof(double)));
+    GQ_TRY(b->tables.ensure(o.total));
+    GQ_CUDA(cudaMemcpyAsync(b->tables.p, e.staging.p, o.total, cudaMemcpyHostToDevice, e.stream));
+    GQ_CUDA(cudaEventRecord(e.staged, e.stream));
+    e.staged_pending = true;
+    e.stats.h2d_bytes += (int64_t)o.total;
+    char* d = (char*)b->tables.p;
+    cplx<T>* states = (cplx<T>*)b->states.p;
+    cplx<T>* lams = (cplx<T>*)b->lams.p;
+    double* partial = (double*)b->partials.p;
+
+    const bool replay = b->use_graph && b->graph && b->graph_sig == P.signature && !resized;
+    int64_t launches = 0;
+    auto record = [&]() -> int {
+        GQ_CUDA(cudaMemsetAsync(states, 0, P.total_amps * sizeof(cplx<T>), e.stream));
+        k_batch_basis<T><<<(unsigned)((n + 127) / 128), 128, 0, e.stream>>>(states, (const uint64_t*)(d + o.soff), n);
+        ++launches;
+        for (size_t li = 0; li < P.launches.size(); ++li) {
+            const BLaunch& L = P.launches[li];
+            const unsigned threads = 1u << (L.m - RQ);
+            if (!L.adjoint) {
+                BatchTile<T>::kernel<<<L.count, threads, sizeof(cplx<T>) << L.m, e.stream>>>(
+                    states, (const BItem*)(d + o.items) + L.item0, (const PassDesc*)(d + o.pass),
+                    (const PhaseDesc*)(d + o.phase), (const KOp*)(d + o.ops), (const cplx<T>*)(d + o.pool));
+                ++launches;
+            } else {
+                k_adjoint_pass_batch<T, kAdjThreads, 2><<<L.count, threads, adj_smem(sizeof(cplx<T>), L.m), e.stream>>>(
+                    states, lams, (const BItem*)(d + o.items) + L.item0, (const uint64_t*)(d + o.part) + L.item0,
+                    (const int*)(d + o.nslots), (const PassDesc*)(d + o.pass), (const PhaseDesc*)(d + o.phase),
+                    (const KOp*)(d + o.ops), (const cplx<T>*)(d + o.pool), partial);
+                ++launches;
+                if (L.ngrp) {
+                    k_grad_reduce_batch<<<L.ngrp, 256, 0, e.stream>>>(partial, (const uint64_t*)(d + o.part),
+                                                                      (const BGradGroup*)(d + o.ggroups) + L.grp0,
+                                                                      (const uint32_t*)(d + o.slotg),
+                                                                      (double*)b->grads.p);
+                    ++launches;
+                }
+            }
+            if (li + 1 == P.n_forward_launches) {
+                // after the forward waves: lambda and the energies
+                k_apply_terms_batch<T><<<(unsigned)P.chunks.size(), 256, 0, e.stream>>>(
+                    states, lams, (const BCircuit*)(d + o.bcirc), (const BChunk*)(d + o.chunks), 4096,
+                    (const DGroup*)(d + o.groups), (const DTerm*)(d + o.terms), partial);
+                k_segment_reduce<<<(unsigned)n, 256, 0, e.stream>>>(partial, (const uint64_t*)(d + o.seg),
+                                                                    (double*)b->energies.p);
+                GQ_CUDA(cudaMemsetAsync(b->grads.p, 0, std::max<size_t>(1, P.total_params) * sizeof(double), e.stream));
+                launches += 2;
+            }
+        }
+        if (P.n_forward_launches == 0) {
+            k_apply_terms_batch<T><<<(unsigned)P.chunks.size(), 256, 0, e.stream>>>(
+                states, lams, (const BCircuit*)(d + o.bcirc), (const BChunk*)(d + o.chunks), 4096,
+                (const DGroup*)(d + o.groups), (const DTerm*)(d + o.terms), partial);
+            k_segment_reduce<<<(unsigned)n, 256, 0, e.stream>>>(partial, (const uint64_t*)(d + o.seg),
+                                                                (double*)b->energies.p);
+            GQ_CUDA(cudaMemsetAsync(b->grads.p, 0, std::max<size_t>(1, P.total_params) * sizeof(double), e.stream));
+            launches += 2;
+        }
+        GQ_CUDA(cudaGetLastError());
+        return GQ_OK;
+    };
+    if (replay) {
+        GQ_CUDA(cudaGraphLaunch(b->graph, e.stream));
+        launches = b->graph_launches;  // the recorded sequence
+    } else if (b->use_graph) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        GQ_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+        int rc = record();
+        cudaError_t ce = cudaStreamEndCapture(e.stream, &g);
+        if (rc != GQ_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(GQ_ECUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+            b->graph = nullptr;
+            return fail(GQ_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        }
+        b->graph_sig = P.signature;
+        b->graph_launches = launches;
+        GQ_CUDA(cudaGraphLaunch(b->graph, e.stream));
+    } else {
+        GQ_TRY(record());
+    }
+    e.stats.kernel_launches = launches;
+    if (energies) GQ_CUDA(cudaMemcpyAsync(energies, b->energies.p, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+    if (grads && grad_out && P.total_params)
+        GQ_CUDA(cudaMemcpyAsync(grad_out, b->grads.p, P.total_params * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+    e.stats.d2h_bytes += (int64_t)(n * sizeof(double) + (grads ? P.total_params * sizeof(double) : 0));
+    GQ_CUDA(cudaStreamSynchronize(e.stream));
+    return GQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gq_batch_create(int precision, gq_batch** out) {
+    if (!out) return fail(GQ_EINVAL, "null output handle");
+    *out = nullptr;
+    if (!valid_prec(precision)) return fail(GQ_EINVAL, "unknown precision");
+    gq_batch* b = new gq_batch();
+    int rc = b->e.init(RQ, precision);
+    if (rc == GQ_OK) rc = precision == GQ_C64 ? set_batch_attrs<float>() : set_batch_attrs<double>();
+    if (rc != GQ_OK) {
+        b->e.destroy();
+        delete b;
+        return rc;
+    }
+    b->e.opt.tile_qubits = precision == GQ_C64 ? 12 : 11;
+    *out = b;
+    return GQ_OK;
+}
+
+int gq_batch_destroy(gq_batch* b) {
+    if (!b) return GQ_OK;
+    if (b->e.stream) cudaStreamSynchronize(b->e.stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->states.release();
+    b->lams.release();
+    b->partials.release();
+    b->energies.release();
+    b->grads.release();
+    b->tables.release();
+    b->e.destroy();
+    delete b;
+    return GQ_OK;
+}
+
+int gq_batch_run(gq_batch* b, const gq_batch_item* items, size_t n_items, int want_gradients, double* energies_out,
+                 double* grads_out) {
+    if (!b) return fail(GQ_EINVAL, "null handle");
+    if (n_items == 0) return GQ_OK;
+    if (!items) return fail(GQ_EINVAL, "null items");
+    Engine& e = b->e;
+    e.clear_stats();
+    GQ_TRY(e.time_begin());
+    GQ_TRY(build_batch_plan(e.prec, items, n_items, want_gradients != 0, e.opt, b->plan));
+    const int rc = e.prec == GQ_C64 ? batch_run_t<float>(b, want_gradients != 0, n_items, energies_out, grads_out)
+                                    : batch_run_t<double>(b, want_gradients != 0, n_items, energies_out, grads_out);
+    if (rc != GQ_OK) return rc;
+    e.stats.passes = (int64_t)b->plan.prog.passes.size();
+    e.stats.phases = (int64_t)b->plan.prog.phases.size();
+    e.stats.state_bytes = (int64_t)(b->plan.total_amps * e.amp_bytes());
+    return e.time_end();
+}
+
+int gq_batch_set_option(gq_batch* b, int key, int64_t value) {
+    if (!b) return fail(GQ_EINVAL, "null handle");
+    switch (key) {
+        case GQ_OPT_TIMING: b->e.timing = value != 0; return GQ_OK;
+        case GQ_OPT_PASS_BUDGET: b->e.opt.budget = value == 0 ? kDefaultBudget : (int)value; return GQ_OK;
+        case GQ_OPT_USE_GRAPH: b->use_graph = value != 0; return GQ_OK;
+        default: return fail(GQ_EINVAL, "unknown option");
+    }
+}
+
+int gq_batch_stats(const gq_batch* b, gq_stats* out) {
+    if (!b || !out) return fail(GQ_EINVAL, "null argument");
+    *out = b->e.stats;
+    return GQ_OK;
+}
+
+}  // extern "C"

@@ -22,18 +22,15 @@ constexpr TileVariant kVariantsC128[] = {{128, 3}, {128, 4}, {256, 2}, {64, 6}};
 constexpr TileVariant kVariantsC64[] = {{256, 2}, {128, 4}, {512, 1}, {128, 3}};
 constexpr int kNumVariants = 4;
 
-template <class T, int THREADS, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB)
-    k_tile_pass(cplx<T>* __restrict__ st, const PassDesc* __restrict__ pdp,
-                                                   const PhaseDesc* __restrict__ phases,
-                                                   const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
-    const PassDesc& pd = *pdp;
+// One CTA's share of a pass over the state `st` (CTA index `cta` of pass pd).
+template <class T>
+__device__ __forceinline__ void tile_pass_body(cplx<T>* __restrict__ st, const PassDesc& pd,
+                                               const PhaseDesc* __restrict__ phases, const KOp* __restrict__ ops,
+                                               const cplx<T>* __restrict__ pool, uint64_t cta, cplx<T>* sm) {
     const int m = pd.m;
     const int tbits = m - RQ;
     const uint32_t t = threadIdx.x;
-    const uint64_t base = cta_base(pd, blockIdx.x);
+    const uint64_t base = cta_base(pd, cta);
 
     // Linear staging index lin = it * 2^tbits + t: thread bits are tile bits
     // [0, tbits), `it` supplies tile bits [tbits, m).
@@ -102,25 +99,50 @@ __global__ void __launch_bounds__(THREADS, MINB)
     }
 }
 
+template <class T, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_tile_pass(cplx<T>* __restrict__ st, const PassDesc* __restrict__ pdp, const PhaseDesc* __restrict__ phases,
+                const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    tile_pass_body<T>(st, *pdp, phases, ops, pool, blockIdx.x, reinterpret_cast<cplx<T>*>(smraw));
+}
+
+// A batch of independent states: block b runs CTA items[b].cta of pass
+// items[b].pass on the state starting at amplitude items[b].state.
+struct BItem {
+    uint64_t state;
+    uint32_t pass;
+    uint32_t cta;
+};
+
+template <class T, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_tile_pass_batch(cplx<T>* __restrict__ states, const BItem* __restrict__ items, const PassDesc* __restrict__ passes,
+                      const PhaseDesc* __restrict__ phases, const KOp* __restrict__ ops,
+                      const cplx<T>* __restrict__ pool) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const BItem it = items[blockIdx.x];
+    tile_pass_body<T>(states + it.state, passes[it.pass], phases, ops, pool, it.cta, reinterpret_cast<cplx<T>*>(smraw));
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint reverse pass: the tile pass on two states (psi, lambda) at once,
 // with gradient ops. Each warp writes its sum for every gradient slot once
 // per pass into shared memory; the CTA's per-slot totals go to
 // partial[cta * nslots + slot] (summed per slot by k_grad_reduce).
-template <class T, int THREADS, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB)
-    k_adjoint_pass(cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam, const PassDesc* __restrict__ pdp,
-                   const PhaseDesc* __restrict__ phases, const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool,
-                   double* __restrict__ partial, int nslots) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const PassDesc& pd = *pdp;
+template <class T>
+__device__ __forceinline__ void adjoint_pass_body(cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam,
+                                                  const PassDesc& pd, const PhaseDesc* __restrict__ phases,
+                                                  const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool,
+                                                  uint64_t cta, double* __restrict__ partial_out, int nslots,
+                                                  unsigned char* smraw) {
     const int m = pd.m;
     const int tbits = m - RQ;
     cplx<T>* sa = reinterpret_cast<cplx<T>*>(smraw);
     cplx<T>* sb = sa + (1u << m);
     double* gsm = reinterpret_cast<double*>(sb + (1u << m));  // [warps][MAX_GRAD_SLOTS]
     const uint32_t t = threadIdx.x;
-    const uint64_t base = cta_base(pd, blockIdx.x);
+    const uint64_t base = cta_base(pd, cta);
     uint64_t gt = 0;
     uint32_t stt = 0;
     for (int b = 0; b < tbits; ++b)
@@ -167,11 +189,36 @@ __global__ void __launch_bounds__(THREADS, MINB)
         psi[g] = sa[s];
         lam[g] = sb[s];
     }
-    if ((int)t < nslots) {
+    __syncthreads();
+    for (int sl = (int)t; sl < nslots; sl += (int)blockDim.x) {  // tiles may have fewer threads than slots
         double acc = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += gsm[w * MAX_GRAD_SLOTS + t];
-        partial[(uint64_t)blockIdx.x * nslots + t] = acc;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) acc += gsm[w * MAX_GRAD_SLOTS + sl];
+        partial_out[sl] = acc;
     }
+}
+
+template <class T, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_adjoint_pass(cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam, const PassDesc* __restrict__ pdp,
+                   const PhaseDesc* __restrict__ phases, const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool,
+                   double* __restrict__ partial, int nslots) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    adjoint_pass_body<T>(psi, lam, *pdp, phases, ops, pool, blockIdx.x, partial + (uint64_t)blockIdx.x * nslots,
+                         nslots, smraw);
+}
+
+// Batched reverse passes: item b's gradient partials go to
+// partial[part_off[b] .. + nslots of its pass].
+template <class T, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+    k_adjoint_pass_batch(cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam, const BItem* __restrict__ items,
+                         const uint64_t* __restrict__ part_off, const int* __restrict__ pass_nslots,
+                         const PassDesc* __restrict__ passes, const PhaseDesc* __restrict__ phases,
+                         const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool, double* __restrict__ partial) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const BItem it = items[blockIdx.x];
+    adjoint_pass_body<T>(psi + it.state, lam + it.state, passes[it.pass], phases, ops, pool, it.cta,
+                         partial + part_off[blockIdx.x], pass_nslots[it.pass], smraw);
 }
 
 // grad[slot_param[s]] += 2 * sum over CTAs of partial[cta][s], slots in order
@@ -656,6 +703,114 @@ __global__ void k_apply_terms(const cplx<T>* __restrict__ psi, cplx<T>* __restri
         e += (double)a.x * lr + (double)a.y * li;
     }
     block_reduce_store(e, 0.0, partial);
+}
+
+// ---------------------------------------------------------------------------
+// Batched reductions for many small states.
+struct BCircuit {
+    uint64_t state;   // first amplitude of the circuit's state (and lambda)
+    uint64_t n_amps;
+    int32_t group0, ngroups;  // its Pauli groups in the concatenated arrays
+};
+struct BChunk {
+    uint32_t circuit;
+    uint32_t begin;  // first amplitude of this block's chunk
+};
+
+// lambda = sum_t Re(c_t) P_t psi per circuit, and per-block partials of
+// Re <psi|lambda> (summed per circuit by k_segment_reduce).
+template <class T>
+__global__ void k_apply_terms_batch(const cplx<T>* __restrict__ psi_all, cplx<T>* __restrict__ lam_all,
+                                    const BCircuit* __restrict__ circ, const BChunk* __restrict__ chunks,
+                                    uint32_t chunk_len, const DGroup* __restrict__ groups,
+                                    const DTerm* __restrict__ terms, double* __restrict__ partial) {
+    const BChunk ch = chunks[blockIdx.x];
+    const BCircuit c = circ[ch.circuit];
+    const cplx<T>* psi = psi_all + c.state;
+    cplx<T>* lam = lam_all + c.state;
+    const uint64_t end = (uint64_t)ch.begin + chunk_len < c.n_amps ? (uint64_t)ch.begin + chunk_len : c.n_amps;
+    double e = 0.0;
+    for (uint64_t i = ch.begin + threadIdx.x; i < end; i += blockDim.x) {
+        double lr = 0.0, li = 0.0;
+        for (int g = c.group0; g < c.group0 + c.ngroups; ++g) {
+            const DGroup gr = groups[g];
+            const uint64_t j = i ^ gr.x;
+            const cplx<T> v = psi[j];
+            double fr = 0.0, fi = 0.0;
+            for (int k = gr.t0; k < gr.t1; ++k) {
+                const DTerm tm = terms[k];
+                const double sg = (__popcll(j & tm.z) & 1) ? -1.0 : 1.0;
+                fr += sg * tm.wre;
+                fi += sg * tm.wim;
+            }
+            lr += fr * (double)v.x - fi * (double)v.y;
+            li += fr * (double)v.y + fi * (double)v.x;
+        }
+        lam[i] = {(T)lr, (T)li};
+        const cplx<T> a = psi[i];
+        e += (double)a.x * lr + (double)a.y * li;
+    }
+    e = warp_sum(e);
+    __shared__ double ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (unsigned w = 0; w < (blockDim.x >> 5); ++w) tot += ws[w];
+        partial[blockIdx.x] = tot;
+    }
+}
+
+// out[s] = sum of partial[seg[s] .. seg[s+1]) (one block per segment).
+__global__ void k_segment_reduce(const double* __restrict__ partial, const uint64_t* __restrict__ seg,
+                                 double* __restrict__ out) {
+    const uint64_t b = seg[blockIdx.x], e = seg[blockIdx.x + 1];
+    double v = 0.0;
+    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) v += partial[i];
+    v = warp_sum(v);
+    __shared__ double ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (unsigned w = 0; w < (blockDim.x >> 5); ++w) tot += ws[w];
+        out[blockIdx.x] = tot;
+    }
+}
+
+// Gradient partials of one reverse wave: group g covers items [ib, ie) of
+// one circuit's pass, each item holding nslots partials from part_off[item];
+// grad[slot_grad[slot0 + s]] += 2 * sum over the group's items.
+struct BGradGroup {
+    uint32_t item_begin, item_end;
+    uint32_t slot0;   // into slot_grad
+    uint32_t nslots;
+};
+__global__ void k_grad_reduce_batch(const double* __restrict__ partial, const uint64_t* __restrict__ part_off,
+                                    const BGradGroup* __restrict__ grp, const uint32_t* __restrict__ slot_grad,
+                                    double* __restrict__ grad) {
+    const BGradGroup g = grp[blockIdx.x];
+    __shared__ double ws[32];
+    for (uint32_t s = 0; s < g.nslots; ++s) {
+        double v = 0.0;
+        for (uint32_t it = g.item_begin + threadIdx.x; it < g.item_end; it += blockDim.x) v += partial[part_off[it] + s];
+        v = warp_sum(v);
+        if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (unsigned w = 0; w < (blockDim.x >> 5); ++w) tot += ws[w];
+            grad[slot_grad[g.slot0 + s]] += 2.0 * tot;
+        }
+        __syncthreads();
+    }
+}
+
+// |0...0> in every state of a batch (after a memset to zero).
+template <class T>
+__global__ void k_batch_basis(cplx<T>* __restrict__ states, const uint64_t* __restrict__ offs, uint64_t n) {
+    const uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (c < n) states[offs[c]] = {T(1), T(0)};
 }
 
 }  // namespace gq

@@ -176,6 +176,7 @@ int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 #define GQ_OPT_TIMING 4         /* 1: record CUDA events around every apply        */
 #define GQ_OPT_KERNEL_VARIANT 5 /* tile-pass launch shape (0..3); sets the tile size */
 #define GQ_OPT_ADJOINT_SEGMENTS 6 /* adjoint: forward checkpoints (0 = automatic, 1 = none) */
+#define GQ_OPT_USE_GRAPH 7      /* batches: capture launches in a CUDA graph (default 1) */
 int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
 
 /* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */
@@ -210,6 +211,31 @@ int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* 
                  size_t shots, uint64_t* idx_out);
 int gq_dm_stats(const gq_dm* dm, gq_stats* out);
 int gq_dm_set_option(gq_dm* dm, int key, int64_t value);
+
+/* ---- batches of independent circuits ------------------------------------
+ * Replaces the per-point loop of sweep.RunSim (sweep/run.go:27-97) and the
+ * cost / gradient evaluations of algorithm/qaoa (qaoa.go:100-126) and
+ * algorithm/vqe: every item is a circuit applied to |0...0> with a Pauli sum;
+ * gq_batch_run returns Re <psi|H|psi> per item and, with want_gradients, the
+ * adjoint gradient of each item (n_params entries per item, concatenated in
+ * item order). All items run in one sequence of batched launches.          */
+typedef struct gq_batch gq_batch;
+typedef struct gq_batch_item {
+    int32_t num_qubits;
+    int32_t reserved;
+    const gq_op* ops;
+    size_t n_ops;
+    const gq_pauli_term* terms;
+    size_t n_terms;
+    size_t n_params;
+} gq_batch_item;
+
+int gq_batch_create(int precision, gq_batch** out);
+int gq_batch_destroy(gq_batch* b);
+int gq_batch_run(gq_batch* b, const gq_batch_item* items, size_t n_items, int want_gradients,
+                 double* energies_out, double* grads_out);
+int gq_batch_set_option(gq_batch* b, int key, int64_t value);
+int gq_batch_stats(const gq_batch* b, gq_stats* out);
 
 #ifdef __cplusplus
 }
