@@ -50,6 +50,8 @@ GQ_OPT_KERNEL_VARIANT = 5
 GQ_OPT_ADJOINT_SEGMENTS = 6
 GQ_OPT_USE_GRAPH = 7
 
+GQ_NOALLOC_MAX_TERMS = 2048
+
 _DBL_P = ctypes.POINTER(ctypes.c_double)
 
 
@@ -163,6 +165,7 @@ SIGNATURES = {
     "gq_batch_run": (_I, [_VP, ctypes.POINTER(gq_batch_item), _SZ, _I, _DBL_P, _DBL_P]),
     "gq_batch_set_option": (_I, [_VP, _I, ctypes.c_int64]),
     "gq_batch_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
+    "gq_expect_pauli_sum_noalloc": (_I, [_VP, _I, _I, _TP, _SZ, _VP, _DBL_P, _DBL_P]),
 }
 
 

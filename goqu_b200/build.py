@@ -17,7 +17,7 @@ NVCC_FLAGS = [
     "-shared",
 ]
 
-ENGINE_SOURCES = ["engine.cu", "schedule.cpp"]
+ENGINE_SOURCES = ["engine.cu", "noalloc.cu", "schedule.cpp"]
 EMULATOR_SOURCES = ["emulate.cpp", "schedule.cpp"]
 HEADERS = ["tile_core.cuh", "kernels.cuh", "schedule.hpp", os.path.join("..", "..", "include", "gqb200.h")]
 

@@ -505,6 +505,11 @@ bool valid_prec(int p) { return p == GQ_C128 || p == GQ_C64; }
 
 }  // namespace
 
+namespace gq {
+// The calling thread's last error, for entry points defined in other files.
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace gq
+
 // ============================================================================
 struct gq_sv {
     Engine e;

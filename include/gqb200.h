@@ -237,6 +237,24 @@ int gq_batch_run(gq_batch* b, const gq_batch_item* items, size_t n_items, int wa
 int gq_batch_set_option(gq_batch* b, int key, int64_t value);
 int gq_batch_stats(const gq_batch* b, gq_stats* out);
 
+/* ---- expectation without allocation ---------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that own
+ * their device memory and must not have the library call cudaMalloc or
+ * cudaFree (an application allocator that has reserved the GPU's memory, a
+ * latency-critical loop that cannot take the synchronisation cudaFree may
+ * imply). Computes sum_t coeff_t <psi|P_t|psi> of a state the caller
+ * allocated (2^num_qubits interleaved complex128 or complex64 amplitudes at
+ * device_state) on `stream` (a cudaStream_t, NULL for the default stream).
+ * Its scratch is a 256 KiB array compiled into the library, so at most
+ * GQ_NOALLOC_MAX_TERMS terms are accepted (larger sums return GQ_EINVAL).
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture. Calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller.                             */
+#define GQ_NOALLOC_MAX_TERMS 2048
+int gq_expect_pauli_sum_noalloc(const void* device_state, int num_qubits, int precision,
+                                const gq_pauli_term* terms, size_t n_terms, void* stream,
+                                double* out_re, double* out_im);
+
 #ifdef __cplusplus
 }
 #endif
