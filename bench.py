@@ -3,21 +3,27 @@
 Workload (one step): goqu statevector Evolve of a seeded 28-qubit circuit of
 40 layers (U3 with uniform [0, 2 pi) angles on every qubit, then a CNOT
 brickwork) followed by a 28-qubit QFT (algorithm/qpe/qpe.go:170-182): 2080
-gates on a 4 GiB complex128 state, which is 32x the B200 L2 cache, so every
-pass streams HBM (no flush needed). The device is timed with CUDA events on the
-engine's stream; e2e is the public C-ABI call gq_sv_run (Evolve + 1024
+gates on a 4 GiB complex128 state, 32x the B200 L2 cache, so every pass
+streams HBM (no flush needed). The device is timed with CUDA events on the
+engine's stream. e2e is the public C-ABI call gq_sv_run (Evolve + 1024
 inverse-CDF shots) with the op stream coming from host memory and the sampled
 indices copied back, timed on the host around the call.
+
+Extras (other configurations of the same path, reported in "extras"):
+adjoint gradients of a 20-qubit 400-parameter ansatz against the engine's own
+parameter shift; a noisy 12-qubit density matrix; a batch of 4096 QAOA MaxCut
+circuits (complex64, energies + gradients).
 
 --impl reference times the CPU restatement of goqu's pure-Go path (the oracle,
 threaded like goqu's auto-parallel kernels) on this host's cores, on a bounded
 sample of the same circuit (the first gates of the 2080). Multi-GPU runs
-(torchrun) are independent replicas, one 28-qubit state per GPU.
+(torchrun) are independent replicas, one state per GPU.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -29,11 +35,14 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-N_QUBITS = 28
 LAYERS = 40
 SEED = 2028
 SHOTS = 1024
-WORKLOAD = f"statevector {N_QUBITS}q complex128: {LAYERS} U3+CNOT brickwork layers + QFT{N_QUBITS} (2080 gates), {SHOTS} shots"
+
+
+def workload_name(n, precision):
+    return (f"statevector {n}q {'complex64' if precision == 'c64' else 'complex128'}: {LAYERS} U3+CNOT "
+            f"brickwork layers + QFT{n}, {SHOTS} shots")
 
 
 def peaks():
@@ -127,75 +136,153 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def build_workload():
+def build_workload(n):
     from goqu_b200 import encode, workloads
-    c = workloads.random_layers_qft(N_QUBITS, LAYERS, SEED)
+    c = workloads.random_layers_qft(n, LAYERS, SEED)
     return c, encode.statevector_ops(c), workloads.count_gates(c)
 
 
-def cpu_baseline(stream, gates_total, budget_s=20.0):
+def cpu_baseline(n, stream, gates_total, budget_s=20.0):
     """Oracle (goqu's CPU algorithm restated, threaded like goqu) on the first
     gates of the same circuit at full size."""
-    from oracle import binding as orc
-    from goqu_b200 import encode as enc
-    threads = os.cpu_count() or 1
-    state = orc.zero_state(N_QUBITS)
-    sub = enc.OpStream(N_QUBITS)
-    done = 0
-    t_used = 0.0
-    # apply gates one at a time until the time budget is spent
-    ops = stream.array()
     import ctypes
+
+    from oracle import binding as orc
+    threads = os.cpu_count() or 1
+    state = orc.zero_state(n)
+    ops = stream.array()
+    done, t_used = 0, 0.0
     for i in range(len(stream)):
         one = (type(ops[0]) * 1)(ops[i])
         t0 = time.perf_counter()
-        rc = orc.lib().or_sv_apply(N_QUBITS, state.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+        rc = orc.lib().or_sv_apply(n, state.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                    ctypes.cast(one, ctypes.POINTER(type(ops[0]))), 1, threads)
         t_used += time.perf_counter() - t0
         assert rc == 0
         done += 1
         if t_used > budget_s:
             break
-    del sub
-    rate = done / t_used
-    return {"value": rate, "unit": "gates/s", "cores": threads, "kind": "port",
-            "sample": f"first {done} of {gates_total} gates at {N_QUBITS} qubits (complex128, {t_used:.1f} s), "
+    return {"value": done / t_used, "unit": "gates/s", "cores": threads, "kind": "port",
+            "sample": f"first {done} of {gates_total} gates at {n} qubits (complex128, {t_used:.1f} s), "
                       f"oracle threaded like goqu's GOMAXPROCS workers"}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    from goqu_b200 import encode  # noqa: F401
-    c, stream, gates = build_workload()
+    n = args.qubits
+    c, stream, gates = build_workload(n)
     budget = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
-        cpu_baseline(stream, gates, budget_s=min(budget, 3.0))
-    vals = []
-    last = None
+        cpu_baseline(n, stream, gates, budget_s=min(budget, 3.0))
+    vals, last = [], None
     for _ in range(args.steps):
-        last = cpu_baseline(stream, gates, budget_s=budget)
+        last = cpu_baseline(n, stream, gates, budget_s=budget)
         vals.append(last["value"])
     value = float(np.mean(vals))
-    line = {"impl": "reference", "metric": "28q gates/s", "value": value, "unit": "gates/s", "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": f"{n}q gates/s", "value": value, "unit": "gates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * gates / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "gates": gates, "seed": SEED,
+            "config": {"workload": workload_name(n, "c128"), "qubits": n, "gates": gates, "seed": SEED,
                        "l2": "state 4 GiB > 126 MB L2 (no flush needed)"},
             "cpu_baseline": dict(last, value=value),
             "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
+def extra_adjoint():
+    """20-qubit hardware-efficient ansatz (10 layers RY,RZ + CZ ring, 400
+    parameters), transverse-field Ising observable: adjoint gradient vs the
+    full 800-evaluation parameter shift on the same engine."""
+    from goqu_b200 import _abi, gradient, workloads
+    c, names = workloads.hardware_efficient_ansatz(20, 10)
+    h = workloads.ising_hamiltonian(20)
+    x = np.random.default_rng(20).uniform(0, 2 * np.pi, len(names))
+    ev = gradient.AdjointEvaluator(c, h, names)
+    ev.sim.set_option(_abi.GQ_OPT_TIMING, 1)
+    for _ in range(3):
+        ev(x)
+    dev, t0 = [], time.perf_counter()
+    for _ in range(10):
+        _, g_adj = ev(x)
+        dev.append(ev.sim.stats()["last_ms"])
+    wall = (time.perf_counter() - t0) / 10
+    f = gradient.CostFunc(c, h, names)
+    f.sim.set_option(_abi.GQ_OPT_TIMING, 1)
+    f(x)
+    g_ps = np.empty(len(names))
+    ps_dev, t1 = 0.0, time.perf_counter()
+    for i in range(len(names)):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += math.pi / 2
+        xm[i] -= math.pi / 2
+        ep = f(xp)
+        ps_dev += f.sim.stats()["last_ms"]
+        em = f(xm)
+        ps_dev += f.sim.stats()["last_ms"]
+        g_ps[i] = (ep - em) / 2
+    ps_wall = time.perf_counter() - t1
+    adj_ms = float(np.median(dev))
+    return {"workload": "adjoint gradient, 20q HEA 10 layers, 400 params, Ising H (39 terms), complex128",
+            "adjoint_grads_per_s": 1000.0 / adj_ms, "adjoint_ms_device": adj_ms, "adjoint_ms_wall": wall * 1e3,
+            "param_shift_grads_per_s": 1000.0 / ps_dev, "param_shift_ms_device": ps_dev,
+            "param_shift_ms_wall": ps_wall * 1e3, "speedup_device": ps_dev / adj_ms,
+            "speedup_wall": ps_wall / wall, "max_abs_diff_vs_param_shift": float(np.max(np.abs(g_adj - g_ps)))}
+
+
+def extra_density():
+    """Noisy 12-qubit density matrix: 30 U3 + CNOT brickwork layers,
+    depolarizing 1e-3 after every gate, amplitude damping 1e-3 on idle qubits."""
+    from goqu_b200 import _abi, densitymatrix, encode, pauli, workloads
+    c, nm = workloads.noisy_brickwork(12, layers=30, seed=12)
+    dm = densitymatrix.New(12).WithNoise(nm)
+    dm.set_option(_abi.GQ_OPT_TIMING, 1)
+    s = encode.density_ops(c, nm)
+    lib = _abi.lib()
+    for _ in range(2):
+        _abi.check(lib.gq_dm_evolve(dm._h, s.ptr(), len(s)))
+    ms = []
+    for _ in range(5):
+        _abi.check(lib.gq_dm_evolve(dm._h, s.ptr(), len(s)))
+        ms.append(dm.stats()["last_ms"])
+    st = dm.stats()
+    z = [dm.ExpectPauliString(pauli.ZOn([q], 12)) for q in range(12)]
+    tr = dm.Trace()
+    return {"workload": "density matrix 12q, 30 noisy U3+CNOT layers (depolarizing + amplitude damping)",
+            "ms_device": float(np.median(ms)), "gates": workloads.count_gates(c), "ops_with_channels": len(s),
+            "passes": st["passes"], "trace_minus_one": abs(tr - 1.0), "z_expectations": z[:3]}
+
+
+def extra_qaoa():
+    """4096 QAOA MaxCut circuits on seeded random 3-regular graphs, n in
+    {10..20} even, p in 1..4, complex64: energies + adjoint gradients in one
+    batched call (second call replays the captured CUDA graph)."""
+    from goqu_b200 import _abi, batch, workloads
+    t0 = time.perf_counter()
+    evals = workloads.qaoa_batch(4096, seed=4)
+    streams, terms = batch.Batch.encode(evals)
+    host_s = time.perf_counter() - t0
+    npar = [len(e[1]) for e in evals]
+    b = batch.Batch(_abi.GQ_C64)
+    b.set_option(_abi.GQ_OPT_TIMING, 1)
+    ms = []
+    for _ in range(3):
+        b.run_encoded(streams, terms, npar)
+        ms.append(b.stats()["last_ms"])
+    st = b.stats()
+    return {"workload": "4096 QAOA MaxCut circuits (n 10..20, p 1..4), complex64, energies + gradients",
+            "circuits_per_s": 4096 / (ms[-1] / 1000.0), "ms_device_first": ms[0], "ms_device_replay": ms[-1],
+            "passes": st["passes"], "launches": st["kernel_launches"], "host_encode_s": host_s}
+
+
 def run_gpu(args, world, rank, local):
     import ctypes
 
     from goqu_b200 import _abi, statevector
-    c, stream, gates = build_workload()
-    sim = statevector.New(N_QUBITS, _abi.GQ_C64 if args.precision == "c64" else _abi.GQ_C128)
+    n = args.qubits
+    c, stream, gates = build_workload(n)
+    sim = statevector.New(n, _abi.GQ_C64 if args.precision == "c64" else _abi.GQ_C128)
     sim.set_option(_abi.GQ_OPT_TIMING, 1)
-    if args.tile:
-        sim.set_option(_abi.GQ_OPT_TILE_QUBITS, args.tile)
     if args.budget:
         sim.set_option(_abi.GQ_OPT_PASS_BUDGET, args.budget)
     lib = _abi.lib()
@@ -238,7 +325,7 @@ def run_gpu(args, world, rank, local):
     # ---- roofline of the dominant kernel (the tile pass)
     peak, peak_kind = peaks()
     amp_bytes = 8 if args.precision == "c64" else 16
-    alg_bytes = 2 * amp_bytes * (1 << N_QUBITS)  # one read + one write of the state per pass
+    alg_bytes = 2 * amp_bytes * (1 << n)  # one read + one write of the state per pass
     per_launch_ms = float(np.sum(pass_ms)) / max(1, passes)
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     traffic = None
@@ -246,16 +333,18 @@ def run_gpu(args, world, rank, local):
     if os.path.exists(tf):
         with open(tf) as f:
             tj = json.load(f)
-        traffic = tj.get(args.precision, {}).get("bytes_per_launch")
+        t = tj.get(args.precision, {})
+        if t.get("bytes_per_launch_24q"):
+            traffic = t["bytes_per_launch_24q"] * float(1 << (n - 24))  # traffic scales with 2^n
 
     line = {
-        "metric": "28q gates/s", "value": value, "unit": "gates/s", "n_gpus": world, "steps": args.steps,
+        "metric": f"{n}q gates/s", "value": value, "unit": "gates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "c64" else "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "qubits": N_QUBITS, "gates": gates, "seed": SEED,
+        "config": {"workload": workload_name(n, args.precision), "qubits": n, "gates": gates, "seed": SEED,
                    "precision": args.precision, "parallelism": f"replicas{world}" if world > 1 else "single",
-                   "l2": "state 4 GiB > 126 MB L2 (no flush needed)",
+                   "l2": f"state {amp_bytes << n >> 20} MiB vs 126 MB L2 (no flush between steps)",
                    "passes_per_step": passes / args.steps, "pass_ms_per_step": float(np.mean(pass_ms))},
         "e2e": {"value": e2e, "unit": "gates/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
@@ -265,9 +354,17 @@ def run_gpu(args, world, rank, local):
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
-    if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(stream, gates, budget_s=args.cpu_seconds)
     sim.Close()
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(n, stream, gates, budget_s=args.cpu_seconds)
+    if rank == 0 and not args.no_extras:
+        extras = {}
+        for name, fn in (("adjoint", extra_adjoint), ("density_matrix", extra_density), ("qaoa_batch", extra_qaoa)):
+            try:
+                extras[name] = fn()
+            except Exception as exc:  # an extra must not hide the headline line
+                extras[name] = {"error": repr(exc)}
+        line["extras"] = extras
     if rank == 0:
         print(json.dumps(line))
 
@@ -279,10 +376,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
-    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--qubits", type=int, default=28)
     ap.add_argument("--budget", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

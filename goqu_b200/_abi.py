@@ -49,6 +49,7 @@ GQ_OPT_TIMING = 4
 GQ_OPT_KERNEL_VARIANT = 5
 GQ_OPT_ADJOINT_SEGMENTS = 6
 GQ_OPT_USE_GRAPH = 7
+GQ_OPT_FUSE_DENSE = 8
 
 GQ_NOALLOC_MAX_TERMS = 2048
 

@@ -57,8 +57,22 @@ const char* gqx_last_error(void) { return g_err.c_str(); }
 // Applies ops to a host state (2^nq interleaved doubles) through the
 // scheduler and the tile-pass code, emulated on the CPU. precision GQ_C64
 // runs the float instantiation. Returns GQ_OK or an error code.
+static int emulate_sv_impl(int nq, int precision, double* state, const gq_op* ops, size_t n_ops, int tile_qubits,
+                           int budget, int fuse, int64_t* passes_out, int64_t* phases_out);
+
 int gqx_emulate_sv(int nq, int precision, double* state, const gq_op* ops, size_t n_ops, int tile_qubits,
                    int budget, int64_t* passes_out, int64_t* phases_out) {
+    return emulate_sv_impl(nq, precision, state, ops, n_ops, tile_qubits, budget, 0, passes_out, phases_out);
+}
+
+// The same with dense fusion of register-local gate runs switched on.
+int gqx_emulate_sv_fused(int nq, int precision, double* state, const gq_op* ops, size_t n_ops, int tile_qubits,
+                         int budget, int64_t* passes_out, int64_t* phases_out) {
+    return emulate_sv_impl(nq, precision, state, ops, n_ops, tile_qubits, budget, 1, passes_out, phases_out);
+}
+
+static int emulate_sv_impl(int nq, int precision, double* state, const gq_op* ops, size_t n_ops, int tile_qubits,
+                           int budget, int fuse, int64_t* passes_out, int64_t* phases_out) {
     const int nphys = nq < gq::RQ ? gq::RQ : nq;
     std::vector<gq::NGate> gates;
     for (size_t i = 0; i < n_ops; ++i) {
@@ -70,6 +84,7 @@ int gqx_emulate_sv(int nq, int precision, double* state, const gq_op* ops, size_
     if (budget > 0) opt.budget = budget;
     opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
     opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    opt.fuse_dense = fuse != 0;
     gq::Program prog;
     gq::schedule(gates, nphys, opt, prog);
     const uint64_t n = 1ull << nphys;
@@ -89,6 +104,36 @@ int gqx_emulate_sv(int nq, int precision, double* state, const gq_op* ops, size_
     }
     if (passes_out) *passes_out = (int64_t)prog.passes.size();
     if (phases_out) *phases_out = (int64_t)prog.phases.size();
+    return GQ_OK;
+}
+
+// Schedule only: out = {passes, phases, ops, sum over ops of their FMA-per-
+// amplitude cost}, for comparing scheduler settings without running anything.
+int gqx_schedule_stats(int nq, int precision, const gq_op* ops, size_t n_ops, int tile_qubits, int budget, int fuse,
+                       int64_t* out) {
+    const int nphys = nq < gq::RQ ? gq::RQ : nq;
+    std::vector<gq::NGate> gates;
+    for (size_t i = 0; i < n_ops; ++i) {
+        int rc = gq::normalize_op(ops[i], nq, gates, g_err);
+        if (rc != GQ_OK) return rc;
+    }
+    gq::SchedOptions opt;
+    if (tile_qubits > 0) opt.tile_qubits = tile_qubits;
+    if (budget > 0) opt.budget = budget;
+    opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
+    opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    opt.fuse_dense = fuse != 0;
+    gq::Program prog;
+    gq::schedule(gates, nphys, opt, prog);
+    int64_t cost = 0;
+    for (const gq::KOp& op : prog.ops) {
+        static const int c[] = {0, 8, 16, 32, 64, 1, 1, 3, 1, 4, 16};
+        cost += c[op.type] + 6;
+    }
+    out[0] = (int64_t)prog.passes.size();
+    out[1] = (int64_t)prog.phases.size();
+    out[2] = (int64_t)prog.ops.size();
+    out[3] = cost;
     return GQ_OK;
 }
 

@@ -102,7 +102,7 @@ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 // FMA-per-amplitude budget of a pass: the measured optimum of the 28-qubit
 // layered benchmark (larger budgets trade passes for compute per pass).
-constexpr int kDefaultBudget = 256;
+constexpr int kDefaultBudget = 320;
 
 // Tile-pass kernel instantiations (see kVariants* in kernels.cuh).
 using TileKernelD = void (*)(cplx<double>*, const PassDesc*, const PhaseDesc*, const KOp*, const cplx<double>*);
@@ -719,6 +719,9 @@ int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
         case GQ_OPT_ADJOINT_SEGMENTS:
             if (value < 0 || value > 4096) return fail(GQ_EINVAL, "adjoint segments out of range [0, 4096]");
             e.adj_segments = (int)value;
+            return GQ_OK;
+        case GQ_OPT_FUSE_DENSE:
+            e.opt.fuse_dense = value != 0;
             return GQ_OK;
         default:
             return fail(GQ_EINVAL, "unknown option");

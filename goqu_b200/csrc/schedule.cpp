@@ -269,6 +269,152 @@ void greedy_groups(const std::vector<NGate>& gates, std::vector<int> list, Fits 
     }
 }
 
+// ---- dense fusion inside a phase ---------------------------------------------
+// Every thread holds all 2^4 amplitudes of the phase's register qubits, so a
+// run of gates whose qubits (controls included) all lie in the register set
+// acts on them as one dense 2^k x 2^k matrix, k = qubits the run touches. The
+// run is replaced by that product when it costs fewer FMA per amplitude than
+// the separate ops plus their per-op overhead.
+constexpr int kOpOverhead = 6;
+
+Z zmul(Z a, Z b) { return Z{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+// Applies gate g to v, a state over the qubits qs (local bit p <-> qs[p]).
+void apply_small(const NGate& g, const std::vector<int>& qs, std::vector<Z>& v) {
+    auto pos = [&](int q) {
+        for (size_t p = 0; p < qs.size(); ++p)
+            if (qs[p] == q) return (int)p;
+        return -1;
+    };
+    uint32_t cm = 0;
+    for (size_t p = 0; p < qs.size(); ++p)
+        if (g.ctrl & (1ull << qs[p])) cm |= 1u << p;
+    const int t = (int)g.targets.size();
+    std::vector<int> tb(t);
+    uint32_t tm = 0;
+    for (int i = 0; i < t; ++i) {
+        tb[i] = pos(g.targets[i]);
+        tm |= 1u << tb[i];
+    }
+    const uint32_t dim = 1u << qs.size();
+    auto sub = [&](uint32_t x, uint32_t r) {  // x with the target bits set from r (first target = MSB)
+        for (int i = 0; i < t; ++i)
+            if ((r >> (t - 1 - i)) & 1) x |= 1u << tb[i];
+        return x;
+    };
+    switch (g.type) {
+        case K_PHASE:
+            for (uint32_t x = 0; x < dim; ++x)
+                if ((x & cm) == cm) v[x] = zmul(g.data[0], v[x]);
+            return;
+        case K_DIAG:
+            for (uint32_t x = 0; x < dim; ++x) {
+                if ((x & cm) != cm) continue;
+                uint32_t idx = 0;
+                for (int i = 0; i < t; ++i) idx |= ((x >> tb[i]) & 1u) << (t - 1 - i);
+                v[x] = zmul(g.data[idx], v[x]);
+            }
+            return;
+        case K_X:
+            for (uint32_t x = 0; x < dim; ++x) {
+                if ((x & cm) != cm || (x & tm)) continue;
+                const uint32_t y = x | tm;
+                const Z a0 = v[x], a1 = v[y];
+                v[x] = zmul(g.data[0], a1);
+                v[y] = zmul(g.data[1], a0);
+            }
+            return;
+        case K_SWAP:
+            for (uint32_t x = 0; x < dim; ++x) {
+                if ((x & cm) != cm) continue;
+                const uint32_t b0 = (x >> tb[0]) & 1u, b1 = (x >> tb[1]) & 1u;
+                if (b0 == 1 && b1 == 0) std::swap(v[x], v[(x & ~(1u << tb[0])) | (1u << tb[1])]);
+            }
+            return;
+        default: {  // K_U1..K_U4
+            const uint32_t td = 1u << t;
+            std::vector<Z> in(td), out(td);
+            for (uint32_t x = 0; x < dim; ++x) {
+                if ((x & cm) != cm || (x & tm)) continue;
+                for (uint32_t r = 0; r < td; ++r) in[r] = v[sub(x, r)];
+                for (uint32_t r = 0; r < td; ++r) {
+                    Z acc{0, 0};
+                    for (uint32_t c = 0; c < td; ++c) {
+                        const Z p = zmul(g.data[r * td + c], in[c]);
+                        acc.re += p.re;
+                        acc.im += p.im;
+                    }
+                    out[r] = acc;
+                }
+                for (uint32_t r = 0; r < td; ++r) v[sub(x, r)] = out[r];
+            }
+            return;
+        }
+    }
+}
+
+bool foldable(const NGate& g, uint64_t R) {
+    if (g.type == K_GRAD || g.type == K_RESET || g.type == K_NONE) return false;
+    uint64_t q = g.ctrl;
+    for (int x : g.targets) q |= 1ull << x;
+    return (q & ~R) == 0;
+}
+
+// The phase's gates, with runs of register-local gates folded into dense
+// blocks where that is cheaper. rq[k] is the qubit of register bit k.
+std::vector<NGate> fuse_phase(const std::vector<NGate>& gates, const std::vector<int>& group, uint64_t R,
+                              const int* rq, bool enable) {
+    std::vector<NGate> out;
+    std::vector<int> run;
+    auto flush = [&]() {
+        if (run.empty()) return;
+        uint64_t touched = 0;
+        int sparse = 0;
+        for (int gi : run) {
+            const NGate& g = gates[gi];
+            touched |= g.ctrl;
+            for (int x : g.targets) touched |= 1ull << x;
+            sparse += g.cost + kOpOverhead;
+        }
+        std::vector<int> qs;  // ascending register bit
+        for (int k = 0; k < RQ; ++k)
+            if (touched & (1ull << rq[k])) qs.push_back(rq[k]);
+        const int k = (int)qs.size();
+        const int dense = k ? cost_of((KType)(K_U1 + k - 1)) + kOpOverhead : 1 << 30;
+        if (!enable || run.size() < 2 || dense >= sparse) {
+            for (int gi : run) out.push_back(gates[gi]);
+            run.clear();
+            return;
+        }
+        const uint32_t dim = 1u << k;
+        std::vector<Z> B(dim * dim, Z{0, 0});  // column c = image of basis state c
+        for (uint32_t c = 0; c < dim; ++c) {
+            std::vector<Z> v(dim, Z{0, 0});
+            v[c] = Z{1, 0};
+            for (int gi : run) apply_small(gates[gi], qs, v);
+            for (uint32_t r = 0; r < dim; ++r) B[r * dim + c] = v[r];
+        }
+        NGate d;
+        d.type = (KType)(K_U1 + k - 1);
+        for (int p = k - 1; p >= 0; --p) d.targets.push_back(qs[p]);  // MSB first: local bit p <-> qs[p]
+        d.data = B;
+        d.src = gates[run.front()].src;
+        finish(d);
+        out.push_back(d);
+        run.clear();
+    };
+    for (int gi : group) {
+        if (foldable(gates[gi], R)) {
+            run.push_back(gi);
+        } else {
+            flush();
+            out.push_back(gates[gi]);
+        }
+    }
+    flush();
+    return out;
+}
+
 int rank_gf2(std::vector<uint32_t> v) {
     int r = 0;
     for (int bit = 31; bit >= 0; --bit) {
@@ -459,8 +605,8 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                 return -1;
             };
             ph.op_begin = (int32_t)prog.ops.size();
-            for (int gi : groups[p]) {
-                const NGate& g = gates[gi];
+            const std::vector<NGate> fused = fuse_phase(gates, groups[p], R, rq, opt.fuse_dense);
+            for (const NGate& g : fused) {
                 KOp op;
                 std::memset(&op, 0, sizeof(op));
                 op.type = g.type;

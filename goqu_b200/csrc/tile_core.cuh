@@ -222,14 +222,28 @@ GQ_HD void k_u3(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
 // 16x16 on all register bits. The outputs go straight to the thread's own
 // shared-memory slots (so only the 16 inputs stay live in registers) and are
 // read back afterwards; no other thread touches those slots in this phase.
+// 16x16 on all register bits. Four output rows at a time, each summed in two
+// interleaved partial sums (16 independent FMA chains); the outputs go to the
+// thread's own shared-memory slots, so only the 16 inputs stay in registers,
+// and are read back at the end (no other thread touches those slots in this
+// phase).
 template <class T>
 GQ_HD void k_u4(cplx<T> (&a)[NREG], const cplx<T>* m, cplx<T>* sm, uint32_t sbase, const uint32_t* rslot) {
 #pragma unroll 1
-    for (int r = 0; r < NREG; ++r) {
-        cplx<T> o = {T(0), T(0)};
+    for (int r0 = 0; r0 < NREG; r0 += 4) {
+        cplx<T> o[4], e[4];
 #pragma unroll
-        for (int c = 0; c < NREG; ++c) o = cfma(ldc_v(m, r * NREG + c), a[c], o);
-        sm[sbase ^ rslot[r]] = o;
+        for (int q = 0; q < 4; ++q) o[q] = e[q] = cplx<T>{T(0), T(0)};
+#pragma unroll
+        for (int c = 0; c < NREG; c += 2) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                o[q] = cfma(ldc_v(m, (r0 + q) * NREG + c), a[c], o[q]);
+                e[q] = cfma(ldc_v(m, (r0 + q) * NREG + c + 1), a[c + 1], e[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sm[sbase ^ rslot[r0 + q]] = cplx<T>{o[q].x + e[q].x, o[q].y + e[q].y};
     }
 #pragma unroll
     for (int r = 0; r < NREG; ++r) a[r] = sm[sbase ^ rslot[r]];

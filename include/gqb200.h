@@ -177,6 +177,7 @@ int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 #define GQ_OPT_KERNEL_VARIANT 5 /* tile-pass launch shape (0..3); sets the tile size */
 #define GQ_OPT_ADJOINT_SEGMENTS 6 /* adjoint: forward checkpoints (0 = automatic, 1 = none) */
 #define GQ_OPT_USE_GRAPH 7      /* batches: capture launches in a CUDA graph (default 1) */
+#define GQ_OPT_FUSE_DENSE 8     /* 1: fold register-local gate runs into dense blocks (default 0) */
 int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
 
 /* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */

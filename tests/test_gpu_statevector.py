@@ -234,3 +234,13 @@ def test_large_state_properties_26q():
     sim.Apply(inv)
     a0 = sim.StateVector()[0]
     assert abs(a0 - 1.0) < 1e-10
+
+
+@pytest.mark.parametrize("n,seed", [(9, 71), (14, 72)])
+def test_dense_fusion_option_matches_oracle(n, seed):
+    c = random_circuit(n, 150, seed, allow_reset=True)
+    want = orc.sv_evolve(encode.statevector_ops(c))
+    sim = statevector.New(n)
+    sim.set_option(_abi.GQ_OPT_FUSE_DENSE, 1)
+    sim.Evolve(c)
+    assert np.max(np.abs(sim.StateVector() - want)) < TOL128

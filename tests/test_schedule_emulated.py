@@ -195,3 +195,20 @@ def test_emulated_adjoint_general_gates(emu):
         fd[i] = (_oracle_energy(c, names, xp, h) - _oracle_energy(c, names, xm, h)) / 2e-5
     assert abs(e - _oracle_energy(c, names, x, h)) < 1e-12
     np.testing.assert_allclose(g, fd, atol=1e-7, rtol=0)
+
+
+@pytest.mark.parametrize("n,seed,tile", [(5, 31, 0), (8, 32, 7), (11, 33, 9), (13, 34, 11)])
+def test_emulated_dense_fusion_matches_oracle(emu, n, seed, tile):
+    # GQ_OPT_FUSE_DENSE: runs of register-local gates folded into dense blocks
+    c = random_circuit(n, 120, seed, allow_reset=True)
+    ops = encode.statevector_ops(c)
+    want = orc.sv_evolve(ops)
+    st = np.zeros(1 << n, dtype=np.complex128)
+    st[0] = 1
+    emu.gqx_emulate_sv_fused.restype = ctypes.c_int
+    emu.gqx_emulate_sv_fused.argtypes = emu.gqx_emulate_sv.argtypes
+    p, q = ctypes.c_int64(), ctypes.c_int64()
+    rc = emu.gqx_emulate_sv_fused(n, 0, st.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                  ops.ptr(), len(ops), tile, 400, ctypes.byref(p), ctypes.byref(q))
+    assert rc == 0
+    np.testing.assert_allclose(st, want, atol=1e-12, rtol=0)
