@@ -200,6 +200,7 @@ def extra_adjoint():
     x = np.random.default_rng(20).uniform(0, 2 * np.pi, len(names))
     ev = gradient.AdjointEvaluator(c, h, names)
     ev.sim.set_option(_abi.GQ_OPT_TIMING, 1)
+    ev.sim.set_option(_abi.GQ_OPT_JIT, 2)
     for _ in range(3):
         ev(x)
     dev, t0 = [], time.perf_counter()
@@ -209,6 +210,7 @@ def extra_adjoint():
     wall = (time.perf_counter() - t0) / 10
     f = gradient.CostFunc(c, h, names)
     f.sim.set_option(_abi.GQ_OPT_TIMING, 1)
+    f.sim.set_option(_abi.GQ_OPT_JIT, 2)
     f(x)
     g_ps = np.empty(len(names))
     ps_dev, t1 = 0.0, time.perf_counter()
@@ -237,6 +239,7 @@ def extra_density():
     c, nm = workloads.noisy_brickwork(12, layers=30, seed=12)
     dm = densitymatrix.New(12).WithNoise(nm)
     dm.set_option(_abi.GQ_OPT_TIMING, 1)
+    dm.set_option(_abi.GQ_OPT_JIT, 2)
     s = encode.density_ops(c, nm)
     lib = _abi.lib()
     for _ in range(2):
@@ -283,6 +286,7 @@ def run_gpu(args, world, rank, local):
     c, stream, gates = build_workload(n)
     sim = statevector.New(n, _abi.GQ_C64 if args.precision == "c64" else _abi.GQ_C128)
     sim.set_option(_abi.GQ_OPT_TIMING, 1)
+    sim.set_option(_abi.GQ_OPT_JIT, args.jit)
     if args.budget:
         sim.set_option(_abi.GQ_OPT_PASS_BUDGET, args.budget)
     lib = _abi.lib()
@@ -292,10 +296,14 @@ def run_gpu(args, world, rank, local):
     idx_p = idx.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
 
     # ---- device-resident throughput: Evolve only, CUDA events on the engine stream
-    for _ in range(args.warmup):
+    # (the first warm-up call compiles the specialised pass kernels)
+    t_first = time.perf_counter()
+    for w in range(args.warmup):
         sim.evolve_ops(stream)
+        if w == 0:
+            t_first = time.perf_counter() - t_first
     barrier(world)
-    step_ms, pass_ms, launches, passes = [], [], 0, 0
+    step_ms, pass_ms, launches, passes, jit_passes = [], [], 0, 0, 0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             sim.evolve_ops(stream)
@@ -304,6 +312,7 @@ def run_gpu(args, world, rank, local):
             pass_ms.append(st["pass_ms"])
             launches += st["kernel_launches"]
             passes += st["passes"]
+            jit_passes += st["jit_passes"]
     barrier(world)
     total_ms = max_over_ranks(float(np.sum(step_ms)), world)
     value = world * gates * args.steps / (total_ms / 1000.0)
@@ -352,6 +361,8 @@ def run_gpu(args, world, rank, local):
                      "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": per_launch_ms},
         "gpu_launches": launches,
+        "jit": {"mode": args.jit, "passes_specialised_per_step": jit_passes / args.steps,
+                "first_call_s": t_first, "compile_ms_total": sim.stats()["jit_compile_ms"]},
         "clocks": clk.summary(),
     }
     sim.Close()
@@ -381,6 +392,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--jit", type=int, choices=[0, 1, 2], default=2,
+                    help="specialised pass kernels: 0 off, 1 when compiled, 2 wait for them (default)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

@@ -50,6 +50,8 @@ GQ_OPT_KERNEL_VARIANT = 5
 GQ_OPT_ADJOINT_SEGMENTS = 6
 GQ_OPT_USE_GRAPH = 7
 GQ_OPT_FUSE_DENSE = 8
+GQ_OPT_JIT = 9
+GQ_OPT_JIT_MIN_QUBITS = 10
 
 GQ_NOALLOC_MAX_TERMS = 2048
 
@@ -90,6 +92,8 @@ class gq_stats(ctypes.Structure):
         ("pass_ms", ctypes.c_double),
         ("h2d_bytes", ctypes.c_int64),
         ("d2h_bytes", ctypes.c_int64),
+        ("jit_passes", ctypes.c_int64),
+        ("jit_compile_ms", ctypes.c_double),
     ]
 
 

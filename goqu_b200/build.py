@@ -17,9 +17,25 @@ NVCC_FLAGS = [
     "-shared",
 ]
 
-ENGINE_SOURCES = ["engine.cu", "noalloc.cu", "schedule.cpp"]
-EMULATOR_SOURCES = ["emulate.cpp", "schedule.cpp"]
-HEADERS = ["tile_core.cuh", "kernels.cuh", "schedule.hpp", os.path.join("..", "..", "include", "gqb200.h")]
+ENGINE_SOURCES = ["engine.cu", "noalloc.cu", "schedule.cpp", "jit.cpp", "jit_gen.cpp"]
+EMULATOR_SOURCES = ["emulate.cpp", "schedule.cpp", "jit_gen.cpp"]
+HEADERS = ["tile_core.cuh", "kernels.cuh", "schedule.hpp", "jit.hpp", os.path.join("..", "..", "include", "gqb200.h")]
+# tile_core.cuh as a C++ string literal, compiled into the engine for the
+# run-time specialised pass kernels (generated; not committed).
+TILE_CORE_INC = os.path.join(CSRC, "tile_core_src.inc")
+
+
+def write_tile_core_inc():
+    with open(os.path.join(CSRC, "tile_core.cuh")) as f:
+        text = f.read()
+    assert ")GQSRC\"" not in text
+    body = 'R"GQSRC(' + text + ')GQSRC"\n'
+    if os.path.exists(TILE_CORE_INC):
+        with open(TILE_CORE_INC) as f:
+            if f.read() == body:
+                return
+    with open(TILE_CORE_INC, "w") as f:
+        f.write(body)
 
 
 def _stale(target, sources):
@@ -35,9 +51,10 @@ def nvcc():
 
 
 def build_engine(force=False, verbose=False):
+    write_tile_core_inc()
     if not force and not _stale(ENGINE, ENGINE_SOURCES):
         return ENGINE
-    cmd = [nvcc()] + NVCC_FLAGS + [os.path.join(CSRC, s) for s in ENGINE_SOURCES] + ["-o", ENGINE]
+    cmd = [nvcc()] + NVCC_FLAGS + [os.path.join(CSRC, s) for s in ENGINE_SOURCES] + ["-o", ENGINE, "-ldl"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
@@ -45,10 +62,12 @@ def build_engine(force=False, verbose=False):
 
 
 def build_emulator(force=False):
+    write_tile_core_inc()
     if not force and not _stale(EMULATOR, EMULATOR_SOURCES):
         return EMULATOR
-    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-Wno-unknown-pragmas", "-x", "c++"]
-    cmd += [os.path.join(CSRC, s) for s in EMULATOR_SOURCES] + ["-o", EMULATOR]
+    inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-Wno-unknown-pragmas", "-I", inc, "-x", "c++"]
+    cmd += [os.path.join(CSRC, s) for s in EMULATOR_SOURCES] + ["-o", EMULATOR, "-ldl"]
     subprocess.run(cmd, check=True)
     return EMULATOR
 

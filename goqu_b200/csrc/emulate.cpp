@@ -9,6 +9,9 @@
 #include <string>
 #include <vector>
 
+#include <set>
+
+#include "jit.hpp"
 #include "schedule.hpp"
 #include "tile_core.cuh"
 
@@ -229,6 +232,63 @@ int gqx_emulate_adjoint(int nq, const gq_op* ops, size_t n_ops, const gq_pauli_t
     }
     for (size_t i = 0; i < n_params; ++i) grad_out[i] = grad[i];
     if (energy_out) *energy_out = energy;
+    return GQ_OK;
+}
+
+// Specialised pass kernels without a device: schedules `ops` (a statevector
+// program, or with dm != 0 the density-matrix program of an n-qubit rho) the
+// way the engine does, generates the kernel text of every pass and compiles
+// up to `max_compile` distinct texts with NVRTC for sm_100a.
+// out: [passes, passes with a kernel text, distinct texts, compiled, compiled
+// with register spills]. GQ_EUNSUPPORTED when libnvrtc cannot be loaded.
+int gqx_jit_check(int nq, int precision, const gq_op* ops, size_t n_ops, int tile_qubits, int budget, int dm,
+                  int max_compile, int64_t* out) {
+    if (!gq::jit_available()) {
+        g_err = "libnvrtc not found";
+        return GQ_EUNSUPPORTED;
+    }
+    std::vector<gq::NGate> gates;
+    int nphys;
+    if (dm) {
+        nphys = 2 * nq < gq::RQ ? gq::RQ : 2 * nq;
+        const int rc = gq::dm_gates(nq, ops, n_ops, gates, g_err);
+        if (rc != GQ_OK) return rc;
+    } else {
+        nphys = nq < gq::RQ ? gq::RQ : nq;
+        for (size_t i = 0; i < n_ops; ++i) {
+            const int rc = gq::normalize_op(ops[i], nphys, gates, g_err);
+            if (rc != GQ_OK) return rc;
+        }
+    }
+    gq::SchedOptions opt;
+    opt.tile_qubits = tile_qubits > 0 ? tile_qubits : 11;  // the engine's default launch shapes: 128 threads
+    opt.budget = budget > 0 ? budget : 320;
+    opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
+    opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    gq::Program prog;
+    gq::schedule(gates, nphys, opt, prog);
+    std::set<std::string> texts;
+    int64_t planned = 0, compiled = 0, spills = 0;
+    for (size_t i = 0; i < prog.passes.size(); ++i) {
+        gq::JitPlan pl;
+        const int threads = 1 << (prog.passes[i].m - gq::RQ);
+        if (!gq::jit_plan(prog, i, precision == GQ_C64, threads, precision == GQ_C64 ? 4 : 3, pl)) continue;
+        ++planned;
+        if (!texts.insert(pl.source).second || compiled >= max_compile) continue;
+        std::string log;
+        const std::string err = gq::jit_compile_only(pl.source, nullptr, &log);
+        if (!err.empty()) {
+            g_err = err.substr(0, 4000);
+            return GQ_ECUDA;
+        }
+        ++compiled;
+        if (log.find(" 0 bytes spill stores") == std::string::npos) ++spills;
+    }
+    out[0] = (int64_t)prog.passes.size();
+    out[1] = planned;
+    out[2] = (int64_t)texts.size();
+    out[3] = compiled;
+    out[4] = spills;
     return GQ_OK;
 }
 

@@ -16,6 +16,7 @@
 
 #include "../../include/gqb200.h"
 #include "kernels.cuh"
+#include "jit.hpp"
 #include "schedule.hpp"
 
 using namespace gq;
@@ -194,6 +195,8 @@ struct Engine {
     gq_stats stats{};
 
     int variant = 0;
+    int jit_mode = 1;         // GQ_OPT_JIT
+    int jit_min_qubits = 20;  // GQ_OPT_JIT_MIN_QUBITS
     size_t amp_bytes() const { return prec == GQ_C64 ? 8 : 16; }
     int max_tile() const {
         return RQ + log2i(prec == GQ_C64 ? kVariantsC64[variant].threads : kVariantsC128[variant].threads);
@@ -291,17 +294,57 @@ struct Engine {
         for (size_t i = 0; i < pr.pool.size(); ++i) pool[i] = {(T)pr.pool[i].re, (T)pr.pool[i].im};
         GQ_TRY(upload(prog, total));
         char* d = (char*)prog.p;
+        // Specialised kernels for the passes whose compilation has finished
+        // (or, with GQ_OPT_JIT = 2, once it has); the others run interpreted.
+        const size_t np = pr.passes.size();
+        std::vector<const void*> jfn(np, nullptr);
+        std::vector<JitPlan> plans;
+        if (jit_mode != 0 && nphys >= jit_min_qubits && jit_available()) {
+            plans.resize(np);
+            const int minb = prec == GQ_C64 ? kVariantsC64[variant].min_blocks : kVariantsC128[variant].min_blocks;
+            std::vector<char> planned(np, 0);
+            for (size_t i = 0; i < np; ++i) {
+                const PassDesc& pd = pr.passes[i];
+                if (!jit_plan(pr, i, prec == GQ_C64, 1 << (pd.m - RQ), minb, plans[i])) continue;
+                planned[i] = 1;
+                jit_lookup(plans[i].source, sizeof(cplx<T>) << pd.m, true, &jfn[i]);
+            }
+            if (jit_mode == 2) {
+                jit_wait(600000.0);
+                for (size_t i = 0; i < np; ++i)
+                    if (planned[i] && !jfn[i])
+                        jit_lookup(plans[i].source, sizeof(cplx<T>) << pr.passes[i].m, false, &jfn[i]);
+            }
+        }
         if (timing) GQ_CUDA(cudaEventRecord(ev_pass0, stream));
-        for (size_t i = 0; i < pr.passes.size(); ++i) {
+        std::vector<cplx<T>> pblock;
+        int64_t jitted = 0;
+        for (size_t i = 0; i < np; ++i) {
             const PassDesc& pd = pr.passes[i];
             const unsigned threads = 1u << (pd.m - RQ);
             const size_t smem = sizeof(cplx<T>) << pd.m;
             const unsigned grid = 1u << pd.n_outer;
+            if (jfn[i]) {
+                const JitPlan& pl = plans[i];
+                pblock.assign(pl.n_param, cplx<T>{T(0), T(0)});
+                size_t k = 0;
+                for (const auto& c : pl.copies)
+                    for (uint32_t j = 0; j < c.second; ++j, ++k)
+                        pblock[k] = {(T)pr.pool[c.first + j].re, (T)pr.pool[c.first + j].im};
+                cplx<T>* stp = (cplx<T>*)state.p;
+                const cplx<T>* poolp = (const cplx<T>*)(d + o_pool);
+                const PhaseDesc* php = (const PhaseDesc*)(d + o_phase);
+                void* args[4] = {&stp, pblock.data(), &poolp, &php};
+                GQ_CUDA(cudaLaunchKernel(jfn[i], dim3(grid), dim3(threads), args, smem, stream));
+                ++jitted;
+                continue;
+            }
             TileTable<T>::get(variant)<<<grid, threads, smem, stream>>>(
                 (cplx<T>*)state.p, (const PassDesc*)(d + o_pass) + i, (const PhaseDesc*)(d + o_phase),
                 (const KOp*)(d + o_ops), (const cplx<T>*)(d + o_pool));
         }
         GQ_CUDA(cudaGetLastError());
+        stats.jit_passes += jitted;
         if (timing) {
             GQ_CUDA(cudaEventRecord(ev_pass1, stream));
             pass_timed = true;
@@ -379,6 +422,23 @@ struct Engine {
         schedule(gates, nphys, opt, pr);
         stats.gates_in += pr.gates;
         return prec == GQ_C64 ? run_program_t<float>(pr) : run_program_t<double>(pr);
+    }
+
+    int set_jit_option(int key, int64_t value) {
+        if (key == GQ_OPT_JIT) {
+            if (value < 0 || value > 2) return fail(GQ_EINVAL, "jit mode out of range [0, 2]");
+            jit_mode = (int)value;
+        } else {
+            if (value < 0 || value > 64) return fail(GQ_EINVAL, "jit min qubits out of range [0, 64]");
+            jit_min_qubits = (int)value;
+        }
+        return GQ_OK;
+    }
+
+    gq_stats get_stats() const {
+        gq_stats s = stats;
+        jit_counters(&s.jit_compile_ms, nullptr, nullptr);
+        return s;
     }
 
     void clear_stats() {
@@ -687,7 +747,7 @@ int gq_sv_expect_z_mask(gq_sv* sv, uint64_t mask, double* out) {
 
 int gq_sv_stats(const gq_sv* sv, gq_stats* out) {
     if (!sv || !out) return fail(GQ_EINVAL, "null argument");
-    *out = sv->e.stats;
+    *out = sv->e.get_stats();
     return GQ_OK;
 }
 
@@ -723,6 +783,9 @@ int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
         case GQ_OPT_FUSE_DENSE:
             e.opt.fuse_dense = value != 0;
             return GQ_OK;
+        case GQ_OPT_JIT:
+        case GQ_OPT_JIT_MIN_QUBITS:
+            return e.set_jit_option(key, value);
         default:
             return fail(GQ_EINVAL, "unknown option");
     }
@@ -887,6 +950,7 @@ int gq_dm_set_option(gq_dm* dm, int key, int64_t value) {
         dm->e.opt.tile_qubits = dm->e.max_tile();
         return GQ_OK;
     }
+    if (key == GQ_OPT_JIT || key == GQ_OPT_JIT_MIN_QUBITS) return dm->e.set_jit_option(key, value);
     return fail(GQ_EINVAL, "unknown option");
 }
 
@@ -1001,7 +1065,7 @@ int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* 
 
 int gq_dm_stats(const gq_dm* dm, gq_stats* out) {
     if (!dm || !out) return fail(GQ_EINVAL, "null argument");
-    *out = dm->e.stats;
+    *out = dm->e.get_stats();
     return GQ_OK;
 }
 
@@ -1473,7 +1537,7 @@ int gq_batch_set_option(gq_batch* b, int key, int64_t value) {
 
 int gq_batch_stats(const gq_batch* b, gq_stats* out) {
     if (!b || !out) return fail(GQ_EINVAL, "null argument");
-    *out = b->e.stats;
+    *out = b->e.get_stats();
     return GQ_OK;
 }
 

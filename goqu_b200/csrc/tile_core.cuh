@@ -12,7 +12,9 @@
 // scheduler emits, so the code below is pure index arithmetic plus complex
 // FMAs and is compiled both for sm_100a and for the host emulator.
 #pragma once
+#if !defined(__CUDACC_RTC__)
 #include <stdint.h>
+#endif
 
 #if defined(__CUDACC__)
 #define GQ_HD __host__ __device__ __forceinline__
@@ -140,6 +142,22 @@ GQ_HD cplx<float> ldc_v(const cplx<float>* p, uint32_t i) {
 #endif
 }
 
+// Matrix held in kernel parameter space (the specialised pass kernels pass
+// each pass's matrices by value): indexed with compile-time offsets, so the
+// entries become constant-bank operands.
+template <class T>
+struct PMat {
+    const cplx<T>* p;
+};
+template <class T>
+GQ_HD cplx<T> ldc(PMat<T> m, uint32_t i) {
+    return m.p[i];
+}
+template <class T>
+GQ_HD cplx<T> ldc_v(PMat<T> m, uint32_t i) {
+    return m.p[i];
+}
+
 GQ_HD uint64_t pext64(uint64_t v, uint64_t mask) {
     uint64_t r = 0;
     int k = 0;
@@ -158,8 +176,8 @@ GQ_HD uint64_t pext64(uint64_t v, uint64_t mask) {
 
 // ---- register-level gate bodies (S* are register bits, compile-time) -------
 
-template <class T, int S, bool C>
-GQ_HD void k_u1(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
+template <class T, int S, bool C, class MP>
+GQ_HD void k_u1(cplx<T> (&a)[NREG], MP m, uint32_t creg) {
     const cplx<T> m0 = ldc(m, 0), m1 = ldc(m, 1), m2 = ldc(m, 2), m3 = ldc(m, 3);
 #pragma unroll
     for (int j = 0; j < NREG; ++j) {
@@ -176,8 +194,8 @@ GQ_HD void k_u1(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
     }
 }
 
-template <class T, int S0, int S1, bool C>
-GQ_HD void k_u2(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
+template <class T, int S0, int S1, bool C, class MP>
+GQ_HD void k_u2(cplx<T> (&a)[NREG], MP m, uint32_t creg) {
 #pragma unroll
     for (int j = 0; j < NREG; ++j) {
         if (j & ((1 << S0) | (1 << S1))) continue;
@@ -196,8 +214,8 @@ GQ_HD void k_u2(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
     }
 }
 
-template <class T, int S0, int S1, int S2>
-GQ_HD void k_u3(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
+template <class T, int S0, int S1, int S2, class MP>
+GQ_HD void k_u3(cplx<T> (&a)[NREG], MP m, uint32_t creg) {
 #pragma unroll
     for (int j = 0; j < NREG; ++j) {
         if (j & ((1 << S0) | (1 << S1) | (1 << S2))) continue;
@@ -219,16 +237,13 @@ GQ_HD void k_u3(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg) {
     }
 }
 
-// 16x16 on all register bits. The outputs go straight to the thread's own
-// shared-memory slots (so only the 16 inputs stay live in registers) and are
-// read back afterwards; no other thread touches those slots in this phase.
 // 16x16 on all register bits. Four output rows at a time, each summed in two
 // interleaved partial sums (16 independent FMA chains); the outputs go to the
 // thread's own shared-memory slots, so only the 16 inputs stay in registers,
 // and are read back at the end (no other thread touches those slots in this
 // phase).
-template <class T>
-GQ_HD void k_u4(cplx<T> (&a)[NREG], const cplx<T>* m, cplx<T>* sm, uint32_t sbase, const uint32_t* rslot) {
+template <class T, class MP>
+GQ_HD void k_u4(cplx<T> (&a)[NREG], MP m, cplx<T>* sm, uint32_t sbase, const uint32_t* rslot) {
 #pragma unroll 1
     for (int r0 = 0; r0 < NREG; r0 += 4) {
         cplx<T> o[4], e[4];
@@ -249,8 +264,8 @@ GQ_HD void k_u4(cplx<T> (&a)[NREG], const cplx<T>* m, cplx<T>* sm, uint32_t sbas
     for (int r = 0; r < NREG; ++r) a[r] = sm[sbase ^ rslot[r]];
 }
 
-template <class T, int S, bool C>
-GQ_HD void k_x(cplx<T> (&a)[NREG], const cplx<T>* m, uint32_t creg, bool pure) {
+template <class T, int S, bool C, class MP>
+GQ_HD void k_x(cplx<T> (&a)[NREG], MP m, uint32_t creg, bool pure) {
     if (pure) {
 #pragma unroll
         for (int j = 0; j < NREG; ++j) {
@@ -303,11 +318,11 @@ GQ_HD void k_reset(cplx<T> (&a)[NREG]) {
     }
 }
 
+// Diagonal with its table index's global part `hi` already extracted.
 template <class T>
-GQ_HD void k_diag(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* d, uint64_t g0) {
-    const uint32_t hi = (uint32_t)(pext64(g0, op.dmask) << op.nreg);
-    const uint32_t creg = op.creg;
-    if (op.nreg == 0) {
+GQ_HD void k_diag_hi(cplx<T> (&a)[NREG], const cplx<T>* d, uint32_t hi, uint32_t nreg, uint32_t creg,
+                     uint64_t ridx) {
+    if (nreg == 0) {
         const cplx<T> f = ldc(d, hi);
         if (f.x == T(1) && f.y == T(0)) return;
 #pragma unroll
@@ -318,9 +333,14 @@ GQ_HD void k_diag(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* d, uint64_t 
 #pragma unroll
     for (int j = 0; j < NREG; ++j) {
         if ((j & creg) != creg) continue;
-        const uint32_t idx = hi | (uint32_t)((op.ridx >> (4 * j)) & 15u);
+        const uint32_t idx = hi | (uint32_t)((ridx >> (4 * j)) & 15u);
         a[j] = cmul(ldc(d, idx), a[j]);
     }
+}
+
+template <class T>
+GQ_HD void k_diag(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* d, uint64_t g0) {
+    k_diag_hi<T>(a, d, (uint32_t)(pext64(g0, op.dmask) << op.nreg), op.nreg, op.creg, op.ridx);
 }
 
 template <class T>

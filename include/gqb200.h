@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define GQ_ABI_VERSION 1
+#define GQ_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define GQ_OK 0
@@ -115,6 +115,8 @@ typedef struct gq_stats {
     double pass_ms;          /* device time of its tile passes alone                */
     int64_t h2d_bytes;       /* host->device bytes the last call copied (program, inputs) */
     int64_t d2h_bytes;       /* device->host bytes the last call copied (results)   */
+    int64_t jit_passes;      /* passes of the last call run by a specialised kernel */
+    double jit_compile_ms;   /* process total: milliseconds spent compiling them    */
 } gq_stats;
 
 /* ---- library ------------------------------------------------------------- */
@@ -178,6 +180,11 @@ int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 #define GQ_OPT_ADJOINT_SEGMENTS 6 /* adjoint: forward checkpoints (0 = automatic, 1 = none) */
 #define GQ_OPT_USE_GRAPH 7      /* batches: capture launches in a CUDA graph (default 1) */
 #define GQ_OPT_FUSE_DENSE 8     /* 1: fold register-local gate runs into dense blocks (default 0) */
+/* Specialised pass kernels (NVRTC, compiled on background threads and cached
+ * per process by pass structure): 0 off, 1 use when compiled and run the
+ * interpreted kernel until then (default), 2 wait for the compilation. */
+#define GQ_OPT_JIT 9
+#define GQ_OPT_JIT_MIN_QUBITS 10 /* smallest state (physical qubits) that uses them (default 20) */
 int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
 
 /* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */
