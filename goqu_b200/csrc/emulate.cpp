@@ -5,6 +5,10 @@
 // threads executed one after another, so that scheduling, swizzle and index
 // tables can be checked against the oracle without a GPU. It is built into
 // libgqb200_emu.so, which only the tests load.
+#include <dlfcn.h>
+
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -20,35 +24,105 @@ namespace {
 thread_local std::string g_err;
 
 template <class T>
-void run_program(std::vector<gq::cplx<T>>& st, const gq::Program& prog) {
-    std::vector<gq::cplx<T>> pool(prog.pool.size());
-    for (size_t i = 0; i < pool.size(); ++i) pool[i] = {(T)prog.pool[i].re, (T)prog.pool[i].im};
-    for (const gq::PassDesc& pd : prog.passes) {
-        const int m = pd.m;
-        const uint32_t tpb = 1u << (m - gq::RQ);
-        const uint64_t n_cta = 1ull << pd.n_outer;
-        std::vector<gq::cplx<T>> sm(1u << m);
-        for (uint64_t cta = 0; cta < n_cta; ++cta) {
-            const uint64_t base = gq::cta_base(pd, cta);
-            for (uint32_t lin = 0; lin < (1u << m); ++lin) {
-                uint64_t goff;
-                uint32_t slot;
-                gq::linear_slot(pd, lin, goff, slot);
-                sm[slot] = st[base | goff];
-            }
-            for (int p = 0; p < pd.n_phases; ++p) {
-                const gq::PhaseDesc& ph = prog.phases[pd.phase0 + p];
-                for (uint32_t t = 0; t < tpb; ++t)
-                    gq::run_phase<T>(sm.data(), ph, prog.ops.data(), pool.data(), t, base);
-            }
-            for (uint32_t lin = 0; lin < (1u << m); ++lin) {
-                uint64_t goff;
-                uint32_t slot;
-                gq::linear_slot(pd, lin, goff, slot);
-                st[base | goff] = sm[slot];
-            }
+void run_pass(std::vector<gq::cplx<T>>& st, const gq::Program& prog, const std::vector<gq::cplx<T>>& pool, size_t pi) {
+    const gq::PassDesc& pd = prog.passes[pi];
+    const int m = pd.m;
+    const uint32_t tpb = 1u << (m - gq::RQ);
+    const uint64_t n_cta = 1ull << pd.n_outer;
+    std::vector<gq::cplx<T>> sm(1u << m);
+    for (uint64_t cta = 0; cta < n_cta; ++cta) {
+        const uint64_t base = gq::cta_base(pd, cta);
+        for (uint32_t lin = 0; lin < (1u << m); ++lin) {
+            uint64_t goff;
+            uint32_t slot;
+            gq::linear_slot(pd, lin, goff, slot);
+            sm[slot] = st[base | goff];
+        }
+        for (int p = 0; p < pd.n_phases; ++p) {
+            const gq::PhaseDesc& ph = prog.phases[pd.phase0 + p];
+            for (uint32_t t = 0; t < tpb; ++t) gq::run_phase<T>(sm.data(), ph, prog.ops.data(), pool.data(), t, base);
+        }
+        for (uint32_t lin = 0; lin < (1u << m); ++lin) {
+            uint64_t goff;
+            uint32_t slot;
+            gq::linear_slot(pd, lin, goff, slot);
+            st[base | goff] = sm[slot];
         }
     }
+}
+
+template <class T>
+std::vector<gq::cplx<T>> pool_of(const gq::Program& prog) {
+    std::vector<gq::cplx<T>> pool(prog.pool.size());
+    for (size_t i = 0; i < pool.size(); ++i) pool[i] = {(T)prog.pool[i].re, (T)prog.pool[i].im};
+    return pool;
+}
+
+template <class T>
+void run_program(std::vector<gq::cplx<T>>& st, const gq::Program& prog) {
+    const std::vector<gq::cplx<T>> pool = pool_of<T>(prog);
+    for (size_t i = 0; i < prog.passes.size(); ++i) run_pass<T>(st, prog, pool, i);
+}
+
+// Runs a program through the specialised kernels' host form: every pass's
+// generated code is compiled with the host compiler into one library and
+// called with its packed parameter block; passes without a plan or whose
+// block does not pack run through the emulated interpreter.
+template <class T>
+int run_program_jit(std::vector<gq::cplx<T>>& st, const gq::Program& prog, bool c64, const char* csrc,
+                    const char* work, int64_t* jitted) {
+    std::vector<gq::JitPlan> plans(prog.passes.size());
+    std::vector<char> ok(prog.passes.size(), 0);
+    std::string src;
+    for (size_t i = 0; i < prog.passes.size(); ++i) {
+        const int threads = 1 << (prog.passes[i].m - gq::RQ);
+        if (!gq::jit_plan(prog, i, c64, threads, 1, plans[i], true)) continue;
+        ok[i] = 1;
+        src += plans[i].host_source;
+    }
+    const std::string dir = work;
+    const std::string cpp = dir + "/gqj_host.cpp", so = dir + "/gqj_host.so";
+    {
+        FILE* f = std::fopen(cpp.c_str(), "w");
+        if (!f) {
+            g_err = "cannot write " + cpp;
+            return GQ_EINVAL;
+        }
+        std::fwrite(src.data(), 1, src.size(), f);
+        std::fclose(f);
+    }
+    const std::string cmd = "g++ -O1 -std=c++17 -shared -fPIC -w -I'" + std::string(csrc) + "' '" + cpp + "' -o '" +
+                            so + "' 2>'" + dir + "/gqj_host.log'";
+    if (std::system(cmd.c_str()) != 0) {
+        g_err = "host compile of the generated passes failed (" + dir + "/gqj_host.log)";
+        return GQ_EINVAL;
+    }
+    void* h = dlopen(so.c_str(), RTLD_NOW | RTLD_LOCAL);
+    if (!h) {
+        g_err = dlerror();
+        return GQ_EINVAL;
+    }
+    typedef void (*PassFn)(gq::cplx<T>*, const gq::cplx<T>*, const gq::cplx<T>*, const gq::PhaseDesc*, gq::cplx<T>*);
+    const std::vector<gq::cplx<T>> pool = pool_of<T>(prog);
+    *jitted = 0;
+    for (size_t i = 0; i < prog.passes.size(); ++i) {
+        std::vector<gq::cplx<T>> block;
+        PassFn fn = nullptr;
+        if (ok[i]) {
+            block.resize(plans[i].n_param);
+            if (gq::jit_pack(prog, plans[i], c64, block.data()))
+                fn = (PassFn)dlsym(h, ("gqj_host_" + std::to_string(i)).c_str());
+        }
+        if (!fn) {
+            run_pass<T>(st, prog, pool, i);
+            continue;
+        }
+        std::vector<gq::cplx<T>> sm(1u << prog.passes[i].m);
+        fn(st.data(), block.data(), pool.data(), prog.phases.data(), sm.data());
+        ++*jitted;
+    }
+    dlclose(h);
+    return GQ_OK;
 }
 
 }  // namespace
@@ -290,6 +364,54 @@ int gqx_jit_check(int nq, int precision, const gq_op* ops, size_t n_ops, int til
     out[3] = compiled;
     out[4] = spills;
     return GQ_OK;
+}
+
+// The specialised kernels' code run on the CPU (see run_program_jit): a
+// statevector program (dm = 0, `state` 2^nq amplitudes) or the density-matrix
+// program of an nq-qubit rho (dm = 1, `state` 4^nq amplitudes), scheduled
+// as the engine does. csrc: directory of tile_core.cuh; work: a writable
+// directory for the generated library. out = {passes, passes run specialised}.
+int gqx_jit_emulate(int nq, int precision, double* state, const gq_op* ops, size_t n_ops, int tile_qubits,
+                    int budget, int dm, const char* csrc, const char* work, int64_t* out) {
+    std::vector<gq::NGate> gates;
+    const int nvec = dm ? 2 * nq : nq;
+    const int nphys = nvec < gq::RQ ? gq::RQ : nvec;
+    if (dm) {
+        const int rc = gq::dm_gates(nq, ops, n_ops, gates, g_err);
+        if (rc != GQ_OK) return rc;
+    } else {
+        for (size_t i = 0; i < n_ops; ++i) {
+            const int rc = gq::normalize_op(ops[i], nphys, gates, g_err);
+            if (rc != GQ_OK) return rc;
+        }
+    }
+    gq::SchedOptions opt;
+    opt.tile_qubits = tile_qubits > 0 ? tile_qubits : 11;
+    opt.budget = budget > 0 ? budget : 320;
+    opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
+    opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    gq::Program prog;
+    gq::schedule(gates, nphys, opt, prog);
+    const uint64_t n = 1ull << nphys, nv = 1ull << nvec;
+    int64_t jitted = 0;
+    int rc;
+    if (precision == GQ_C64) {
+        std::vector<gq::cplx<float>> st(n, {0.f, 0.f});
+        for (uint64_t i = 0; i < nv; ++i) st[i] = {(float)state[2 * i], (float)state[2 * i + 1]};
+        rc = run_program_jit<float>(st, prog, true, csrc, work, &jitted);
+        for (uint64_t i = 0; i < nv; ++i) {
+            state[2 * i] = st[i].x;
+            state[2 * i + 1] = st[i].y;
+        }
+    } else {
+        std::vector<gq::cplx<double>> st(n, {0.0, 0.0});
+        std::memcpy(st.data(), state, sizeof(double) * 2 * nv);
+        rc = run_program_jit<double>(st, prog, false, csrc, work, &jitted);
+        std::memcpy(state, st.data(), sizeof(double) * 2 * nv);
+    }
+    out[0] = (int64_t)prog.passes.size();
+    out[1] = jitted;
+    return rc;
 }
 
 }  // extern "C"

@@ -197,6 +197,7 @@ struct Engine {
     int variant = 0;
     int jit_mode = 1;         // GQ_OPT_JIT
     int jit_min_qubits = 20;  // GQ_OPT_JIT_MIN_QUBITS
+    int jit_min_blocks = 0;   // GQ_OPT_JIT_MIN_BLOCKS (0: the variant's)
     size_t amp_bytes() const { return prec == GQ_C64 ? 8 : 16; }
     int max_tile() const {
         return RQ + log2i(prec == GQ_C64 ? kVariantsC64[variant].threads : kVariantsC128[variant].threads);
@@ -301,7 +302,11 @@ struct Engine {
         std::vector<JitPlan> plans;
         if (jit_mode != 0 && nphys >= jit_min_qubits && jit_available()) {
             plans.resize(np);
-            const int minb = prec == GQ_C64 ? kVariantsC64[variant].min_blocks : kVariantsC128[variant].min_blocks;
+            // 4 CTAs of 128 threads per SM (128 registers) measured fastest for
+            // both precisions; other launch shapes keep their own bound
+            const TileVariant tv = prec == GQ_C64 ? kVariantsC64[variant] : kVariantsC128[variant];
+            const int minb = jit_min_blocks > 0 ? jit_min_blocks
+                                                : (tv.threads == 128 ? std::max(tv.min_blocks, 4) : tv.min_blocks);
             std::vector<char> planned(np, 0);
             for (size_t i = 0; i < np; ++i) {
                 const PassDesc& pd = pr.passes[i];
@@ -324,13 +329,8 @@ struct Engine {
             const unsigned threads = 1u << (pd.m - RQ);
             const size_t smem = sizeof(cplx<T>) << pd.m;
             const unsigned grid = 1u << pd.n_outer;
-            if (jfn[i]) {
-                const JitPlan& pl = plans[i];
-                pblock.assign(pl.n_param, cplx<T>{T(0), T(0)});
-                size_t k = 0;
-                for (const auto& c : pl.copies)
-                    for (uint32_t j = 0; j < c.second; ++j, ++k)
-                        pblock[k] = {(T)pr.pool[c.first + j].re, (T)pr.pool[c.first + j].im};
+            if (jfn[i]) pblock.resize(plans[i].n_param);
+            if (jfn[i] && jit_pack(pr, plans[i], prec == GQ_C64, pblock.data())) {
                 cplx<T>* stp = (cplx<T>*)state.p;
                 const cplx<T>* poolp = (const cplx<T>*)(d + o_pool);
                 const PhaseDesc* php = (const PhaseDesc*)(d + o_phase);
@@ -428,6 +428,9 @@ struct Engine {
         if (key == GQ_OPT_JIT) {
             if (value < 0 || value > 2) return fail(GQ_EINVAL, "jit mode out of range [0, 2]");
             jit_mode = (int)value;
+        } else if (key == GQ_OPT_JIT_MIN_BLOCKS) {
+            if (value < 0 || value > 16) return fail(GQ_EINVAL, "jit min blocks out of range [0, 16]");
+            jit_min_blocks = (int)value;
         } else {
             if (value < 0 || value > 64) return fail(GQ_EINVAL, "jit min qubits out of range [0, 64]");
             jit_min_qubits = (int)value;
@@ -785,6 +788,7 @@ int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
             return GQ_OK;
         case GQ_OPT_JIT:
         case GQ_OPT_JIT_MIN_QUBITS:
+        case GQ_OPT_JIT_MIN_BLOCKS:
             return e.set_jit_option(key, value);
         default:
             return fail(GQ_EINVAL, "unknown option");
@@ -950,7 +954,8 @@ int gq_dm_set_option(gq_dm* dm, int key, int64_t value) {
         dm->e.opt.tile_qubits = dm->e.max_tile();
         return GQ_OK;
     }
-    if (key == GQ_OPT_JIT || key == GQ_OPT_JIT_MIN_QUBITS) return dm->e.set_jit_option(key, value);
+    if (key == GQ_OPT_JIT || key == GQ_OPT_JIT_MIN_QUBITS || key == GQ_OPT_JIT_MIN_BLOCKS)
+        return dm->e.set_jit_option(key, value);
     return fail(GQ_EINVAL, "unknown option");
 }
 

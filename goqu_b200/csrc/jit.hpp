@@ -3,16 +3,25 @@
 // The interpreted pass kernel (k_tile_pass) reads every op of a pass from the
 // program at run time and dispatches on its kind, target register bits and
 // controls. For a pass whose structure is known, jit_plan() emits the same
-// pass as straight-line CUDA C++: the same tile_core.cuh op bodies, but with
-// target bits, controls, shared-memory slots and global index columns as
-// compile-time constants, and the pass's matrices passed by value as a kernel
-// parameter block (constant-bank operands of the FMAs). The kernel text holds
-// no matrix values, so passes with the same structure and different angles
-// share one compiled kernel.
+// pass as straight-line CUDA C++: the tile_core.cuh op bodies with target
+// bits, controls, shared-memory slots and global index columns as
+// compile-time constants, and the pass's numbers passed by value as a kernel
+// parameter block (constant-bank operands of the FMAs).
 //
-// Compilation runs on background threads; until a pass's kernel is ready the
-// engine launches the interpreted kernel for it (GQ_OPT_JIT = 1), or waits
-// for it (GQ_OPT_JIT = 2).
+// Within a phase the generator also keeps a pending factor per register slot
+// (a product of "atoms": diagonal entries, phases): diagonal ops and
+// permutations without run-time conditions cost no arithmetic, and a general
+// one-qubit unitary U = g diag(1, e^{i phi}) cos(theta/2) [[1, -t], [t, 1]]
+// diag(1, e^{i lambda}) (t = tan(theta/2)) costs one complex multiply on half
+// the slots (to equalise the pair's factors) plus a real shear. Factors are
+// folded into the amplitudes before any op that needs them equal across its
+// group and at the end of the phase. Products and ratios of atoms are
+// evaluated on the host by jit_pack() when the pass is launched.
+//
+// The kernel text holds no numbers, so passes with the same structure and
+// other angles share one compiled kernel. Compilation runs on background
+// threads; until a pass's kernel is ready the engine launches the
+// interpreted kernel for it (GQ_OPT_JIT = 1), or waits for it (GQ_OPT_JIT = 2).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -24,17 +33,45 @@
 
 namespace gq {
 
+// A factor value: pool[ref] (kind 0), or for the one-qubit unitary at
+// ops[ref]: e^{i lambda} (1), g cos(theta/2) (2), g cos(theta/2) e^{i phi} (3).
+struct JitAtom {
+    uint8_t kind;
+    uint32_t ref;
+};
+
+// One parameter-block entry: `count` pool values from pool[ref] (kind 0), the
+// shear t of the one-qubit unitary ops[ref] (kind 1, real part), or the
+// product of atoms `num` divided by the product of atoms `den` (kind 2).
+struct JitEntry {
+    uint8_t kind;
+    uint32_t ref, count;
+    std::vector<uint32_t> num, den;
+};
+
 struct JitPlan {
-    std::string source;  // kernel text (the cache key)
-    // Matrix entries packed into the parameter block, in order: (pool offset, count).
-    std::vector<std::pair<uint32_t, uint32_t>> copies;
-    uint32_t n_param = 0;  // complex entries of the parameter block (>= 1)
+    std::string source;       // device kernel text (the cache key)
+    std::string host_source;  // the same pass as a host function (CPU tests), when asked for
+    std::vector<JitAtom> atoms;
+    std::vector<JitEntry> entries;
+    uint32_t n_param = 0;                             // complex entries of the parameter block (>= 1)
+    std::vector<std::vector<uint32_t>> phase_shears;  // shear ops of each phase (range check)
 };
 
 // Kernel text for pass `pass` of `pr` at precision c64 / c128 with the given
-// launch bounds. Returns false for passes the generator does not cover
-// (gradient ops), which stay on the interpreted kernel.
-bool jit_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks, JitPlan& out);
+// launch bounds (and, with `host`, the host-function form in host_source).
+// Returns false for passes the generator does not cover (gradient ops, or a
+// parameter block over the kernel-parameter limit): they stay interpreted.
+bool jit_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks, JitPlan& out,
+              bool host = false);
+// Fills the parameter block (n_param complex values of float or double) from
+// the program's current numbers. Returns false when the pass's shears could
+// leave the floating-point range; the pass then runs interpreted.
+bool jit_pack(const Program& pr, const JitPlan& plan, bool c64, void* block);
+// Decomposition of a one-qubit unitary m (row major) into the shear form
+// above. False when m is not unitary to 1e-12 or cos / sin(theta/2) is below
+// 1e-150 (the generator then keeps the dense 2x2).
+bool u1_decompose(const Z* m, double* t, Z* lam, Z* post0, Z* post1);
 
 // Process-wide cache of compiled kernels, keyed by kernel text.
 enum JitState { JIT_MISSING = 0, JIT_PENDING = 1, JIT_READY = 2, JIT_FAILED = 3 };

@@ -1,12 +1,16 @@
-// Specialised tile-pass kernels: code generation and NVRTC compilation (see
-// jit.hpp). Needs no device; the emulator library links it for the CPU tests.
+// Specialised tile-pass kernels: code generation, parameter packing and
+// NVRTC compilation (see jit.hpp). Needs no device; the emulator library
+// links it for the CPU tests.
 #include "jit.hpp"
 
 #include <dlfcn.h>
 #include <nvrtc.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 
 namespace gq {
 
@@ -27,59 +31,129 @@ std::string hex32(uint32_t v) {
     std::snprintf(b, sizeof b, "0x%xu", v);
     return b;
 }
+std::string num(long long v) { return std::to_string(v); }
 
 int ctz64(uint64_t v) { return __builtin_ctzll(v); }
 
-// Emits `dst |= (uint64_t)((src >> from) & mask) << to` for every run of bit k
-// of `src` (k = 0..n-1) going to qubit q[k], merging runs of consecutive
-// positions into one shift.
-void emit_deposit(std::string& s, const char* dst, const char* src, const int* q, int n) {
+// Emits `dst |= ((src >> k) & mask) << q[k]` for every run of bits k of `src`
+// (k = 0..n-1) going to consecutive positions q[k].
+void emit_deposit(std::string& s, const char* ind, const char* dst, const char* src, const int* q, int n) {
     int k = 0;
     while (k < n) {
         int len = 1;
         while (k + len < n && q[k + len] == q[k] + len) ++len;
         const uint64_t mask = len >= 64 ? ~0ull : ((1ull << len) - 1);
-        s += "    ";
+        s += ind;
         s += dst;
         s += " |= ((uint64_t)(";
         s += src;
-        s += " >> " + std::to_string(k) + ") & " + hex64(mask) + ") << " + std::to_string(q[k]) + ";\n";
+        s += " >> " + num(k) + ") & " + hex64(mask) + ") << " + num(q[k]) + ";\n";
         k += len;
     }
 }
 
-int mat_len(const KOp& op) {
-    switch (op.type) {
-        case K_U1: return 4;
-        case K_U2: return 16;
-        case K_U3: return 64;
-        case K_U4: return 256;
-        case K_X: return (op.flags & 1) ? 0 : 2;
-        case K_PHASE: return 1;
-        default: return 0;
-    }
+Z zmul(Z a, Z b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+Z zdiv(Z a, Z b) {
+    const double d = b.re * b.re + b.im * b.im;
+    return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
 }
+double zabs(Z a) { return std::hypot(a.re, a.im); }
+
+using Pend = std::vector<uint32_t>;  // sorted atom ids
+
+// Code generation state of one pass.
+struct Gen {
+    const Program& pr;
+    JitPlan& out;
+    uint32_t cap;
+    uint32_t np = 0;
+    bool overflow = false;
+    std::map<std::pair<uint8_t, uint32_t>, uint32_t> atom_ids;
+    std::map<std::string, uint32_t> entry_ids;  // dedupe key -> parameter offset
+
+    Gen(const Program& p, JitPlan& o, uint32_t c) : pr(p), out(o), cap(c) {}
+
+    uint32_t atom(uint8_t kind, uint32_t ref) {
+        auto it = atom_ids.find({kind, ref});
+        if (it != atom_ids.end()) return it->second;
+        const uint32_t id = (uint32_t)out.atoms.size();
+        out.atoms.push_back({kind, ref});
+        atom_ids[{kind, ref}] = id;
+        return id;
+    }
+    uint32_t add_entry(const std::string& key, JitEntry e) {
+        auto it = entry_ids.find(key);
+        if (it != entry_ids.end()) return it->second;
+        const uint32_t n = e.kind == 0 ? e.count : 1;
+        if (np + n > cap) {
+            overflow = true;
+            return 0;
+        }
+        const uint32_t off = np;
+        np += n;
+        out.entries.push_back(std::move(e));
+        entry_ids[key] = off;
+        return off;
+    }
+    uint32_t copy(uint32_t ref, uint32_t count) {
+        return add_entry("C" + num(ref) + ":" + num(count), JitEntry{0, ref, count, {}, {}});
+    }
+    uint32_t shear_t(uint32_t op) { return add_entry("T" + num(op), JitEntry{1, op, 1, {}, {}}); }
+    // Offset of prod(num) / prod(den) after cancelling common atoms; -1 if 1.
+    long ratio(const Pend& n0, const Pend& d0) {
+        Pend n, d;
+        std::set_difference(n0.begin(), n0.end(), d0.begin(), d0.end(), std::back_inserter(n));
+        std::set_difference(d0.begin(), d0.end(), n0.begin(), n0.end(), std::back_inserter(d));
+        if (n.empty() && d.empty()) return -1;
+        std::string key = "P";
+        for (uint32_t a : n) key += num(a) + ",";
+        key += "/";
+        for (uint32_t a : d) key += num(a) + ",";
+        return add_entry(key, JitEntry{2, 0, 1, n, d});
+    }
+};
+
+void pend_add(Pend& p, uint32_t a) { p.insert(std::upper_bound(p.begin(), p.end(), a), a); }
 
 }  // namespace
 
-bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, JitPlan& out) {
+bool u1_decompose(const Z* m, double* t, Z* lam, Z* post0, Z* post1) {
+    // unitary: columns orthonormal
+    const double n0 = m[0].re * m[0].re + m[0].im * m[0].im + m[2].re * m[2].re + m[2].im * m[2].im;
+    const double n1 = m[1].re * m[1].re + m[1].im * m[1].im + m[3].re * m[3].re + m[3].im * m[3].im;
+    const Z ip = {m[0].re * m[1].re + m[0].im * m[1].im + m[2].re * m[3].re + m[2].im * m[3].im,
+                  m[0].re * m[1].im - m[0].im * m[1].re + m[2].re * m[3].im - m[2].im * m[3].re};
+    if (std::fabs(n0 - 1) > 1e-12 || std::fabs(n1 - 1) > 1e-12 || zabs(ip) > 1e-12) return false;
+    const double c = zabs(m[0]), s = zabs(m[2]);
+    if (c < 1e-150 || s < 1e-150) return false;
+    const Z g = {m[0].re / c, m[0].im / c};
+    const Z eph = zdiv({m[2].re / s, m[2].im / s}, g);      // e^{i phi}
+    const Z elam = zdiv({-m[1].re / s, -m[1].im / s}, g);   // e^{i lambda}
+    *t = s / c;
+    *lam = elam;
+    *post0 = {g.re * c, g.im * c};
+    *post1 = zmul(*post0, eph);
+    return true;
+}
+
+bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, JitPlan& out, bool host) {
     const PassDesc& pd = pr.passes[pi];
     const int m = pd.m, tbits = m - RQ;
     if (tbits < 0 || (1 << tbits) != threads) return false;
-    out.copies.clear();
-    const uint32_t cap = c64 ? 3900u : 1950u;  // parameter block entries (32 KB of kernel parameters)
-    uint32_t np = 0;
+    out.atoms.clear();
+    out.entries.clear();
+    out.phase_shears.clear();
+    Gen gen(pr, out, c64 ? 3900u : 1950u);  // 32 KB of kernel parameters
 
-    std::string b;  // kernel body
-    b.reserve(1 << 16);
-    b += "    const uint32_t t = threadIdx.x;\n    const uint64_t cta = blockIdx.x;\n    uint64_t base = 0;\n";
-    emit_deposit(b, "base", "cta", pd.outer_q, pd.n_outer);
-    // staging: thread bits are tile bits [0, tbits), the 16 register slots
-    // of the linear staging are tile bits [tbits, m)
-    b += "    uint64_t gt = base;\n    uint32_t stt = 0;\n";
-    emit_deposit(b, "gt", "t", pd.tile_q, tbits);
+    // ---- prologue: CTA base, staging columns (thread bits = tile bits [0, tbits))
+    std::string pro;
+    pro += "    uint64_t base = 0;\n";
+    emit_deposit(pro, "    ", "base", "cta", pd.outer_q, pd.n_outer);
+    pro += "    uint64_t gt = base;\n    uint32_t stt = 0;\n";
+    emit_deposit(pro, "    ", "gt", "t", pd.tile_q, tbits);
     for (int k = 0; k < tbits; ++k)
-        b += "    stt ^= (0u - ((t >> " + std::to_string(k) + ") & 1u)) & " + hex32(pd.acol[k]) + ";\n";
+        pro += "    stt ^= (0u - ((t >> " + num(k) + ") & 1u)) & " + hex32(pd.acol[k]) + ";\n";
+    pro += "    (void)gt;\n    (void)stt;\n";
     uint64_t G[NREG];
     uint32_t S[NREG];
     for (int it = 0; it < NREG; ++it) {
@@ -91,124 +165,309 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                 S[it] ^= pd.acol[tbits + k];
             }
     }
-    b += "    {\n        cplx<T> v[16];\n";
-    for (int it = 0; it < NREG; ++it) b += "        v[" + std::to_string(it) + "] = st[gt | " + hex64(G[it]) + "];\n";
-    for (int it = 0; it < NREG; ++it)
-        b += "        sm[stt ^ " + hex32(S[it]) + "] = v[" + std::to_string(it) + "];\n";
-    b += "    }\n    __syncthreads();\n";
+    std::string seg_in = "    {\n        cplx<T> v[16];\n";
+    for (int it = 0; it < NREG; ++it) seg_in += "        v[" + num(it) + "] = st[gt | " + hex64(G[it]) + "];\n";
+    for (int it = 0; it < NREG; ++it) seg_in += "        sm[stt ^ " + hex32(S[it]) + "] = v[" + num(it) + "];\n";
+    seg_in += "    }\n";
+    std::string seg_out = "    {\n        cplx<T> v[16];\n";
+    for (int it = 0; it < NREG; ++it) seg_out += "        v[" + num(it) + "] = sm[stt ^ " + hex32(S[it]) + "];\n";
+    for (int it = 0; it < NREG; ++it) seg_out += "        st[gt | " + hex64(G[it]) + "] = v[" + num(it) + "];\n";
+    seg_out += "    }\n";
 
+    std::vector<std::string> seg_ph;
     for (int p = 0; p < pd.n_phases; ++p) {
         const int phi = pd.phase0 + p;
         const PhaseDesc& ph = pr.phases[phi];
-        // thread-bit columns of the phase's tables
+        out.phase_shears.emplace_back();
         uint32_t tslot[MAX_TILE];
         int tq[MAX_TILE];
         for (int k = 0; k < tbits; ++k) {
-            const uint32_t s = k < 4 ? ph.tlo_slot[1u << k] : ph.thi_slot[1u << (k - 4)];
+            const uint32_t sv = k < 4 ? ph.tlo_slot[1u << k] : ph.thi_slot[1u << (k - 4)];
             const uint64_t g = k < 4 ? ph.tlo_glob[1u << k] : ph.thi_glob[1u << (k - 4)];
             if (g == 0 || (g & (g - 1))) return false;
-            tslot[k] = s;
+            tslot[k] = sv;
             tq[k] = ctz64(g);
         }
-        // the tables must be the XOR / OR of those columns
-        for (int v = 0; v < TLO && v < (1 << tbits); ++v) {
-            uint32_t s = 0;
+        for (int v = 0; v < TLO && v < (1 << tbits); ++v) {  // the tables are XOR / OR of those columns
+            uint32_t sv = 0;
             uint64_t g = 0;
             for (int k = 0; k < 4 && k < tbits; ++k)
                 if ((v >> k) & 1) {
-                    s ^= tslot[k];
+                    sv ^= tslot[k];
                     g |= 1ull << tq[k];
                 }
-            if (s != ph.tlo_slot[v] || g != ph.tlo_glob[v]) return false;
+            if (sv != ph.tlo_slot[v] || g != ph.tlo_glob[v]) return false;
         }
-        b += "    {\n        uint32_t sb = 0;\n        uint64_t g0 = base;\n";
+        std::string b = "    {\n        uint32_t sb = 0;\n        uint64_t g0 = base;\n";
         for (int k = 0; k < tbits; ++k)
-            b += "        sb ^= (0u - ((t >> " + std::to_string(k) + ") & 1u)) & " + hex32(tslot[k]) + ";\n";
-        {
-            std::string d;
-            emit_deposit(d, "g0", "t", tq, tbits);
-            b += d;
-        }
-        b += "        cplx<T> a[16];\n";
-        for (int j = 0; j < NREG; ++j)
-            b += "        a[" + std::to_string(j) + "] = sm[sb ^ " + hex32(ph.rslot[j]) + "];\n";
+            b += "        sb ^= (0u - ((t >> " + num(k) + ") & 1u)) & " + hex32(tslot[k]) + ";\n";
+        emit_deposit(b, "        ", "g0", "t", tq, tbits);
+        b += "        (void)g0;\n        cplx<T> a[16];\n";
+        for (int j = 0; j < NREG; ++j) b += "        a[" + num(j) + "] = sm[sb ^ " + hex32(ph.rslot[j]) + "];\n";
+
+        Pend pend[NREG];
+        auto scale = [&](int j, long off) {
+            if (off >= 0) b += "        a[" + num(j) + "] = cmul(p.m[" + num(off) + "], a[" + num(j) + "]);\n";
+        };
+        // Groups of an op on target bits `tm` under register controls `creg`.
+        auto groups = [&](uint32_t tm, uint32_t creg) {
+            std::vector<std::vector<int>> gs;
+            for (int j = 0; j < NREG; ++j) {
+                if ((j & tm) || (j & creg) != creg) continue;
+                std::vector<int> g;
+                for (int sub = 0; sub < NREG; ++sub)
+                    if ((sub & ~tm) == 0) g.push_back(j | sub);
+                gs.push_back(g);
+            }
+            return gs;
+        };
+        auto normalize = [&](const std::vector<int>& g) {
+            for (size_t i = 1; i < g.size(); ++i)
+                if (pend[g[i]] != pend[g[0]]) {
+                    scale(g[i], gen.ratio(pend[g[i]], pend[g[0]]));
+                    pend[g[i]] = pend[g[0]];
+                }
+        };
+        auto resolve = [&](int j) {
+            if (pend[j].empty()) return;
+            scale(j, gen.ratio(pend[j], {}));
+            pend[j].clear();
+        };
+
         for (int o = ph.op_begin; o < ph.op_end; ++o) {
             const KOp& op = pr.ops[o];
             if (op.type == K_GRAD || op.type == K_NONE || op.type > K_RESET) return false;
-            const int ml = mat_len(op);
-            std::string M;
-            if (ml > 0 && np + (uint32_t)ml <= cap) {
-                M = "PMat<T>{p.m + " + std::to_string(np) + "}";
-                out.copies.push_back({op.mat, (uint32_t)ml});
-                np += (uint32_t)ml;
-            } else {
-                M = "(pool + " + std::to_string(op.mat) + "u)";
-            }
-            const std::string creg = std::to_string(op.creg) + "u";
+            const std::string creg = num(op.creg) + "u";
             const std::string C = op.creg ? "true" : "false";
             std::string cond;
             if (op.cmask) cond = "if ((g0 & " + hex64(op.cmask) + ") == " + hex64(op.cmask) + ") ";
-            const std::string S0 = std::to_string(op.t0), S1 = std::to_string(op.t1), S2 = std::to_string(op.t2);
-            std::string call;
+            const std::string S0 = num(op.t0), S1 = num(op.t1), S2 = num(op.t2);
+            auto pm = [&](uint32_t off) { return "PMat<T>{p.m + " + num(off) + "}"; };
             switch (op.type) {
-                case K_U1: call = "k_u1<T, " + S0 + ", " + C + ">(a, " + M + ", " + creg + ");"; break;
-                case K_U2: call = "k_u2<T, " + S0 + ", " + S1 + ", " + C + ">(a, " + M + ", " + creg + ");"; break;
-                case K_U3: call = "k_u3<T, " + S0 + ", " + S1 + ", " + S2 + ">(a, " + M + ", " + creg + ");"; break;
-                case K_U4:
-                    call = "k_u4<T>(a, " + M + ", sm, sb, phases[" + std::to_string(phi) + "].rslot);";
-                    break;
-                case K_X:
-                    call = "k_x<T, " + S0 + ", " + C + ">(a, " + ((op.flags & 1) ? std::string("pool") : M) + ", " +
-                           creg + ", " + ((op.flags & 1) ? "true" : "false") + ");";
-                    break;
-                case K_SWAP: call = "k_swap<T, " + S0 + ", " + S1 + ">(a, " + creg + ");"; break;
-                case K_PHASE: call = "k_phase<T>(a, ldc(" + M + ", 0), " + creg + ");"; break;
-                case K_RESET: call = "k_reset<T, " + S0 + ">(a);"; break;
-                case K_DIAG: {
-                    std::string h = "{ uint32_t hi = 0; ";
-                    int k = 0;
-                    for (uint64_t dm = op.dmask; dm; dm &= dm - 1, ++k)
-                        h += "hi |= (uint32_t)((g0 >> " + std::to_string(ctz64(dm)) + ") & 1ull) << " +
-                             std::to_string(k) + "; ";
-                    h += "k_diag_hi<T>(a, pool + " + std::to_string(op.mat) + "u, hi << " + std::to_string(op.nreg) +
-                         ", " + std::to_string(op.nreg) + "u, " + creg + ", " + hex64(op.ridx) + "); }";
-                    call = h;
+                case K_U1: {
+                    const uint32_t tm = 1u << op.t0;
+                    double tv;
+                    Z lam, p0, p1;
+                    if (!op.cmask && u1_decompose(&pr.pool[op.mat], &tv, &lam, &p0, &p1)) {
+                        const uint32_t a_l = gen.atom(1, (uint32_t)o), a_0 = gen.atom(2, (uint32_t)o),
+                                       a_1 = gen.atom(3, (uint32_t)o);
+                        const auto gs = groups(tm, op.creg);
+                        for (const auto& g : gs) {
+                            pend_add(pend[g[1]], a_l);
+                            normalize(g);
+                        }
+                        b += "        k_shear<T, " + S0 + ", " + C + ">(a, p.m[" + num(gen.shear_t((uint32_t)o)) +
+                             "].x, " + creg + ");\n";
+                        for (const auto& g : gs) {
+                            pend[g[1]] = pend[g[0]];
+                            pend_add(pend[g[1]], a_1);
+                            pend_add(pend[g[0]], a_0);
+                        }
+                        out.phase_shears.back().push_back((uint32_t)o);
+                    } else {
+                        for (const auto& g : groups(tm, op.creg)) normalize(g);
+                        b += "        " + cond + "k_u1<T, " + S0 + ", " + C + ">(a, " + pm(gen.copy(op.mat, 4)) +
+                             ", " + creg + ");\n";
+                    }
                     break;
                 }
-                default: return false;
+                case K_U2:
+                    for (const auto& g : groups((1u << op.t0) | (1u << op.t1), op.creg)) normalize(g);
+                    b += "        " + cond + "k_u2<T, " + S0 + ", " + S1 + ", " + C + ">(a, " +
+                         pm(gen.copy(op.mat, 16)) + ", " + creg + ");\n";
+                    break;
+                case K_U3:
+                    for (const auto& g : groups((1u << op.t0) | (1u << op.t1) | (1u << op.t2), op.creg)) normalize(g);
+                    b += "        " + cond + "k_u3<T, " + S0 + ", " + S1 + ", " + S2 + ">(a, " +
+                         pm(gen.copy(op.mat, 64)) + ", " + creg + ");\n";
+                    break;
+                case K_U4:
+                    for (const auto& g : groups(15u, 0u)) normalize(g);
+                    b += "        " + cond + "k_u4<T>(a, " + pm(gen.copy(op.mat, 256)) + ", sm, sb, phases[" +
+                         num(phi) + "].rslot);\n";
+                    break;
+                case K_X: {
+                    const uint32_t tm = 1u << op.t0;
+                    const bool pure = op.flags & 1;
+                    if (op.cmask) {
+                        for (const auto& g : groups(tm, op.creg)) normalize(g);
+                        b += "        " + cond + "k_x<T, " + S0 + ", " + C + ">(a, " +
+                             (pure ? std::string("pool") : pm(gen.copy(op.mat, 2))) + ", " + creg + ", " +
+                             (pure ? "true" : "false") + ");\n";
+                    } else {
+                        // a compile-time permutation; the phases p0, p1 become pending factors
+                        b += "        k_x<T, " + S0 + ", " + C + ">(a, pool, " + creg + ", true);\n";
+                        for (const auto& g : groups(tm, op.creg)) {
+                            std::swap(pend[g[0]], pend[g[1]]);
+                            if (!pure) {
+                                pend_add(pend[g[0]], gen.atom(0, op.mat));
+                                pend_add(pend[g[1]], gen.atom(0, op.mat + 1));
+                            }
+                        }
+                    }
+                    break;
+                }
+                case K_SWAP: {
+                    std::vector<std::pair<int, int>> prs;
+                    for (int j = 0; j < NREG; ++j) {
+                        if (!(j & (1 << op.t0)) || (j & (1 << op.t1))) continue;
+                        if ((j & op.creg) != op.creg) continue;
+                        prs.push_back({j, (j & ~(1 << op.t0)) | (1 << op.t1)});
+                    }
+                    if (op.cmask)
+                        for (const auto& q : prs) normalize({q.first, q.second});
+                    else
+                        for (const auto& q : prs) std::swap(pend[q.first], pend[q.second]);
+                    b += "        " + cond + "k_swap<T, " + S0 + ", " + S1 + ">(a, " + creg + ");\n";
+                    break;
+                }
+                case K_PHASE:
+                    if (op.cmask) {
+                        b += "        " + cond + "k_phase<T>(a, p.m[" + num(gen.copy(op.mat, 1)) + "], " + creg +
+                             ");\n";
+                    } else {
+                        const uint32_t a_s = gen.atom(0, op.mat);
+                        for (int j = 0; j < NREG; ++j)
+                            if ((j & op.creg) == op.creg) pend_add(pend[j], a_s);
+                    }
+                    break;
+                case K_DIAG:
+                    if (op.cmask || op.dmask) {
+                        std::string h = "{ uint32_t hi = 0; ";
+                        int k = 0;
+                        for (uint64_t dm = op.dmask; dm; dm &= dm - 1, ++k)
+                            h += "hi |= (uint32_t)((g0 >> " + num(ctz64(dm)) + ") & 1ull) << " + num(k) + "; ";
+                        h += "k_diag_hi<T>(a, pool + " + num(op.mat) + "u, hi << " + num(op.nreg) + ", " +
+                             num(op.nreg) + "u, " + creg + ", " + hex64(op.ridx) + "); }";
+                        b += "        " + cond + h + "\n";
+                    } else {
+                        for (int j = 0; j < NREG; ++j)
+                            if ((j & op.creg) == op.creg)
+                                pend_add(pend[j], gen.atom(0, op.mat + (uint32_t)((op.ridx >> (4 * j)) & 15u)));
+                    }
+                    break;
+                case K_RESET:
+                    for (int j = 0; j < NREG; ++j) resolve(j);
+                    b += "        " + cond + "k_reset<T, " + S0 + ">(a);\n";
+                    break;
+                default:
+                    return false;
             }
-            b += "        " + cond + call + "\n";
+            if (gen.overflow) return false;
         }
-        for (int j = 0; j < NREG; ++j)
-            b += "        sm[sb ^ " + hex32(ph.rslot[j]) + "] = a[" + std::to_string(j) + "];\n";
-        b += "    }\n    __syncthreads();\n";
+        for (int j = 0; j < NREG; ++j) resolve(j);
+        if (gen.overflow) return false;
+        for (int j = 0; j < NREG; ++j) b += "        sm[sb ^ " + hex32(ph.rslot[j]) + "] = a[" + num(j) + "];\n";
+        b += "    }\n";
+        seg_ph.push_back(b);
     }
-    b += "    {\n        cplx<T> v[16];\n";
-    for (int it = 0; it < NREG; ++it)
-        b += "        v[" + std::to_string(it) + "] = sm[stt ^ " + hex32(S[it]) + "];\n";
-    for (int it = 0; it < NREG; ++it) b += "        st[gt | " + hex64(G[it]) + "] = v[" + std::to_string(it) + "];\n";
-    b += "    }\n";
 
-    out.n_param = np > 0 ? np : 1;
-    const char* T = c64 ? "float" : "double";
+    out.n_param = gen.np > 0 ? gen.np : 1;
+    const std::string T = c64 ? "float" : "double";
+    const std::string jp = "namespace gq {\nstruct JP {\n    cplx<" + T + "> m[" + num(out.n_param) + "];\n};\n}\n";
     std::string& s = out.source;
     s.clear();
-    s.reserve(b.size() + 1024);
     s += "// goqu_b200 specialised tile pass\n";
     s += "typedef unsigned char uint8_t;\ntypedef int int32_t;\ntypedef unsigned int uint32_t;\n";
     s += "typedef long long int64_t;\ntypedef unsigned long long uint64_t;\n";
-    s += "#include \"tile_core.cuh\"\n";
-    s += "namespace gq {\nstruct JP {\n    cplx<" + std::string(T) + "> m[" + std::to_string(out.n_param) + "];\n};\n}\n";
-    s += "extern \"C\" __global__ void __launch_bounds__(" + std::to_string(threads) + ", " +
-         std::to_string(min_blocks) + ")\n";
-    s += "gqj_pass(gq::cplx<" + std::string(T) + ">* __restrict__ st, const __grid_constant__ gq::JP p, const gq::cplx<" +
-         std::string(T) + ">* __restrict__ pool, const gq::PhaseDesc* __restrict__ phases) {\n";
-    s += "    using namespace gq;\n    using T = " + std::string(T) + ";\n";
+    s += "#include \"tile_core.cuh\"\n" + jp;
+    s += "extern \"C\" __global__ void __launch_bounds__(" + num(threads) + ", " + num(min_blocks) + ")\n";
+    s += "gqj_pass(gq::cplx<" + T + ">* __restrict__ st, const __grid_constant__ gq::JP p, const gq::cplx<" + T +
+         ">* __restrict__ pool, const gq::PhaseDesc* __restrict__ phases) {\n";
+    s += "    using namespace gq;\n    using T = " + T + ";\n";
     s += "    extern __shared__ __align__(16) unsigned char smraw[];\n";
     s += "    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);\n";
     s += "    (void)pool;\n    (void)phases;\n";
-    s += b;
-    s += "}\n";
+    s += "    const uint32_t t = threadIdx.x;\n    const uint64_t cta = blockIdx.x;\n";
+    s += pro + seg_in + "    __syncthreads();\n";
+    for (const std::string& ph : seg_ph) s += ph + "    __syncthreads();\n";
+    s += seg_out + "}\n";
+
+    if (host) {
+        // the same segments, threads of a CTA run one after another between barriers
+        std::string& h = out.host_source;
+        h.clear();
+        h += "#include \"tile_core.cuh\"\n";
+        h += "extern \"C\" void gqj_host_" + num((long long)pi) + "(gq::cplx<" + T + ">* st, const gq::cplx<" + T +
+             ">* pm, const gq::cplx<" + T + ">* pool, const gq::PhaseDesc* phases, gq::cplx<" + T + ">* sm) {\n";
+        h += "    using namespace gq;\n    using T = " + T + ";\n    (void)pool;\n    (void)phases;\n";
+        h += "    const struct {\n        const cplx<T>* m;\n    } p{pm};\n";
+        h += "    for (uint64_t cta = 0; cta < (1ull << " + num(pd.n_outer) + "); ++cta) {\n";
+        auto loop = [&](const std::string& seg) {
+            h += "    for (uint32_t t = 0; t < " + num(threads) + "u; ++t) {\n" + pro + seg + "    }\n";
+        };
+        loop(seg_in);
+        for (const std::string& ph : seg_ph) loop(ph);
+        loop(seg_out);
+        h += "    }\n}\n";
+    }
+    return true;
+}
+
+bool jit_pack(const Program& pr, const JitPlan& plan, bool c64, void* block) {
+    // atom values
+    std::vector<Z> av(plan.atoms.size());
+    std::vector<double> tv(pr.ops.size(), 0.0);
+    std::vector<char> have(pr.ops.size(), 0);
+    auto dec = [&](uint32_t o, Z* lam, Z* p0, Z* p1) {
+        double t;
+        if (!u1_decompose(&pr.pool[pr.ops[o].mat], &t, lam, p0, p1)) return false;
+        tv[o] = t;
+        have[o] = 1;
+        return true;
+    };
+    for (size_t i = 0; i < plan.atoms.size(); ++i) {
+        const JitAtom& a = plan.atoms[i];
+        if (a.kind == 0) {
+            av[i] = pr.pool[a.ref];
+            continue;
+        }
+        Z lam, p0, p1;
+        if (!dec(a.ref, &lam, &p0, &p1)) return false;  // no longer decomposable: run interpreted
+        av[i] = a.kind == 1 ? lam : (a.kind == 2 ? p0 : p1);
+    }
+    // range check: within a phase the amplitudes grow by at most prod(1 + |t|)
+    const double limit = c64 ? 60.0 : 600.0;  // log2 bound
+    for (const auto& ph : plan.phase_shears) {
+        double lg = 0;
+        for (uint32_t o : ph) {
+            if (!have[o]) {
+                Z l, a, b;
+                if (!dec(o, &l, &a, &b)) return false;
+            }
+            lg += std::log2(1.0 + std::fabs(tv[o]));
+        }
+        if (lg > limit) return false;
+    }
+    std::vector<Z> vals;
+    vals.reserve(plan.n_param);
+    for (const JitEntry& e : plan.entries) {
+        if (e.kind == 0) {
+            for (uint32_t k = 0; k < e.count; ++k) vals.push_back(pr.pool[e.ref + k]);
+        } else if (e.kind == 1) {
+            if (!have[e.ref]) {
+                Z l, a, b;
+                if (!dec(e.ref, &l, &a, &b)) return false;
+            }
+            vals.push_back({tv[e.ref], 0.0});
+        } else {
+            Z nv = {1, 0}, dv = {1, 0};
+            for (uint32_t a : e.num) nv = zmul(nv, av[a]);
+            for (uint32_t a : e.den) dv = zmul(dv, av[a]);
+            if (zabs(dv) < 1e-280) return false;
+            vals.push_back(e.den.empty() ? nv : zdiv(nv, dv));
+        }
+    }
+    vals.resize(plan.n_param, Z{0, 0});
+    if (c64) {
+        float* f = (float*)block;
+        for (size_t i = 0; i < vals.size(); ++i) {
+            f[2 * i] = (float)vals[i].re;
+            f[2 * i + 1] = (float)vals[i].im;
+        }
+    } else {
+        std::memcpy(block, vals.data(), sizeof(Z) * vals.size());
+    }
     return true;
 }
 

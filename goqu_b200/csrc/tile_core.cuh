@@ -288,6 +288,21 @@ GQ_HD void k_x(cplx<T> (&a)[NREG], MP m, uint32_t creg, bool pure) {
     }
 }
 
+// Shear [[1, -t], [t, 1]] on register bit S (t real): the rotation part of a
+// one-qubit unitary once its phases and cos(theta/2) are factored out (the
+// specialised kernels keep those as pending per-slot factors).
+template <class T, int S, bool C>
+GQ_HD void k_shear(cplx<T> (&a)[NREG], T t, uint32_t creg) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (j & (1 << S)) continue;
+        if (C && (j & creg) != creg) continue;
+        const cplx<T> a0 = a[j], a1 = a[j | (1 << S)];
+        a[j] = {a0.x - t * a1.x, a0.y - t * a1.y};
+        a[j | (1 << S)] = {a1.x + t * a0.x, a1.y + t * a0.y};
+    }
+}
+
 template <class T, int S0, int S1>
 GQ_HD void k_swap(cplx<T> (&a)[NREG], uint32_t creg) {
 #pragma unroll

@@ -60,3 +60,74 @@ def test_layered_benchmark_kernels_repeat(emu):
 def test_density_matrix_kernels_compile(emu):
     c, nm = workloads.noisy_brickwork(6, layers=3, seed=1)
     check(emu, encode.density_ops(c, nm), 6, dm=1)
+
+
+# ---- the generated code run on the CPU --------------------------------------
+# gqx_jit_emulate compiles the host form of every pass's generated code (the
+# same segments as the kernel, threads of a CTA run in turn between barriers)
+# and runs it with the packed parameter blocks: this checks the generator's
+# pending-factor bookkeeping, the one-qubit shear decomposition and the
+# parameter packing against the oracle without a GPU.
+
+import numpy as np  # noqa: E402
+
+from oracle import binding as orc  # noqa: E402
+
+CSRC = os.path.join(ROOT, "goqu_b200", "csrc").encode()
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+def jit_emulate(emu, stream, n, tmp_path, precision=_abi.GQ_C128, dm=0, tile=0):
+    emu.gqx_jit_emulate.restype = ctypes.c_int
+    emu.gqx_jit_emulate.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.POINTER(_abi.gq_op), ctypes.c_size_t,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p,
+                                    ctypes.POINTER(ctypes.c_int64)]
+    nv = 2 * n if dm else n
+    st = np.zeros(1 << nv, dtype=np.complex128)
+    st[0] = 1
+    out = (ctypes.c_int64 * 2)()
+    rc = emu.gqx_jit_emulate(n, precision, st.view(np.float64).ctypes.data_as(_D), stream.ptr(), len(stream), tile, 0,
+                             dm, CSRC, str(tmp_path).encode(), out)
+    assert rc == 0, emu.gqx_last_error().decode()
+    passes, jitted = list(out)
+    assert jitted == passes >= 1
+    return st
+
+
+@pytest.mark.parametrize("n,seed,tile", [(6, 1, 0), (9, 2, 7), (12, 3, 0), (13, 4, 10)])
+def test_generated_code_matches_oracle(emu, tmp_path, n, seed, tile):
+    # every gate family, with controls inside and outside the registers and resets
+    c = random_circuit(n, 120, seed, allow_reset=True)
+    ops = encode.statevector_ops(c)
+    got = jit_emulate(emu, ops, n, tmp_path, tile=tile)
+    np.testing.assert_allclose(got, orc.sv_evolve(ops), atol=1e-12, rtol=0)
+
+
+def test_generated_code_layered_qft(emu, tmp_path):
+    # U3 layers (shear form), CNOT permutations, QFT phases (pending factors)
+    c = workloads.random_layers_qft(14, layers=10, seed=5)
+    ops = encode.statevector_ops(c)
+    want = orc.sv_evolve(ops)
+    np.testing.assert_allclose(jit_emulate(emu, ops, 14, tmp_path), want, atol=1e-12, rtol=0)
+    assert np.max(np.abs(jit_emulate(emu, ops, 14, tmp_path, precision=_abi.GQ_C64) - want)) < 2e-5
+
+
+def test_generated_code_extreme_angles(emu, tmp_path):
+    # rotations next to 0 and pi: tan(theta/2) near 0 and near 1e16
+    from goqu_b200 import circuit as ir
+    b = ir.Builder("x", 12)
+    rng = np.random.default_rng(9)
+    for layer in range(6):
+        for q in range(12):
+            th = [1e-14, np.pi - 1e-15, np.pi, 2 * np.pi - 1e-13, rng.uniform(0, 2 * np.pi)][(q + layer) % 5]
+            b.U3(th, rng.uniform(0, 6.3), rng.uniform(0, 6.3), q)
+        for q in range(layer % 2, 11, 2):
+            b.CNOT(q, q + 1)
+    ops = encode.statevector_ops(b.Build())
+    np.testing.assert_allclose(jit_emulate(emu, ops, 12, tmp_path), orc.sv_evolve(ops), atol=1e-12, rtol=0)
+
+
+def test_generated_code_density_matrix(emu, tmp_path):
+    c, nm = workloads.noisy_brickwork(5, layers=3, seed=1)
+    ops = encode.density_ops(c, nm)
+    np.testing.assert_allclose(jit_emulate(emu, ops, 5, tmp_path, dm=1), orc.dm_evolve(ops), atol=1e-12, rtol=0)
