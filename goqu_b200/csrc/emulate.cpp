@@ -76,7 +76,7 @@ int run_program_jit(std::vector<gq::cplx<T>>& st, const gq::Program& prog, bool 
     std::string src;
     for (size_t i = 0; i < prog.passes.size(); ++i) {
         const int threads = 1 << (prog.passes[i].m - gq::RQ);
-        if (!gq::jit_plan(prog, i, c64, threads, 1, plans[i], true)) continue;
+        if (!gq::jit_plan(prog, i, c64, threads, 1, false, plans[i], true)) continue;
         ok[i] = 1;
         src += plans[i].host_source;
     }
@@ -346,7 +346,7 @@ int gqx_jit_check(int nq, int precision, const gq_op* ops, size_t n_ops, int til
     for (size_t i = 0; i < prog.passes.size(); ++i) {
         gq::JitPlan pl;
         const int threads = 1 << (prog.passes[i].m - gq::RQ);
-        if (!gq::jit_plan(prog, i, precision == GQ_C64, threads, precision == GQ_C64 ? 4 : 3, pl)) continue;
+        if (!gq::jit_plan(prog, i, precision == GQ_C64, threads, precision == GQ_C64 ? 4 : 3, true, pl)) continue;
         ++planned;
         if (!texts.insert(pl.source).second || compiled >= max_compile) continue;
         std::string log;

@@ -198,6 +198,13 @@ struct Engine {
     int jit_mode = 1;         // GQ_OPT_JIT
     int jit_min_qubits = 20;  // GQ_OPT_JIT_MIN_QUBITS
     int jit_min_blocks = 0;   // GQ_OPT_JIT_MIN_BLOCKS (0: the variant's)
+    int jit_persistent = 0;   // GQ_OPT_JIT_PERSISTENT (measured slower: 3 CTAs/SM)
+    int jit_minb = 4;         // CTAs per SM of the last specialised launch shape
+    int num_sms = 148;
+    template <class T>
+    size_t jit_smem(int m) const {
+        return (sizeof(cplx<T>) << m) * (jit_persistent ? 2 : 1);
+    }
     size_t amp_bytes() const { return prec == GQ_C64 ? 8 : 16; }
     int max_tile() const {
         return RQ + log2i(prec == GQ_C64 ? kVariantsC64[variant].threads : kVariantsC128[variant].threads);
@@ -209,6 +216,7 @@ struct Engine {
         nphys = nphys_;
         n_amps = 1ull << nphys;
         GQ_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        GQ_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
         GQ_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
         GQ_CUDA(cudaEventCreate(&ev0));
         GQ_CUDA(cudaEventCreate(&ev1));
@@ -302,23 +310,26 @@ struct Engine {
         std::vector<JitPlan> plans;
         if (jit_mode != 0 && nphys >= jit_min_qubits && jit_available()) {
             plans.resize(np);
-            // 4 CTAs of 128 threads per SM (128 registers) measured fastest for
-            // both precisions; other launch shapes keep their own bound
+            // One tile per CTA: 4 CTAs of 128 threads per SM (128 registers)
+            // measured fastest for both precisions. Persistent: as many CTAs
+            // per SM as two tile buffers each allow (3 for complex128).
             const TileVariant tv = prec == GQ_C64 ? kVariantsC64[variant] : kVariantsC128[variant];
-            const int minb = jit_min_blocks > 0 ? jit_min_blocks
-                                                : (tv.threads == 128 ? std::max(tv.min_blocks, 4) : tv.min_blocks);
+            int minb = tv.threads == 128 ? std::max(tv.min_blocks, 4) : tv.min_blocks;
+            if (jit_persistent) minb = std::max(1, std::min(minb, (int)((227u << 10) / (2 * (sizeof(cplx<T>) << max_tile())))));
+            if (jit_min_blocks > 0) minb = jit_min_blocks;
+            jit_minb = minb;
             std::vector<char> planned(np, 0);
             for (size_t i = 0; i < np; ++i) {
                 const PassDesc& pd = pr.passes[i];
-                if (!jit_plan(pr, i, prec == GQ_C64, 1 << (pd.m - RQ), minb, plans[i])) continue;
+                if (!jit_plan(pr, i, prec == GQ_C64, 1 << (pd.m - RQ), minb, jit_persistent != 0, plans[i])) continue;
                 planned[i] = 1;
-                jit_lookup(plans[i].source, sizeof(cplx<T>) << pd.m, true, &jfn[i]);
+                jit_lookup(plans[i].source, jit_smem<T>(pd.m), true, &jfn[i]);
             }
             if (jit_mode == 2) {
                 jit_wait(600000.0);
                 for (size_t i = 0; i < np; ++i)
                     if (planned[i] && !jfn[i])
-                        jit_lookup(plans[i].source, sizeof(cplx<T>) << pr.passes[i].m, false, &jfn[i]);
+                        jit_lookup(plans[i].source, jit_smem<T>(pr.passes[i].m), false, &jfn[i]);
             }
         }
         if (timing) GQ_CUDA(cudaEventRecord(ev_pass0, stream));
@@ -335,7 +346,9 @@ struct Engine {
                 const cplx<T>* poolp = (const cplx<T>*)(d + o_pool);
                 const PhaseDesc* php = (const PhaseDesc*)(d + o_phase);
                 void* args[4] = {&stp, pblock.data(), &poolp, &php};
-                GQ_CUDA(cudaLaunchKernel(jfn[i], dim3(grid), dim3(threads), args, smem, stream));
+                const unsigned jgrid =
+                    jit_persistent ? (unsigned)std::min<uint64_t>(grid, (uint64_t)num_sms * jit_minb) : grid;
+                GQ_CUDA(cudaLaunchKernel(jfn[i], dim3(jgrid), dim3(threads), args, jit_smem<T>(pd.m), stream));
                 ++jitted;
                 continue;
             }
@@ -428,6 +441,8 @@ struct Engine {
         if (key == GQ_OPT_JIT) {
             if (value < 0 || value > 2) return fail(GQ_EINVAL, "jit mode out of range [0, 2]");
             jit_mode = (int)value;
+        } else if (key == GQ_OPT_JIT_PERSISTENT) {
+            jit_persistent = value != 0;
         } else if (key == GQ_OPT_JIT_MIN_BLOCKS) {
             if (value < 0 || value > 16) return fail(GQ_EINVAL, "jit min blocks out of range [0, 16]");
             jit_min_blocks = (int)value;
@@ -789,6 +804,7 @@ int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
         case GQ_OPT_JIT:
         case GQ_OPT_JIT_MIN_QUBITS:
         case GQ_OPT_JIT_MIN_BLOCKS:
+        case GQ_OPT_JIT_PERSISTENT:
             return e.set_jit_option(key, value);
         default:
             return fail(GQ_EINVAL, "unknown option");
@@ -954,7 +970,8 @@ int gq_dm_set_option(gq_dm* dm, int key, int64_t value) {
         dm->e.opt.tile_qubits = dm->e.max_tile();
         return GQ_OK;
     }
-    if (key == GQ_OPT_JIT || key == GQ_OPT_JIT_MIN_QUBITS || key == GQ_OPT_JIT_MIN_BLOCKS)
+    if (key == GQ_OPT_JIT || key == GQ_OPT_JIT_MIN_QUBITS || key == GQ_OPT_JIT_MIN_BLOCKS ||
+        key == GQ_OPT_JIT_PERSISTENT)
         return dm->e.set_jit_option(key, value);
     return fail(GQ_EINVAL, "unknown option");
 }

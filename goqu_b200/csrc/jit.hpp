@@ -60,9 +60,13 @@ struct JitPlan {
 
 // Kernel text for pass `pass` of `pr` at precision c64 / c128 with the given
 // launch bounds (and, with `host`, the host-function form in host_source).
+// persistent: the kernel is launched with fewer CTAs than tiles; each CTA
+// walks tiles blockIdx.x, + gridDim.x, ... with two tile buffers (2 x 2^m
+// amplitudes of dynamic shared memory), copying the next tile in with
+// cp.async while the current one runs. Otherwise one CTA per tile.
 // Returns false for passes the generator does not cover (gradient ops, or a
 // parameter block over the kernel-parameter limit): they stay interpreted.
-bool jit_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks, JitPlan& out,
+bool jit_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks, bool persistent, JitPlan& out,
               bool host = false);
 // Fills the parameter block (n_param complex values of float or double) from
 // the program's current numbers. Returns false when the pass's shears could

@@ -136,7 +136,8 @@ bool u1_decompose(const Z* m, double* t, Z* lam, Z* post0, Z* post1) {
     return true;
 }
 
-bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, JitPlan& out, bool host) {
+bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, bool persistent, JitPlan& out,
+              bool host) {
     const PassDesc& pd = pr.passes[pi];
     const int m = pd.m, tbits = m - RQ;
     if (tbits < 0 || (1 << tbits) != threads) return false;
@@ -146,14 +147,18 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
     Gen gen(pr, out, c64 ? 3900u : 1950u);  // 32 KB of kernel parameters
 
     // ---- prologue: CTA base, staging columns (thread bits = tile bits [0, tbits))
-    std::string pro;
-    pro += "    uint64_t base = 0;\n";
-    emit_deposit(pro, "    ", "base", "cta", pd.outer_q, pd.n_outer);
-    pro += "    uint64_t gt = base;\n    uint32_t stt = 0;\n";
-    emit_deposit(pro, "    ", "gt", "t", pd.tile_q, tbits);
-    for (int k = 0; k < tbits; ++k)
-        pro += "    stt ^= (0u - ((t >> " + num(k) + ") & 1u)) & " + hex32(pd.acol[k]) + ";\n";
-    pro += "    (void)gt;\n    (void)stt;\n";
+    auto make_pro = [&](const char* ctav) {
+        std::string r;
+        r += "    uint64_t base = 0;\n";
+        emit_deposit(r, "    ", "base", ctav, pd.outer_q, pd.n_outer);
+        r += "    uint64_t gt = base;\n    uint32_t stt = 0;\n";
+        emit_deposit(r, "    ", "gt", "t", pd.tile_q, tbits);
+        for (int k = 0; k < tbits; ++k)
+            r += "    stt ^= (0u - ((t >> " + num(k) + ") & 1u)) & " + hex32(pd.acol[k]) + ";\n";
+        r += "    (void)gt;\n    (void)stt;\n";
+        return r;
+    };
+    const std::string pro = make_pro("cta");
     uint64_t G[NREG];
     uint32_t S[NREG];
     for (int it = 0; it < NREG; ++it) {
@@ -376,12 +381,39 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
          ">* __restrict__ pool, const gq::PhaseDesc* __restrict__ phases) {\n";
     s += "    using namespace gq;\n    using T = " + T + ";\n";
     s += "    extern __shared__ __align__(16) unsigned char smraw[];\n";
-    s += "    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);\n";
     s += "    (void)pool;\n    (void)phases;\n";
-    s += "    const uint32_t t = threadIdx.x;\n    const uint64_t cta = blockIdx.x;\n";
-    s += pro + seg_in + "    __syncthreads();\n";
-    for (const std::string& ph : seg_ph) s += ph + "    __syncthreads();\n";
-    s += seg_out + "}\n";
+    s += "    const uint32_t t = threadIdx.x;\n";
+    if (!persistent) {
+        s += "    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);\n";
+        s += "    const uint64_t cta = blockIdx.x;\n";
+        s += pro + seg_in + "    __syncthreads();\n";
+        for (const std::string& ph : seg_ph) s += ph + "    __syncthreads();\n";
+        s += seg_out + "}\n";
+    } else {
+        // persistent CTAs, two tile buffers: the next tile's amplitudes are
+        // copied asynchronously while the current one runs its phases
+        auto issue = [&](const char* buf) {
+            std::string r;
+            for (int it = 0; it < NREG; ++it)
+                r += "    cp_async_amp(" + std::string(buf) + " + (stt ^ " + hex32(S[it]) + "), st + (gt | " +
+                     hex64(G[it]) + "));\n";
+            return r;
+        };
+        s += "    cplx<T>* const buf0 = reinterpret_cast<cplx<T>*>(smraw);\n";
+        s += "    cplx<T>* const buf1 = buf0 + " + num(1ll << m) + ";\n";
+        s += "    const uint64_t ntiles = 1ull << " + num(pd.n_outer) + ";\n";
+        s += "    uint64_t cta = blockIdx.x;\n    if (cta >= ntiles) return;\n";
+        s += "    {\n" + pro + issue("buf0") + "    }\n    cp_async_commit();\n";
+        s += "    for (uint32_t k = 0;; ++k) {\n";
+        s += "    cplx<T>* const sm = (k & 1u) ? buf1 : buf0;\n";
+        s += "    const uint64_t nxt = cta + gridDim.x;\n";
+        s += "    if (nxt < ntiles) {\n" + make_pro("nxt") + issue("((k & 1u) ? buf0 : buf1)") + "    }\n";
+        s += "    cp_async_commit();\n    cp_async_wait_prev();\n    __syncthreads();\n";
+        s += "    {\n" + pro;
+        for (const std::string& ph : seg_ph) s += ph + "    __syncthreads();\n";
+        s += seg_out + "    }\n    __syncthreads();\n";
+        s += "    cta = nxt;\n    if (cta >= ntiles) break;\n    }\n}\n";
+    }
 
     if (host) {
         // the same segments, threads of a CTA run one after another between barriers

@@ -186,6 +186,7 @@ int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 #define GQ_OPT_JIT 9
 #define GQ_OPT_JIT_MIN_QUBITS 10 /* smallest state (physical qubits) that uses them (default 20) */
 #define GQ_OPT_JIT_MIN_BLOCKS 11 /* their CTAs per SM (register bound); 0 = the launch shape's */
+#define GQ_OPT_JIT_PERSISTENT 12 /* 1: persistent CTAs prefetching the next tile; 0: one CTA per tile (default) */
 int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
 
 /* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */
