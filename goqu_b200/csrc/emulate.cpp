@@ -346,7 +346,7 @@ int gqx_jit_check(int nq, int precision, const gq_op* ops, size_t n_ops, int til
     for (size_t i = 0; i < prog.passes.size(); ++i) {
         gq::JitPlan pl;
         const int threads = 1 << (prog.passes[i].m - gq::RQ);
-        if (!gq::jit_plan(prog, i, precision == GQ_C64, threads, precision == GQ_C64 ? 4 : 3, true, pl)) continue;
+        if (!gq::jit_plan(prog, i, precision == GQ_C64, threads, 4, false, pl)) continue;  // the engine's default shape
         ++planned;
         if (!texts.insert(pl.source).second || compiled >= max_compile) continue;
         std::string log;
