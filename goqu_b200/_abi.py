@@ -150,6 +150,10 @@ SIGNATURES = {
     "gq_sv_expect_pauli_sum": (_I, [_VP, _TP, _SZ, _DBL_P, _DBL_P]),
     "gq_sv_expect_z_mask": (_I, [_VP, ctypes.c_uint64, _DBL_P]),
     "gq_sv_adjoint_gradient": (_I, [_VP, _OPP, _SZ, _TP, _SZ, _SZ, _DBL_P, _DBL_P]),
+    "gq_sv_prob0": (_I, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "gq_sv_collapse": (_I, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+    "gq_sv_measure": (_I, [_VP, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
+    "gq_sv_copy_state": (_I, [_VP, _VP]),
     "gq_sv_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
     "gq_sv_set_option": (_I, [_VP, _I, ctypes.c_int64]),
     "gq_dm_create": (_I, [_I, ctypes.POINTER(_VP)]),
@@ -165,6 +169,10 @@ SIGNATURES = {
     "gq_dm_purity": (_I, [_VP, _DBL_P]),
     "gq_dm_fidelity": (_I, [_VP, _DBL_P, _SZ, _DBL_P]),
     "gq_dm_sample": (_I, [_VP, _DBL_P, _DBL_P, _DBL_P, _SZ, _U64P]),
+    "gq_dm_prob0": (_I, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "gq_dm_collapse": (_I, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+    "gq_dm_measure": (_I, [_VP, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
+    "gq_dm_copy_state": (_I, [_VP, _VP]),
     "gq_dm_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
     "gq_dm_set_option": (_I, [_VP, _I, ctypes.c_int64]),
     "gq_batch_create": (_I, [_I, ctypes.POINTER(_VP)]),

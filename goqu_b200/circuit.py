@@ -19,6 +19,33 @@ class Condition:
     value: int
 
 
+# Structured control flow (ir/circuit.go:94-129).
+ControlFlowWhile, ControlFlowFor, ControlFlowSwitch, ControlFlowIfElse = 1, 2, 3, 4
+MaxControlFlowIterations = 1000  # while-loop cap at simulation time
+
+
+@dataclass
+class ForRange:
+    Start: int
+    End: int  # exclusive
+    Step: int
+
+
+@dataclass
+class SwitchArg:
+    Clbits: list
+    Cases: list  # case value of each body, in order
+
+
+@dataclass
+class ControlFlow:
+    Type: int
+    Condition: object = None  # While and IfElse
+    Bodies: list = field(default_factory=list)  # While[0], IfElse[0]/[1], Switch[i] (+ default last)
+    ForRange: object = None
+    SwitchArg: object = None
+
+
 @dataclass
 class Operation:
     Gate: object = None
@@ -214,6 +241,74 @@ class Builder:
 
     def Reset(self, q):
         return self.Apply(_gate.Reset, q)
+
+    # Classical control (builder.go:424-600).
+    def _clbit(self, c):
+        if self._err is None and c < 0:
+            self._err = ValueError(f"clbit {c} out of range")
+        if c >= self._nc:
+            self._nc = c + 1
+        return self._err is None
+
+    def _sub(self, fn):
+        sub = Builder(self._name, self._nq)
+        sub._nc = self._nc
+        fn(sub)
+        if sub._err:
+            self._err = sub._err
+        self._nc = max(self._nc, sub._nc)
+        return sub._ops
+
+    def If(self, clbit, value, g, *qubits):
+        """A gate applied only when clbit == value."""
+        if self._clbit(clbit) and self._check(list(qubits), g.Qubits()):
+            self._ops.append(Operation(g, list(qubits), Condition=Condition(clbit, value)))
+        return self
+
+    def IfBlock(self, clbit, value, fn):
+        """Every op fn adds is conditioned on clbit == value."""
+        if self._clbit(clbit):
+            start = len(self._ops)
+            fn(self)
+            for op in self._ops[start:]:
+                op.Condition = Condition(clbit, value)
+        return self
+
+    def IfElseBlock(self, clbit, value, if_body, else_body):
+        if self._clbit(clbit):
+            a, b = self._sub(if_body), self._sub(else_body)
+            self._ops.append(Operation(ControlFlow=ControlFlow(ControlFlowIfElse, Condition(clbit, value), [a, b])))
+        return self
+
+    def While(self, clbit, value, body):
+        if self._clbit(clbit):
+            ops = self._sub(body)
+            self._ops.append(Operation(ControlFlow=ControlFlow(ControlFlowWhile, Condition(clbit, value), [ops])))
+        return self
+
+    def For(self, clbit, start, end, step, body):
+        if self._clbit(clbit):
+            if step == 0:
+                self._err = ValueError("for loop step must be non-zero")
+                return self
+            ops = self._sub(body)
+            self._ops.append(Operation(ControlFlow=ControlFlow(ControlFlowFor, None, [ops],
+                                                               ForRange=ForRange(start, end, step))))
+        return self
+
+    def Switch(self, clbits, cases, default_body=None):
+        """cases: {value: body}; bodies in ascending case value, default last."""
+        for c in clbits:
+            self._clbit(c)
+        if self._err:
+            return self
+        vals = sorted(cases)
+        bodies = [self._sub(cases[v]) for v in vals]
+        if default_body is not None:
+            bodies.append(self._sub(default_body))
+        self._ops.append(Operation(ControlFlow=ControlFlow(ControlFlowSwitch, None, bodies,
+                                                           SwitchArg=SwitchArg(list(clbits), vals))))
+        return self
 
     def Delay(self, q, duration, unit="ns"):
         return self.Apply(_gate.Delay(duration, unit), q)

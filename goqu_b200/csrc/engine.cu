@@ -763,6 +763,62 @@ int gq_sv_expect_z_mask(gq_sv* sv, uint64_t mask, double* out) {
     return gq_sv_expect_pauli_sum(sv, &t, 1, out, nullptr);
 }
 
+int gq_sv_prob0(gq_sv* sv, int qubit, double* p0) {
+    if (!sv || !p0) return fail(GQ_EINVAL, "null argument");
+    if (qubit < 0 || qubit >= sv->nq) return fail(GQ_EINVAL, "qubit out of range");
+    Engine& e = sv->e;
+    const int nb = e.reduce_grid();
+    GQ_TRY(e.scratch.ensure((nb + 1) * sizeof(double2)));
+    const uint64_t na = 1ull << sv->nq;
+    if (e.prec == GQ_C64)
+        k_prob_bit<float><<<nb, 256, 0, e.stream>>>((const cplx<float>*)e.state.p, na, qubit, (double2*)e.scratch.p);
+    else
+        k_prob_bit<double><<<nb, 256, 0, e.stream>>>((const cplx<double>*)e.state.p, na, qubit, (double2*)e.scratch.p);
+    GQ_CUDA(cudaGetLastError());
+    return e.finish_reduce(nb, p0, nullptr);
+}
+
+int gq_sv_collapse(gq_sv* sv, int qubit, int outcome, double p0) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    if (qubit < 0 || qubit >= sv->nq) return fail(GQ_EINVAL, "qubit out of range");
+    if (outcome != 0 && outcome != 1) return fail(GQ_EINVAL, "outcome must be 0 or 1");
+    // dynamic.go:203-229: norm from prob0 (1 - prob0 for outcome 1); a
+    // norm below 1e-15 means the outcome was certain and nothing changes
+    const double norm = outcome == 0 ? std::sqrt(p0) : std::sqrt(1.0 - p0);
+    if (!(norm >= 1e-15)) return GQ_OK;
+    Engine& e = sv->e;
+    const uint64_t na = 1ull << sv->nq;
+    const int nb = e.reduce_grid();
+    if (e.prec == GQ_C64)
+        k_collapse<float><<<nb, 256, 0, e.stream>>>((cplx<float>*)e.state.p, na, qubit, outcome, 1.0 / norm);
+    else
+        k_collapse<double><<<nb, 256, 0, e.stream>>>((cplx<double>*)e.state.p, na, qubit, outcome, 1.0 / norm);
+    GQ_CUDA(cudaGetLastError());
+    e.stats.kernel_launches += 1;
+    return GQ_OK;
+}
+
+int gq_sv_measure(gq_sv* sv, int qubit, double u, int* outcome) {
+    if (!sv || !outcome) return fail(GQ_EINVAL, "null argument");
+    double p0 = 0.0;
+    GQ_TRY(gq_sv_prob0(sv, qubit, &p0));
+    *outcome = u >= p0 ? 1 : 0;  // dynamic.go:197-200
+    return gq_sv_collapse(sv, qubit, *outcome, p0);
+}
+
+int gq_sv_copy_state(gq_sv* dst, const gq_sv* src) {
+    if (!dst || !src) return fail(GQ_EINVAL, "null handle");
+    if (dst->nq != src->nq || dst->e.prec != src->e.prec)
+        return fail(GQ_EINVAL, "handles differ in qubit count or precision");
+    if (dst == src) return GQ_OK;
+    // both streams are idle on return, so either state may be changed next
+    GQ_CUDA(cudaStreamSynchronize(src->e.stream));
+    GQ_CUDA(cudaMemcpyAsync(dst->e.state.p, src->e.state.p, src->e.n_amps * src->e.amp_bytes(),
+                            cudaMemcpyDeviceToDevice, dst->e.stream));
+    GQ_CUDA(cudaStreamSynchronize(dst->e.stream));
+    return GQ_OK;
+}
+
 int gq_sv_stats(const gq_sv* sv, gq_stats* out) {
     if (!sv || !out) return fail(GQ_EINVAL, "null argument");
     *out = sv->e.get_stats();
@@ -1083,6 +1139,53 @@ int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* 
         }
     GQ_CUDA(cudaGetLastError());
     return e.sample_impl(ProbArray{a}, dim, uniforms, shots, idx_out);
+}
+
+int gq_dm_prob0(gq_dm* dm, int qubit, double* p0) {
+    if (!dm || !p0) return fail(GQ_EINVAL, "null argument");
+    if (qubit < 0 || qubit >= dm->nq) return fail(GQ_EINVAL, "qubit out of range");
+    Engine& e = dm->e;
+    const int nb = e.reduce_grid();
+    GQ_TRY(e.scratch.ensure((nb + 1) * sizeof(double2)));
+    k_dm_prob_bit<<<nb, 256, 0, e.stream>>>((const cplx<double>*)e.state.p, 1ull << dm->nq, qubit,
+                                            (double2*)e.scratch.p);
+    GQ_CUDA(cudaGetLastError());
+    return e.finish_reduce(nb, p0, nullptr);
+}
+
+int gq_dm_collapse(gq_dm* dm, int qubit, int outcome, double p0) {
+    if (!dm) return fail(GQ_EINVAL, "null handle");
+    if (qubit < 0 || qubit >= dm->nq) return fail(GQ_EINVAL, "qubit out of range");
+    if (outcome != 0 && outcome != 1) return fail(GQ_EINVAL, "outcome must be 0 or 1");
+    // dynamic.go:231-254: divide by the outcome's probability (1 - prob0 for
+    // outcome 1); below 1e-15 the outcome was certain and nothing changes
+    const double p = outcome == 0 ? p0 : 1.0 - p0;
+    if (!(p >= 1e-15)) return GQ_OK;
+    Engine& e = dm->e;
+    k_dm_collapse<<<e.reduce_grid(), 256, 0, e.stream>>>((cplx<double>*)e.state.p, 1ull << dm->nq, qubit, outcome,
+                                                         1.0 / p);
+    GQ_CUDA(cudaGetLastError());
+    e.stats.kernel_launches += 1;
+    return GQ_OK;
+}
+
+int gq_dm_measure(gq_dm* dm, int qubit, double u, int* outcome) {
+    if (!dm || !outcome) return fail(GQ_EINVAL, "null argument");
+    double p0 = 0.0;
+    GQ_TRY(gq_dm_prob0(dm, qubit, &p0));
+    *outcome = u >= p0 ? 1 : 0;
+    return gq_dm_collapse(dm, qubit, *outcome, p0);
+}
+
+int gq_dm_copy_state(gq_dm* dst, const gq_dm* src) {
+    if (!dst || !src) return fail(GQ_EINVAL, "null handle");
+    if (dst->nq != src->nq) return fail(GQ_EINVAL, "handles differ in qubit count");
+    if (dst == src) return GQ_OK;
+    GQ_CUDA(cudaStreamSynchronize(src->e.stream));
+    GQ_CUDA(cudaMemcpyAsync(dst->e.state.p, src->e.state.p, src->e.n_amps * src->e.amp_bytes(),
+                            cudaMemcpyDeviceToDevice, dst->e.stream));
+    GQ_CUDA(cudaStreamSynchronize(dst->e.stream));
+    return GQ_OK;
 }
 
 int gq_dm_stats(const gq_dm* dm, gq_stats* out) {

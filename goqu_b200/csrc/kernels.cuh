@@ -530,6 +530,72 @@ __device__ __forceinline__ void block_reduce_store(double re, double im, double2
     }
 }
 
+// Projective measurement of qubit q (measureQubit, sim/statevector/dynamic.go:
+// 179-230): per block, the sums of |a_i|^2 over the amplitudes with bit q
+// clear (x) and set (y).
+template <class T>
+__global__ void k_prob_bit(const cplx<T>* __restrict__ st, uint64_t n, int q, double2* __restrict__ partial) {
+    double p0 = 0.0, p1 = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const cplx<T> a = st[i];
+        const double p = (double)a.x * (double)a.x + (double)a.y * (double)a.y;
+        if ((i >> q) & 1ull)
+            p1 += p;
+        else
+            p0 += p;
+    }
+    block_reduce_store(p0, p1, partial);
+}
+
+// Collapse onto `outcome` of qubit q: amplitudes with the other bit value are
+// zeroed, the rest scaled by `scale` (1 / sqrt of the outcome's probability).
+template <class T>
+__global__ void k_collapse(cplx<T>* __restrict__ st, uint64_t n, int q, int outcome, double scale) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        cplx<T> a = st[i];
+        if ((int)((i >> q) & 1ull) == outcome) {
+            a.x = (T)((double)a.x * scale);
+            a.y = (T)((double)a.y * scale);
+        } else {
+            a.x = T(0);
+            a.y = T(0);
+        }
+        st[i] = a;
+    }
+}
+
+// measureQubitDM (sim/densitymatrix/dynamic.go:198-255): per block, the sums
+// of rho[i,i] over i with bit q clear (x) and set (y).
+__global__ void k_dm_prob_bit(const cplx<double>* __restrict__ rho, uint64_t dim, int q, double2* __restrict__ partial) {
+    double p0 = 0.0, p1 = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double d = rho[i * dim + i].x;
+        if ((i >> q) & 1ull)
+            p1 += d;
+        else
+            p0 += d;
+    }
+    block_reduce_store(p0, p1, partial);
+}
+
+// Projection onto `outcome` of qubit q: rho[r,c] kept (times `scale`) where
+// both r and c have bit q equal to the outcome, zeroed elsewhere.
+__global__ void k_dm_collapse(cplx<double>* __restrict__ rho, uint64_t dim, int q, int outcome, double scale) {
+    const uint64_t n = dim * dim;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = i / dim, c = i % dim;
+        cplx<double> a = rho[i];
+        if ((int)((r >> q) & 1ull) == outcome && (int)((c >> q) & 1ull) == outcome) {
+            a.x *= scale;
+            a.y *= scale;
+        } else {
+            a.x = 0.0;
+            a.y = 0.0;
+        }
+        rho[i] = a;
+    }
+}
+
 // sum_t coeff_t <psi|P_t|psi>: for each amplitude i and each group of terms
 // sharing an x mask, conj(psi[i^x]) psi[i] times sum_t w_t (-1)^popcount(i&z_t)
 // (the formula of pauli.Expect, sim/pauli/expect_sv.go:21-47).

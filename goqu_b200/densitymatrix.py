@@ -69,8 +69,11 @@ class Sim:
         _abi.check(_abi.lib().gq_dm_evolve(self._h, s.ptr(), len(s)))
 
     def Run(self, c, shots, rng=None):
+        """Evolve and sample the readout-mixed diagonal (sim.go:48-66); dynamic
+        circuits run shot groups (RunDynamic, dynamic.go:13-51)."""
         if c.IsDynamic():
-            raise NotImplementedError("densitymatrix: dynamic circuits are not supported by the device engine yet")
+            from . import dynamic
+            return dynamic.run_dynamic_dm(self, c, shots, rng)
         self.Evolve(c)
         return counts_from_indices(self.Sample(uniforms(shots, rng)), self._n)
 

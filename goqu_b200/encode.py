@@ -125,6 +125,9 @@ def density_ops(circuit, noise_model=None):
         g = op.Gate
         if g is None or g.Name() == "barrier":
             continue
+        if getattr(g, "noise_only", None):  # a channel without its gate (dynamic resets)
+            channel(g.noise_only, op.Qubits)
+            continue
         if g.Name() == "delay":
             channel("delay", op.Qubits)
             continue
@@ -143,5 +146,6 @@ def density_ops(circuit, noise_model=None):
             if m is None:
                 continue
             stream.add(g.kind, op.Qubits, m)
-        channel(g.Name(), op.Qubits)
+        if not getattr(g, "noiseless", False):
+            channel(g.Name(), op.Qubits)
     return stream

@@ -169,6 +169,22 @@ int gq_sv_expect_z_mask(gq_sv* sv, uint64_t mask, double* out);
 int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops,
                            const gq_pauli_term* terms, size_t n_terms,
                            size_t n_params, double* grad_out, double* energy_out);
+/* ---- dynamic circuits: replaces measureQubit (sim/statevector/dynamic.go:179-230) ----
+ * The per-shot control flow of RunDynamic (dynamic.go:14-177) stays on the
+ * host; shots sharing a measurement history share one device state. */
+/* P(qubit = 0): sum of |a_i|^2 over the amplitudes with the qubit's bit clear
+ * (dynamic.go:183-194), FP64. */
+int gq_sv_prob0(gq_sv* sv, int qubit, double* p0);
+/* Collapse onto `outcome` given P(0) = p0: the other half is zeroed and the
+ * kept half scaled by 1/sqrt(p0) (outcome 0) or 1/sqrt(1 - p0) (outcome 1);
+ * nothing changes when that norm is below 1e-15 (dynamic.go:203-229). */
+int gq_sv_collapse(gq_sv* sv, int qubit, int outcome, double p0);
+/* measureQubit with the caller's uniform u: outcome 1 iff u >= P(0)
+ * (dynamic.go:197-200), then the collapse. */
+int gq_sv_measure(gq_sv* sv, int qubit, double u, int* outcome);
+/* dst's state <- src's state (same qubit count and precision): the branch
+ * of a measurement history that both outcomes continue from. */
+int gq_sv_copy_state(gq_sv* dst, const gq_sv* src);
 int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 
 /* Engine options (per handle). */
@@ -219,6 +235,14 @@ int gq_dm_fidelity(gq_dm* dm, const double* psi, size_t n, double* out);
  * pairs (ApplyReadoutError, measure.go:29-71); p01[q] < 0 skips qubit q.     */
 int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* uniforms,
                  size_t shots, uint64_t* idx_out);
+/* Dynamic circuits: measureQubitDM (sim/densitymatrix/dynamic.go:198-255).
+ * P(0) = sum of rho[i,i] over i with the qubit's bit clear; the collapse keeps
+ * rho[r,c] with both bits equal to the outcome, divided by its probability
+ * (1 - p0 for outcome 1), unless that probability is below 1e-15. */
+int gq_dm_prob0(gq_dm* dm, int qubit, double* p0);
+int gq_dm_collapse(gq_dm* dm, int qubit, int outcome, double p0);
+int gq_dm_measure(gq_dm* dm, int qubit, double u, int* outcome);
+int gq_dm_copy_state(gq_dm* dst, const gq_dm* src);
 int gq_dm_stats(const gq_dm* dm, gq_stats* out);
 int gq_dm_set_option(gq_dm* dm, int key, int64_t value);
 

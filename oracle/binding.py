@@ -174,3 +174,18 @@ def dm_readout(probs, nq, p01, p10):
     b = np.ascontiguousarray(p10, dtype=np.float64)
     lib().or_dm_readout(nq, _dp(probs), _dp(a), _dp(b))
     return probs
+
+
+def sv_measure(state, qubit, u):
+    """measureQubit with uniform u (in place); returns the outcome."""
+    lib().or_sv_measure.restype = ctypes.c_int
+    lib().or_sv_measure.argtypes = [ctypes.c_int, _D, ctypes.c_int, ctypes.c_double]
+    nq = state.size.bit_length() - 1
+    return lib().or_sv_measure(nq, _dp(state.view(np.float64)), qubit, u)
+
+
+def dm_measure(rho, nq, qubit, u):
+    """measureQubitDM with uniform u (in place); returns the outcome."""
+    lib().or_dm_measure.restype = ctypes.c_int
+    lib().or_dm_measure.argtypes = [ctypes.c_int, _D, ctypes.c_int, ctypes.c_double]
+    return lib().or_dm_measure(nq, _dp(rho.view(np.float64)), qubit, u)

@@ -634,6 +634,67 @@ void or_sv_probabilities(int nq, const double* state, double* probs) {
     for (long long i = 0; i < n; ++i) probs[i] = st[i].re * st[i].re + st[i].im * st[i].im;
 }
 
+// measureQubit (sim/statevector/dynamic.go:179-230) with a caller-supplied
+// uniform in place of the shot's PCG draw: P(0) summed over the blocks in
+// index order, outcome 1 iff u >= P(0), then zero the other half and scale
+// the kept half by 1/norm unless norm < 1e-15. Returns the outcome.
+int or_sv_measure(int nq, double* state, int qubit, double u) {
+    const long long half = 1LL << qubit, block = half << 1, n = 1LL << nq;
+    cd* st = C(state);
+    double p0 = 0.0;
+    for (long long b0 = 0; b0 < n; b0 += block)
+        for (long long off = 0; off < half; ++off) {
+            const cd a = st[b0 + off];
+            p0 += a.re * a.re + a.im * a.im;
+        }
+    const int outcome = u >= p0 ? 1 : 0;
+    const double norm = outcome == 0 ? std::sqrt(p0) : std::sqrt(1 - p0);
+    if (norm < 1e-15) return outcome;
+    const double inv = 1.0 / norm;
+    for (long long b0 = 0; b0 < n; b0 += block)
+        for (long long off = 0; off < half; ++off) {
+            cd& a0 = st[b0 + off];
+            cd& a1 = st[b0 + off + half];
+            if (outcome == 0) {
+                a0 = {a0.re * inv, a0.im * inv};
+                a1 = {0.0, 0.0};
+            } else {
+                a0 = {0.0, 0.0};
+                a1 = {a1.re * inv, a1.im * inv};
+            }
+        }
+    return outcome;
+}
+
+// measureQubitDM (sim/densitymatrix/dynamic.go:198-255) with a caller-supplied
+// uniform: P(0) = sum of Re rho[i,i] over i with the bit clear (index order),
+// outcome 1 iff u >= P(0); entries with both row and column bit equal to the
+// outcome are divided by its probability, the others zeroed, unless that
+// probability is below 1e-15. Returns the outcome.
+int or_dm_measure(int nq, double* rho_, int qubit, double u) {
+    const long long dim = 1LL << nq, mask = 1LL << qubit;
+    cd* rho = C(rho_);
+    double p0 = 0.0;
+    for (long long i = 0; i < dim; ++i)
+        if (!(i & mask)) p0 += rho[i * dim + i].re;
+    const int outcome = u >= p0 ? 1 : 0;
+    const double p = outcome == 0 ? p0 : 1 - p0;
+    if (p < 1e-15) return outcome;
+    const double inv = 1.0 / p;
+    for (long long r = 0; r < dim; ++r) {
+        const int rb = (int)((r >> qubit) & 1);
+        for (long long c = 0; c < dim; ++c) {
+            const int cb = (int)((c >> qubit) & 1);
+            cd& a = rho[r * dim + c];
+            if (rb == outcome && cb == outcome)
+                a = {a.re * inv, a.im * inv};
+            else
+                a = {0.0, 0.0};
+        }
+    }
+    return outcome;
+}
+
 // sampleIndex (sim/statevector/sim.go:288-298) for caller-supplied uniforms.
 void or_sample(const double* probs, uint64_t len, const double* uniforms, size_t shots, uint64_t* out) {
     for (size_t k = 0; k < shots; ++k) {
