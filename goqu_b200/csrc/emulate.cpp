@@ -110,15 +110,17 @@ int run_program_jit(std::vector<gq::cplx<T>>& st, const gq::Program& prog, bool 
         PassFn fn = nullptr;
         if (ok[i]) {
             block.resize(plans[i].n_param);
-            if (gq::jit_pack(prog, plans[i], c64, block.data()))
+            if (gq::jit_pack(prog, i, plans[i], c64, block.data()))
                 fn = (PassFn)dlsym(h, ("gqj_host_" + std::to_string(i)).c_str());
         }
         if (!fn) {
             run_pass<T>(st, prog, pool, i);
             continue;
         }
+        uint32_t op_base, pool_base;
+        gq::jit_bases(prog, i, &op_base, &pool_base);
         std::vector<gq::cplx<T>> sm(1u << prog.passes[i].m);
-        fn(st.data(), block.data(), pool.data(), prog.phases.data(), sm.data());
+        fn(st.data(), block.data(), pool.data() + pool_base, prog.phases.data() + prog.passes[i].phase0, sm.data());
         ++*jitted;
     }
     dlclose(h);

@@ -307,9 +307,8 @@ struct Engine {
         // (or, with GQ_OPT_JIT = 2, once it has); the others run interpreted.
         const size_t np = pr.passes.size();
         std::vector<const void*> jfn(np, nullptr);
-        std::vector<JitPlan> plans;
+        std::vector<const CachedPlan*> plans(np, nullptr);
         if (jit_mode != 0 && nphys >= jit_min_qubits && jit_available()) {
-            plans.resize(np);
             // One tile per CTA: 4 CTAs of 128 threads per SM (128 registers)
             // measured fastest for both precisions. Persistent: as many CTAs
             // per SM as two tile buffers each allow (3 for complex128).
@@ -318,18 +317,15 @@ struct Engine {
             if (jit_persistent) minb = std::max(1, std::min(minb, (int)((227u << 10) / (2 * (sizeof(cplx<T>) << max_tile())))));
             if (jit_min_blocks > 0) minb = jit_min_blocks;
             jit_minb = minb;
-            std::vector<char> planned(np, 0);
             for (size_t i = 0; i < np; ++i) {
                 const PassDesc& pd = pr.passes[i];
-                if (!jit_plan(pr, i, prec == GQ_C64, 1 << (pd.m - RQ), minb, jit_persistent != 0, plans[i])) continue;
-                planned[i] = 1;
-                jit_lookup(plans[i].source, jit_smem<T>(pd.m), true, &jfn[i]);
+                plans[i] = jit_cached_plan(pr, i, prec == GQ_C64, 1 << (pd.m - RQ), minb, jit_persistent != 0);
+                if (plans[i]->ok) jfn[i] = jit_plan_kernel(plans[i], jit_smem<T>(pd.m));
             }
             if (jit_mode == 2) {
                 jit_wait(600000.0);
                 for (size_t i = 0; i < np; ++i)
-                    if (planned[i] && !jfn[i])
-                        jit_lookup(plans[i].source, jit_smem<T>(pr.passes[i].m), false, &jfn[i]);
+                    if (plans[i]->ok && !jfn[i]) jfn[i] = jit_plan_kernel(plans[i], jit_smem<T>(pr.passes[i].m));
             }
         }
         if (timing) GQ_CUDA(cudaEventRecord(ev_pass0, stream));
@@ -340,11 +336,13 @@ struct Engine {
             const unsigned threads = 1u << (pd.m - RQ);
             const size_t smem = sizeof(cplx<T>) << pd.m;
             const unsigned grid = 1u << pd.n_outer;
-            if (jfn[i]) pblock.resize(plans[i].n_param);
-            if (jfn[i] && jit_pack(pr, plans[i], prec == GQ_C64, pblock.data())) {
+            if (jfn[i]) pblock.resize(plans[i]->plan.n_param);
+            if (jfn[i] && jit_pack(pr, i, plans[i]->plan, prec == GQ_C64, pblock.data())) {
+                uint32_t op_base, pool_base;
+                jit_bases(pr, i, &op_base, &pool_base);
                 cplx<T>* stp = (cplx<T>*)state.p;
-                const cplx<T>* poolp = (const cplx<T>*)(d + o_pool);
-                const PhaseDesc* php = (const PhaseDesc*)(d + o_phase);
+                const cplx<T>* poolp = (const cplx<T>*)(d + o_pool) + pool_base;
+                const PhaseDesc* php = (const PhaseDesc*)(d + o_phase) + pd.phase0;
                 void* args[4] = {&stp, pblock.data(), &poolp, &php};
                 const unsigned jgrid =
                     jit_persistent ? (unsigned)std::min<uint64_t>(grid, (uint64_t)num_sms * jit_minb) : grid;

@@ -68,14 +68,37 @@ struct JitPlan {
 // parameter block over the kernel-parameter limit): they stay interpreted.
 bool jit_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks, bool persistent, JitPlan& out,
               bool host = false);
+// Op and pool indices in a plan and its kernel text are relative to the
+// pass: to its first op and that op's first pool entry (jit_bases). The
+// kernel is launched with `pool` advanced by pool_base and `phases` by the
+// pass's phase0, so passes of the same structure anywhere in any program
+// share a plan and a kernel.
+void jit_bases(const Program& pr, size_t pass, uint32_t* op_base, uint32_t* pool_base);
 // Fills the parameter block (n_param complex values of float or double) from
-// the program's current numbers. Returns false when the pass's shears could
-// leave the floating-point range; the pass then runs interpreted.
-bool jit_pack(const Program& pr, const JitPlan& plan, bool c64, void* block);
+// pass `pass` of the program's current numbers. Returns false when the pass's
+// shears could leave the floating-point range; the pass then runs interpreted.
+bool jit_pack(const Program& pr, size_t pass, const JitPlan& plan, bool c64, void* block);
 // Decomposition of a one-qubit unitary m (row major) into the shear form
 // above. False when m is not unitary to 1e-12 or cos / sin(theta/2) is below
 // 1e-150 (the generator then keeps the dense 2x2).
 bool u1_decompose(const Z* m, double* t, Z* lam, Z* post0, Z* post1);
+
+// A pass's plan as cached per process, keyed by the pass's structure (launch
+// shape, tile and phase tables, op kinds, bits, controls, relative pool
+// offsets, which one-qubit unitaries decompose): every pass of that
+// structure reuses the text and, once compiled, the kernel, without
+// generating the text again.
+struct CachedPlan {
+    bool ok = false;        // jit_plan covered the pass
+    JitPlan plan;
+    const void* fn = nullptr;  // compiled kernel, once ready
+    bool failed = false;    // compilation or loading failed
+};
+const CachedPlan* jit_cached_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks,
+                                  bool persistent);
+// The compiled kernel of a cached plan (queues its compilation on first call);
+// nullptr until it is ready.
+const void* jit_plan_kernel(const CachedPlan* cp, size_t smem_bytes);
 
 // Process-wide cache of compiled kernels, keyed by kernel text.
 enum JitState { JIT_MISSING = 0, JIT_PENDING = 1, JIT_READY = 2, JIT_FAILED = 3 };

@@ -136,9 +136,18 @@ bool u1_decompose(const Z* m, double* t, Z* lam, Z* post0, Z* post1) {
     return true;
 }
 
+void jit_bases(const Program& pr, size_t pi, uint32_t* op_base, uint32_t* pool_base) {
+    const PassDesc& pd = pr.passes[pi];
+    const uint32_t ob = pd.n_phases > 0 ? (uint32_t)pr.phases[pd.phase0].op_begin : 0;
+    *op_base = ob;
+    *pool_base = ob < pr.ops.size() ? pr.ops[ob].mat : 0;
+}
+
 bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, bool persistent, JitPlan& out,
               bool host) {
     const PassDesc& pd = pr.passes[pi];
+    uint32_t op_base, pool_base;
+    jit_bases(pr, pi, &op_base, &pool_base);
     const int m = pd.m, tbits = m - RQ;
     if (tbits < 0 || (1 << tbits) != threads) return false;
     out.atoms.clear();
@@ -181,8 +190,7 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
 
     std::vector<std::string> seg_ph;
     for (int p = 0; p < pd.n_phases; ++p) {
-        const int phi = pd.phase0 + p;
-        const PhaseDesc& ph = pr.phases[phi];
+        const PhaseDesc& ph = pr.phases[pd.phase0 + p];
         out.phase_shears.emplace_back();
         uint32_t tslot[MAX_TILE];
         int tq[MAX_TILE];
@@ -239,9 +247,12 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
             pend[j].clear();
         };
 
-        for (int o = ph.op_begin; o < ph.op_end; ++o) {
-            const KOp& op = pr.ops[o];
+        for (int oa = ph.op_begin; oa < ph.op_end; ++oa) {
+            const KOp& op = pr.ops[oa];
             if (op.type == K_GRAD || op.type == K_NONE || op.type > K_RESET) return false;
+            // indices relative to the pass (its first op and first pool entry),
+            // so the kernel text and plan do not depend on the pass's position
+            const uint32_t o = (uint32_t)oa - op_base, rm = op.mat - pool_base;
             const std::string creg = num(op.creg) + "u";
             const std::string C = op.creg ? "true" : "false";
             std::string cond;
@@ -271,7 +282,7 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                         out.phase_shears.back().push_back((uint32_t)o);
                     } else {
                         for (const auto& g : groups(tm, op.creg)) normalize(g);
-                        b += "        " + cond + "k_u1<T, " + S0 + ", " + C + ">(a, " + pm(gen.copy(op.mat, 4)) +
+                        b += "        " + cond + "k_u1<T, " + S0 + ", " + C + ">(a, " + pm(gen.copy(rm, 4)) +
                              ", " + creg + ");\n";
                     }
                     break;
@@ -279,17 +290,17 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                 case K_U2:
                     for (const auto& g : groups((1u << op.t0) | (1u << op.t1), op.creg)) normalize(g);
                     b += "        " + cond + "k_u2<T, " + S0 + ", " + S1 + ", " + C + ">(a, " +
-                         pm(gen.copy(op.mat, 16)) + ", " + creg + ");\n";
+                         pm(gen.copy(rm, 16)) + ", " + creg + ");\n";
                     break;
                 case K_U3:
                     for (const auto& g : groups((1u << op.t0) | (1u << op.t1) | (1u << op.t2), op.creg)) normalize(g);
                     b += "        " + cond + "k_u3<T, " + S0 + ", " + S1 + ", " + S2 + ">(a, " +
-                         pm(gen.copy(op.mat, 64)) + ", " + creg + ");\n";
+                         pm(gen.copy(rm, 64)) + ", " + creg + ");\n";
                     break;
                 case K_U4:
                     for (const auto& g : groups(15u, 0u)) normalize(g);
-                    b += "        " + cond + "k_u4<T>(a, " + pm(gen.copy(op.mat, 256)) + ", sm, sb, phases[" +
-                         num(phi) + "].rslot);\n";
+                    b += "        " + cond + "k_u4<T>(a, " + pm(gen.copy(rm, 256)) + ", sm, sb, phases[" + num(p) +
+                         "].rslot);\n";
                     break;
                 case K_X: {
                     const uint32_t tm = 1u << op.t0;
@@ -297,7 +308,7 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                     if (op.cmask) {
                         for (const auto& g : groups(tm, op.creg)) normalize(g);
                         b += "        " + cond + "k_x<T, " + S0 + ", " + C + ">(a, " +
-                             (pure ? std::string("pool") : pm(gen.copy(op.mat, 2))) + ", " + creg + ", " +
+                             (pure ? std::string("pool") : pm(gen.copy(rm, 2))) + ", " + creg + ", " +
                              (pure ? "true" : "false") + ");\n";
                     } else {
                         // a compile-time permutation; the phases p0, p1 become pending factors
@@ -305,8 +316,8 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                         for (const auto& g : groups(tm, op.creg)) {
                             std::swap(pend[g[0]], pend[g[1]]);
                             if (!pure) {
-                                pend_add(pend[g[0]], gen.atom(0, op.mat));
-                                pend_add(pend[g[1]], gen.atom(0, op.mat + 1));
+                                pend_add(pend[g[0]], gen.atom(0, rm));
+                                pend_add(pend[g[1]], gen.atom(0, rm + 1));
                             }
                         }
                     }
@@ -328,10 +339,10 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                 }
                 case K_PHASE:
                     if (op.cmask) {
-                        b += "        " + cond + "k_phase<T>(a, p.m[" + num(gen.copy(op.mat, 1)) + "], " + creg +
+                        b += "        " + cond + "k_phase<T>(a, p.m[" + num(gen.copy(rm, 1)) + "], " + creg +
                              ");\n";
                     } else {
-                        const uint32_t a_s = gen.atom(0, op.mat);
+                        const uint32_t a_s = gen.atom(0, rm);
                         for (int j = 0; j < NREG; ++j)
                             if ((j & op.creg) == op.creg) pend_add(pend[j], a_s);
                     }
@@ -342,13 +353,13 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                         int k = 0;
                         for (uint64_t dm = op.dmask; dm; dm &= dm - 1, ++k)
                             h += "hi |= (uint32_t)((g0 >> " + num(ctz64(dm)) + ") & 1ull) << " + num(k) + "; ";
-                        h += "k_diag_hi<T>(a, pool + " + num(op.mat) + "u, hi << " + num(op.nreg) + ", " +
+                        h += "k_diag_hi<T>(a, pool + " + num(rm) + "u, hi << " + num(op.nreg) + ", " +
                              num(op.nreg) + "u, " + creg + ", " + hex64(op.ridx) + "); }";
                         b += "        " + cond + h + "\n";
                     } else {
                         for (int j = 0; j < NREG; ++j)
                             if ((j & op.creg) == op.creg)
-                                pend_add(pend[j], gen.atom(0, op.mat + (uint32_t)((op.ridx >> (4 * j)) & 15u)));
+                                pend_add(pend[j], gen.atom(0, rm + (uint32_t)((op.ridx >> (4 * j)) & 15u)));
                     }
                     break;
                 case K_RESET:
@@ -436,14 +447,17 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
     return true;
 }
 
-bool jit_pack(const Program& pr, const JitPlan& plan, bool c64, void* block) {
+bool jit_pack(const Program& pr, size_t pi, const JitPlan& plan, bool c64, void* block) {
+    uint32_t op_base, pool_base;
+    jit_bases(pr, pi, &op_base, &pool_base);
+    const size_t nops = pr.ops.size() - op_base;
     // atom values
     std::vector<Z> av(plan.atoms.size());
-    std::vector<double> tv(pr.ops.size(), 0.0);
-    std::vector<char> have(pr.ops.size(), 0);
+    std::vector<double> tv(nops, 0.0);
+    std::vector<char> have(nops, 0);
     auto dec = [&](uint32_t o, Z* lam, Z* p0, Z* p1) {
         double t;
-        if (!u1_decompose(&pr.pool[pr.ops[o].mat], &t, lam, p0, p1)) return false;
+        if (o >= nops || !u1_decompose(&pr.pool[pr.ops[op_base + o].mat], &t, lam, p0, p1)) return false;
         tv[o] = t;
         have[o] = 1;
         return true;
@@ -451,7 +465,7 @@ bool jit_pack(const Program& pr, const JitPlan& plan, bool c64, void* block) {
     for (size_t i = 0; i < plan.atoms.size(); ++i) {
         const JitAtom& a = plan.atoms[i];
         if (a.kind == 0) {
-            av[i] = pr.pool[a.ref];
+            av[i] = pr.pool[pool_base + a.ref];
             continue;
         }
         Z lam, p0, p1;
@@ -463,6 +477,7 @@ bool jit_pack(const Program& pr, const JitPlan& plan, bool c64, void* block) {
     for (const auto& ph : plan.phase_shears) {
         double lg = 0;
         for (uint32_t o : ph) {
+            if (o >= nops) return false;
             if (!have[o]) {
                 Z l, a, b;
                 if (!dec(o, &l, &a, &b)) return false;
@@ -475,7 +490,7 @@ bool jit_pack(const Program& pr, const JitPlan& plan, bool c64, void* block) {
     vals.reserve(plan.n_param);
     for (const JitEntry& e : plan.entries) {
         if (e.kind == 0) {
-            for (uint32_t k = 0; k < e.count; ++k) vals.push_back(pr.pool[e.ref + k]);
+            for (uint32_t k = 0; k < e.count; ++k) vals.push_back(pr.pool[pool_base + e.ref + k]);
         } else if (e.kind == 1) {
             if (!have[e.ref]) {
                 Z l, a, b;
