@@ -343,8 +343,8 @@ def run_gpu(args, world, rank, local):
         with open(tf) as f:
             tj = json.load(f)
         t = tj.get(args.precision, {})
-        if t.get("bytes_per_launch_24q"):
-            traffic = t["bytes_per_launch_24q"] * float(1 << (n - 24))  # traffic scales with 2^n
+        if t.get("bytes_per_launch"):
+            traffic = t["bytes_per_launch"] * 2.0 ** (n - t["qubits"])  # traffic scales with 2^n
 
     line = {
         "metric": f"{n}q gates/s", "value": value, "unit": "gates/s", "n_gpus": world, "steps": args.steps,
