@@ -353,14 +353,19 @@ __global__ void k_chunk_steps(P prob, uint64_t n, int chunk_log, const double* _
                               long long* __restrict__ steps, int* __restrict__ cexp, int* __restrict__ clean) {
     const uint64_t c = blockIdx.x;
     const double s0 = c ? incl[c - 1] : 0.0, s1 = incl[c];
-    // Predicted binade of the whole chunk, with a margin far above the error
-    // of the approximate sums (~1e-12 relative).
+    // Predicted binade of the whole chunk: that of the approximate sum before
+    // it, with the chunk's end kept below the binade's top by a margin far
+    // above the error of the approximate sums (~1e-12 relative).
+    // (The walk checks the exact running sum's binade and end, so a wrong
+    // prediction only sends the chunk to the element-by-element path; s0 on
+    // a power of two, as after a basis state, is the common case that must
+    // stay clean.)
     bool ok = s0 > 0x1p-1000;
     int e = 0;
     if (ok) {
         e = exponent_of(s0);
-        const double lo = ldexp(1.0, e), hi = ldexp(1.0, e + 1);
-        ok = s0 >= lo * (1.0 + 0x1p-30) && s1 <= hi * (1.0 - 0x1p-30);
+        const double hi = ldexp(1.0, e + 1);
+        ok = s1 <= hi * (1.0 - 0x1p-30);
     }
     if (!ok) {
         if (threadIdx.x == 0) {
@@ -409,62 +414,88 @@ __global__ void k_chunk_steps(P prob, uint64_t n, int chunk_log, const double* _
     }
 }
 
-// One warp walks the chunks 32 at a time. When the running sum s and all 32
-// chunks of a group are clean in s's binade, their ends are s plus u times
-// the group's int64 inclusive prefix (exact while below 2^(e+1)); otherwise
-// the group is walked chunk by chunk, non-clean chunks element by element.
+// One warp walks the chunks with the exact running sum s, a window of
+// 32 x kWalkK chunks at a time (kWalkK consecutive chunks per lane, loaded
+// together). A chunk is taken in O(1) when it is clean in s's binade and
+// s plus its exact step count stays below 2^(e+1): the ends of the window's
+// leading run of such chunks are s plus the int64 window prefix times the
+// ulp of the binade (exact). The first chunk after that run is summed
+// element by element with goqu's own additions (the warp loads 32 elements
+// at a time; every lane adds them in order, so s stays warp-uniform); then
+// the next window starts after it.
+constexpr int kWalkK = 8;
+
 template <class P>
 __global__ void k_chunk_walk(P prob, uint64_t n, int chunk_log, const long long* __restrict__ steps,
                              const int* __restrict__ cexp, const int* __restrict__ clean, uint64_t nchunks,
                              double* __restrict__ ends, int* __restrict__ n_seq) {
     if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x;
+    constexpr int W = 32 * kWalkK;
     double s = 0.0;
     int seq = 0;
     const uint64_t len = (uint64_t)1 << chunk_log;
-    for (uint64_t g = 0; g < nchunks; g += 32) {
-        const uint64_t c = g + lane;
-        const bool in = c < nchunks;
-        const long long st = in ? steps[c] : 0;
-        const int e = in ? cexp[c] : 0;
-        const int cl = in ? clean[c] : 1;
-        // inclusive int64 prefix over the lanes
-        long long pre = st;
+    uint64_t c = 0;
+    while (c < nchunks) {
+        const bool pos = s > 0.0;
+        const int se = pos ? exponent_of(s) : 0;
+        const double lim = pos ? ldexp(1.0, se + 1) : 0.0;
+        long long st[kWalkK];
+        bool ok[kWalkK];
+        long long lsum = 0;
+#pragma unroll
+        for (int k = 0; k < kWalkK; ++k) {
+            const uint64_t idx = c + (uint64_t)lane * kWalkK + k;
+            const bool in = idx < nchunks;
+            st[k] = in ? steps[idx] : 0;
+            ok[k] = in && pos && clean[idx] && cexp[idx] == se;
+            lsum += st[k];
+        }
+        long long pre = lsum;  // inclusive prefix over the lanes
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const long long y = __shfl_up_sync(0xffffffffu, pre, o);
+            const long long y = __shfl_up_sync(full, pre, o);
             if (lane >= o) pre += y;
         }
-        const int se = s > 0.0 ? exponent_of(s) : -100000;
-        const bool lane_ok = !in || (cl && e == se);
-        const long long total = __shfl_sync(0xffffffffu, pre, 31);
-        bool fast = __all_sync(0xffffffffu, lane_ok) && s > 0.0;
-        if (fast) fast = s + ldexp((double)total, se - 52) < ldexp(1.0, se + 1);
-        if (fast) {
-            if (in) ends[c] = s + ldexp((double)pre, se - 52);
-            s = s + ldexp((double)total, se - 52);
-            continue;
+        // first chunk (window order) that cannot be taken in O(1)
+        long long run = pre - lsum;
+        int bad = W;
+#pragma unroll
+        for (int k = 0; k < kWalkK; ++k) {
+            run += st[k];
+            const bool good = ok[k] && s + ldexp((double)run, se - 52) < lim;
+            if (!good && bad == W) bad = lane * kWalkK + k;
         }
-        // slow group: lane 0 walks it, the other lanes wait at the shuffle
-        if (lane == 0) {
-            for (uint64_t cc = g; cc < g + 32 && cc < nchunks; ++cc) {
-                const int ec = cexp[cc];
-                if (clean[cc] && s > 0.0 && exponent_of(s) == ec) {
-                    const double t = s + ldexp((double)steps[cc], ec - 52);
-                    if (t < ldexp(1.0, ec + 1)) {
-                        s = t;
-                        ends[cc] = s;
-                        continue;
-                    }
-                }
-                ++seq;
-                const uint64_t c0 = cc << chunk_log;
-                const uint64_t e1 = c0 + len < n ? c0 + len : n;
-                for (uint64_t jj = c0; jj < e1; ++jj) s = __dadd_rn(s, prob(jj));
-                ends[cc] = s;
-            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bad = min(bad, __shfl_xor_sync(full, bad, o));
+        // ends of the leading good run, and s after it
+        run = pre - lsum;
+        long long upto = 0;
+#pragma unroll
+        for (int k = 0; k < kWalkK; ++k) {
+            run += st[k];
+            const int p = lane * kWalkK + k;
+            if (p < bad) ends[c + p] = s + ldexp((double)run, se - 52);
+            if (p == bad - 1) upto = run;
         }
-        s = __shfl_sync(0xffffffffu, s, 0);
+        if (bad > 0) {
+            upto = __shfl_sync(full, upto, (bad - 1) / kWalkK);
+            s = s + ldexp((double)upto, se - 52);
+        }
+        c += (uint64_t)bad;
+        if (bad == W || c >= nchunks) continue;
+        // chunk c: element by element
+        ++seq;
+        const uint64_t c0 = c << chunk_log;
+        const uint64_t e1 = c0 + len < n ? c0 + len : n;
+        for (uint64_t b = c0; b < e1; b += 32) {
+            const double pv = b + lane < e1 ? prob(b + lane) : 0.0;
+            const int cnt = e1 - b < 32 ? (int)(e1 - b) : 32;
+            for (int k = 0; k < cnt; ++k) s = __dadd_rn(s, __shfl_sync(full, pv, k));
+        }
+        if (lane == 0) ends[c] = s;
+        ++c;
     }
     if (lane == 0) *n_seq = seq;
 }

@@ -173,6 +173,31 @@ def test_sampling_degenerate_states():
     assert np.array_equal(sim.Sample(uu), orc.sample(probs, uu))
 
 
+@pytest.mark.parametrize("n", [18, 22])
+def test_sampling_sparse_and_basis_states(n):
+    # a basis state far into the vector (the running sum is exactly 1 from
+    # there on, a long all-zero tail), and a sparse state whose few weights
+    # span many binades (every crossing walks its chunk element by element)
+    sim = statevector.New(n)
+    u = statevector.uniforms(2000, np.random.default_rng(n))
+    k = (1 << n) - 12345
+    st = np.zeros(1 << n, dtype=np.complex128)
+    st[k] = 1
+    sim.SetStateVector(st)
+    assert np.all(sim.Sample(u) == k)
+    rng = np.random.default_rng(n + 1)
+    idx = np.sort(rng.choice(1 << n, 40, replace=False))
+    st = np.zeros(1 << n, dtype=np.complex128)
+    st[idx] = rng.normal(size=40) * 2.0 ** rng.integers(-20, 0, size=40) + 1j * rng.normal(size=40) * 1e-3
+    st /= np.linalg.norm(st)
+    sim.SetStateVector(st)
+    probs = orc.probabilities(sim.StateVector())
+    _, cum = orc.cumsum_at(probs, idx[:-1])
+    uu = np.concatenate([u, cum, np.nextafter(cum, 0), np.nextafter(cum, 2)])
+    uu = uu[(uu >= 0) & (uu < 1)]
+    assert np.array_equal(sim.Sample(uu), orc.sample_fast(probs, uu))
+
+
 def test_run_counts_statistics():
     # sim/statevector/sim_test.go:135-167: Bell counts only "00"/"11", each ~5000
     c = ir.Builder("bell", 2).H(0).CNOT(0, 1).MeasureAll().Build()
