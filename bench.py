@@ -251,9 +251,24 @@ def extra_density():
     st = dm.stats()
     z = [dm.ExpectPauliString(pauli.ZOn([q], 12)) for q in range(12)]
     tr = dm.Trace()
+    # error against the FP64 oracle (row/column passes and Kraus sums as goqu)
+    # on the same construction at 8 qubits, where the CPU pass takes seconds
+    from oracle import binding as orc
+    c8, nm8 = workloads.noisy_brickwork(8, layers=30, seed=12)
+    s8 = encode.density_ops(c8, nm8)
+    want = orc.dm_evolve(s8)
+    d8 = densitymatrix.New(8).WithNoise(nm8)
+    d8.set_option(_abi.GQ_OPT_JIT, 2)
+    d8.set_option(_abi.GQ_OPT_JIT_MIN_QUBITS, 0)
+    _abi.check(lib.gq_dm_evolve(d8._h, s8.ptr(), len(s8)))
+    terms = [pauli.to_terms(pauli.ZOn([q], 8)) for q in range(8)]
+    z_err = max(abs(d8.ExpectPauliString(pauli.ZOn([q], 8)) - orc.dm_expect_pauli_sum(want, 8, terms[q]).real)
+                for q in range(8))
     return {"workload": "density matrix 12q, 30 noisy U3+CNOT layers (depolarizing + amplitude damping)",
             "ms_device": float(np.median(ms)), "gates": workloads.count_gates(c), "ops_with_channels": len(s),
-            "passes": st["passes"], "trace_minus_one": abs(tr - 1.0), "z_expectations": z[:3]}
+            "passes": st["passes"], "trace_minus_one": abs(tr - 1.0), "z_expectations": z[:3],
+            "error_check_8q": {"max_abs_rho_error_vs_fp64_oracle": float(np.max(np.abs(d8.DensityMatrix() - want))),
+                               "max_abs_z_error_vs_fp64_oracle": z_err}}
 
 
 def extra_qaoa():
@@ -270,12 +285,64 @@ def extra_qaoa():
     b.set_option(_abi.GQ_OPT_TIMING, 1)
     ms = []
     for _ in range(3):
-        b.run_encoded(streams, terms, npar)
+        energies, grads = b.run_encoded(streams, terms, npar)
         ms.append(b.stats()["last_ms"])
     st = b.stats()
+    # error against the FP64 oracle on a sample of the batch: energies and
+    # parameter-shift gradients (exact for RZZ and RX generators)
+    from goqu_b200 import circuit as ir, encode, pauli
+    from oracle import binding as orc
+
+    def energy(c, names, h, x):
+        bound = ir.Bind(c, {nm: float(x[i]) for i, nm in enumerate(names)})
+        return orc.expect_pauli_sum(orc.sv_evolve(encode.statevector_ops(bound)), pauli.to_terms(h)).real
+
+    e_err = g_err = 0.0
+    for k in range(0, 4096, 256):
+        c, names, h, x = evals[k]
+        e_err = max(e_err, abs(energies[k] - energy(c, names, h, x)))
+        for i in range(len(names)):
+            xp, xm = np.array(x, float), np.array(x, float)
+            xp[i] += math.pi / 2
+            xm[i] -= math.pi / 2
+            g_err = max(g_err, abs(grads[k][i] - (energy(c, names, h, xp) - energy(c, names, h, xm)) / 2))
     return {"workload": "4096 QAOA MaxCut circuits (n 10..20, p 1..4), complex64, energies + gradients",
             "circuits_per_s": 4096 / (ms[-1] / 1000.0), "ms_device_first": ms[0], "ms_device_replay": ms[-1],
-            "passes": st["passes"], "launches": st["kernel_launches"], "host_encode_s": host_s}
+            "passes": st["passes"], "launches": st["kernel_launches"], "host_encode_s": host_s,
+            "max_abs_energy_error_vs_fp64_oracle": e_err, "max_abs_grad_error_vs_fp64_param_shift": g_err,
+            "error_sample": "16 circuits (every 256th)"}
+
+
+def extra_parity():
+    """The 20-qubit configuration (20 U3 + CNOT brickwork layers, 590 gates,
+    1024 shots): throughput and error against the FP64 oracle, complex128 and
+    complex64; sampled indices against the oracle's sequential inverse CDF."""
+    from goqu_b200 import _abi, encode, statevector, workloads
+    from oracle import binding as orc
+    c = workloads.random_layers(20, 20, 20)
+    stream = encode.statevector_ops(c)
+    gates = workloads.count_gates(c)
+    want = orc.sv_evolve(stream)
+    u = statevector.uniforms(SHOTS, np.random.default_rng(SEED))
+    out = {"workload": f"statevector 20q: 20 U3+CNOT brickwork layers ({gates} gates), {SHOTS} shots"}
+    for prec, tag in ((_abi.GQ_C128, "c128"), (_abi.GQ_C64, "c64")):
+        sim = statevector.New(20, prec)
+        sim.set_option(_abi.GQ_OPT_TIMING, 1)
+        sim.set_option(_abi.GQ_OPT_JIT, 2)
+        for _ in range(3):
+            sim.evolve_ops(stream)
+        ms = []
+        for _ in range(5):
+            sim.evolve_ops(stream)
+            ms.append(sim.stats()["last_ms"])
+        got = sim.StateVector()
+        out[tag] = {"gates_per_s": gates / (float(np.median(ms)) / 1000.0), "ms_device": float(np.median(ms)),
+                    "max_abs_amplitude_error_vs_fp64_oracle": float(np.max(np.abs(got - want)))}
+        if prec == _abi.GQ_C128:
+            probs = orc.probabilities(got)
+            out[tag]["samples_bit_exact_vs_oracle"] = bool(np.array_equal(sim.Sample(u), orc.sample_fast(probs, u)))
+        sim.Close()
+    return out
 
 
 def run_gpu(args, world, rank, local):
@@ -370,7 +437,8 @@ def run_gpu(args, world, rank, local):
         line["cpu_baseline"] = cpu_baseline(n, stream, gates, budget_s=args.cpu_seconds)
     if rank == 0 and not args.no_extras:
         extras = {}
-        for name, fn in (("adjoint", extra_adjoint), ("density_matrix", extra_density), ("qaoa_batch", extra_qaoa)):
+        for name, fn in (("parity_20q", extra_parity), ("adjoint", extra_adjoint), ("density_matrix", extra_density),
+                         ("qaoa_batch", extra_qaoa)):
             try:
                 extras[name] = fn()
             except Exception as exc:  # an extra must not hide the headline line
