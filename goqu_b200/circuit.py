@@ -89,13 +89,13 @@ class Circuit:
         last_gate = -1
         for i in range(len(self._ops) - 1, -1, -1):
             g = self._ops[i].Gate
-            if g is not None and g.Name() not in ("barrier", "reset"):
+            if g is not None and getattr(g, "directive", None) not in ("barrier", "reset"):
                 last_gate = i
                 break
         for i, op in enumerate(self._ops):
             if op.ControlFlow is not None or op.Condition is not None:
                 return True
-            if op.Gate is not None and op.Gate.Name() == "reset":
+            if op.Gate is not None and getattr(op.Gate, "directive", None) == "reset":
                 return True
             if op.Gate is None and op.Clbits and i < last_gate:
                 return True

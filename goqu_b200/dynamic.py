@@ -228,7 +228,7 @@ def _exec_op(be, g, op, U):
                 out.append(ng)
             return out
         return [g]
-    name = op.Gate.Name()
+    name = getattr(op.Gate, "directive", None)
     if name == "barrier":
         return [g]
     if name == "delay":

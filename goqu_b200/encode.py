@@ -15,51 +15,96 @@ from . import _abi
 from . import gate as _gate
 
 
+def _op_dtype():
+    f = _abi.gq_op
+    return np.dtype({
+        "names": ["kind", "num_qubits", "num_controls", "num_kraus", "qubits", "matrix", "param_index", "reserved",
+                  "dmatrix"],
+        "formats": [np.int32, np.int32, np.int32, np.int32, (np.int32, _abi.GQ_MAX_OP_QUBITS), np.uint64,
+                    (np.int32, _abi.GQ_MAX_OP_PARAMS), np.int32, (np.uint64, _abi.GQ_MAX_OP_PARAMS)],
+        "offsets": [f.kind.offset, f.num_qubits.offset, f.num_controls.offset, f.num_kraus.offset, f.qubits.offset,
+                    f.matrix.offset, f.param_index.offset, f.reserved.offset, f.dmatrix.offset],
+        "itemsize": ctypes.sizeof(f)})
+
+
+_OP_DTYPE = _op_dtype()
+
+
 class OpStream:
-    """A ctypes gq_op array plus the numpy buffers its pointers reference."""
+    """gq_op records (a numpy array with the struct's layout, built once the
+    stream is complete) plus one buffer holding every matrix they point to."""
+
+    _PAD = (0,) * _abi.GQ_MAX_OP_QUBITS
 
     def __init__(self, num_qubits):
         self.num_qubits = num_qubits
-        self._ops = []
-        self._keep = []
-        self._arr = None
+        self._hdr = []   # (kind, num_qubits, num_controls, num_kraus)
+        self._qub = []   # qubits padded to GQ_MAX_OP_QUBITS
+        self._pidx = []  # param indices padded with -1
+        self._mats = []  # complex128 arrays, in order
+        self._nmat = 0   # complex entries so far
+        self._moff = []  # (record, field (-1 = matrix, k = dmatrix[k]), entry offset)
+        self._rec = None
+        self._data = None
         self.n_params = 0
 
-    def _buf(self, m):
-        a = np.ascontiguousarray(np.asarray(m, dtype=np.complex128).reshape(-1)).view(np.float64)
-        self._keep.append(a)
-        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    def _slot(self, m):
+        a = np.asarray(m, dtype=np.complex128).reshape(-1)
+        off = self._nmat
+        self._mats.append(a)
+        self._nmat += a.size
+        return off
 
     def add(self, kind, qubits, matrix=None, num_controls=0, num_kraus=0, params=()):
-        if len(qubits) > _abi.GQ_MAX_OP_QUBITS:
-            raise ValueError(f"op on {len(qubits)} qubits exceeds {_abi.GQ_MAX_OP_QUBITS}")
-        op = _abi.gq_op()
-        op.kind = kind
-        op.num_qubits = len(qubits)
-        op.num_controls = num_controls
-        op.num_kraus = num_kraus
-        for i, q in enumerate(qubits):
-            op.qubits[i] = q
+        nq = len(qubits)
+        if nq > _abi.GQ_MAX_OP_QUBITS:
+            raise ValueError(f"op on {nq} qubits exceeds {_abi.GQ_MAX_OP_QUBITS}")
+        i = len(self._hdr)
+        self._hdr.append((kind, nq, num_controls, num_kraus))
+        self._qub.append(tuple(qubits) + self._PAD[nq:])
         if matrix is not None:
-            op.matrix = self._buf(matrix)
-        for k in range(_abi.GQ_MAX_OP_PARAMS):
-            op.param_index[k] = -1
+            self._moff.append((i, -1, self._slot(matrix)))
+        pi = [-1, -1, -1]
         for k, (pidx, dm) in enumerate(params):
-            op.param_index[k] = pidx
-            op.dmatrix[k] = self._buf(dm)
-        self._ops.append(op)
-        self._arr = None
+            pi[k] = pidx
+            self._moff.append((i, k, self._slot(dm)))
+        self._pidx.append(pi)
+        self._rec = None
 
     def __len__(self):
-        return len(self._ops)
+        return len(self._hdr)
+
+    def _finish(self):
+        if self._rec is not None:
+            return
+        n = len(self._hdr)
+        rec = np.zeros(max(1, n), dtype=_OP_DTYPE)
+        if n:
+            h = np.array(self._hdr, dtype=np.int32)
+            rec["kind"][:n], rec["num_qubits"][:n] = h[:, 0], h[:, 1]
+            rec["num_controls"][:n], rec["num_kraus"][:n] = h[:, 2], h[:, 3]
+            rec["qubits"][:n] = np.array(self._qub, dtype=np.int32)
+            rec["param_index"][:n] = np.array(self._pidx, dtype=np.int32)
+        data = np.concatenate(self._mats) if self._mats else np.zeros(1, dtype=np.complex128)
+        self._data = np.ascontiguousarray(data)
+        if self._moff:
+            m = np.array(self._moff, dtype=np.int64)
+            addr = (self._data.ctypes.data + 16 * m[:, 2]).astype(np.uint64)
+            sel = m[:, 1] < 0
+            rec["matrix"][m[sel, 0]] = addr[sel]
+            for k in range(_abi.GQ_MAX_OP_PARAMS):
+                sk = m[:, 1] == k
+                rec["dmatrix"][m[sk, 0], k] = addr[sk]
+        self._rec = rec
 
     def array(self):
-        if self._arr is None:
-            self._arr = (_abi.gq_op * max(1, len(self._ops)))(*self._ops)
-        return self._arr
+        """The records as a ctypes gq_op array (a view of the same memory)."""
+        self._finish()
+        return (_abi.gq_op * max(1, len(self._hdr))).from_buffer(self._rec)
 
     def ptr(self):
-        return ctypes.cast(self.array(), ctypes.POINTER(_abi.gq_op))
+        self._finish()
+        return ctypes.cast(self._rec.ctypes.data, ctypes.POINTER(_abi.gq_op))
 
 
 def _gate_record(stream, g, qubits, params=()):
@@ -87,9 +132,12 @@ def statevector_ops(circuit, bindings=None, param_names=None):
     stream.n_params = len(index)
     for op in circuit.Ops():
         g = op.Gate
-        if g is None or g.Name() in ("barrier", "delay"):
+        if g is None:
             continue
-        if g.Name() == "reset":
+        d = getattr(g, "directive", None)
+        if d == "barrier" or d == "delay":
+            continue
+        if d == "reset":
             stream.add(_abi.GQ_OP_RESET, [op.Qubits[0]])
             continue
         if hasattr(g, "Bind"):
@@ -123,15 +171,16 @@ def density_ops(circuit, noise_model=None):
 
     for op in circuit.Ops():
         g = op.Gate
-        if g is None or g.Name() == "barrier":
+        d = None if g is None else getattr(g, "directive", None)
+        if g is None or d == "barrier":
             continue
         if getattr(g, "noise_only", None):  # a channel without its gate (dynamic resets)
             channel(g.noise_only, op.Qubits)
             continue
-        if g.Name() == "delay":
+        if d == "delay":
             channel("delay", op.Qubits)
             continue
-        if g.Name() == "reset":
+        if d == "reset":
             stream.add(_abi.GQ_OP_RESET, [op.Qubits[0]])
             channel("reset", op.Qubits)
             continue

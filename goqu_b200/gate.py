@@ -34,6 +34,8 @@ class Gate:
             self.kind = kind
 
     def Name(self):
+        if callable(self._name):  # parameterised gates format their name on first use
+            self._name = self._name()
         return self._name
 
     def Qubits(self):
@@ -51,7 +53,7 @@ class Gate:
         m = self._matrix.reshape(dim, dim)
         inv = np.conj(m.T).reshape(-1)
         params = None if self._params is None else [-p for p in self._params]
-        return Gate(self._name + "†", self._n, inv, params, kind=_inverse_kind(self.kind))
+        return Gate(self.Name() + "†", self._n, inv, params, kind=_inverse_kind(self.kind))
 
     def Decompose(self, qubits):
         return None
@@ -144,34 +146,34 @@ def _fmt(*vals):
 # Parameterized gates (circuit/gate/parameterized.go:91-564).
 def RX(theta):
     c, s = math.cos(theta / 2), math.sin(theta / 2)
-    return _param(f"RX({_fmt(theta)})", 1, [theta], [complex(c, 0), complex(0, -s), complex(0, -s), complex(c, 0)])
+    return _param(lambda: f"RX({_fmt(theta)})", 1, [theta], [complex(c, 0), complex(0, -s), complex(0, -s), complex(c, 0)])
 
 
 def RY(theta):
     c, s = math.cos(theta / 2), math.sin(theta / 2)
-    return _param(f"RY({_fmt(theta)})", 1, [theta], [complex(c, 0), complex(-s, 0), complex(s, 0), complex(c, 0)])
+    return _param(lambda: f"RY({_fmt(theta)})", 1, [theta], [complex(c, 0), complex(-s, 0), complex(s, 0), complex(c, 0)])
 
 
 def RZ(theta):
-    return _param(f"RZ({_fmt(theta)})", 1, [theta], [_e(-theta / 2), 0, 0, _e(theta / 2)])
+    return _param(lambda: f"RZ({_fmt(theta)})", 1, [theta], [_e(-theta / 2), 0, 0, _e(theta / 2)])
 
 
 def Phase(phi):
-    return _param(f"P({_fmt(phi)})", 1, [phi], [1, 0, 0, _e(phi)])
+    return _param(lambda: f"P({_fmt(phi)})", 1, [phi], [1, 0, 0, _e(phi)])
 
 
 def U3(theta, phi, lam):
     c, s = math.cos(theta / 2), math.sin(theta / 2)
-    return _param(f"U3({_fmt(theta, phi, lam)})", 1, [theta, phi, lam],
+    return _param(lambda: f"U3({_fmt(theta, phi, lam)})", 1, [theta, phi, lam],
                   [complex(c, 0), -_e(lam) * complex(s, 0), _e(phi) * complex(s, 0), _e(phi + lam) * complex(c, 0)])
 
 
 def CP(phi):
-    return _param(f"CP({_fmt(phi)})", 2, [phi], np.diag([1, 1, 1, _e(phi)]).reshape(-1), _abi.GQ_OP_CTRL_DIAG_2Q)
+    return _param(lambda: f"CP({_fmt(phi)})", 2, [phi], np.diag([1, 1, 1, _e(phi)]).reshape(-1), _abi.GQ_OP_CTRL_DIAG_2Q)
 
 
 def CRZ(theta):
-    return _param(f"CRZ({_fmt(theta)})", 2, [theta], np.diag([1, 1, _e(-theta / 2), _e(theta / 2)]).reshape(-1),
+    return _param(lambda: f"CRZ({_fmt(theta)})", 2, [theta], np.diag([1, 1, _e(-theta / 2), _e(theta / 2)]).reshape(-1),
                   _abi.GQ_OP_CTRL_DIAG_2Q)
 
 
@@ -183,69 +185,70 @@ def _ctrl_u(u):
 
 def CRX(theta):
     c, s = math.cos(theta / 2), math.sin(theta / 2)
-    return _param(f"CRX({_fmt(theta)})", 2, [theta], _ctrl_u([complex(c, 0), complex(0, -s), complex(0, -s), complex(c, 0)]),
+    return _param(lambda: f"CRX({_fmt(theta)})", 2, [theta], _ctrl_u([complex(c, 0), complex(0, -s), complex(0, -s), complex(c, 0)]),
                   _abi.GQ_OP_CTRL_U_2Q)
 
 
 def CRY(theta):
     c, s = math.cos(theta / 2), math.sin(theta / 2)
-    return _param(f"CRY({_fmt(theta)})", 2, [theta], _ctrl_u([complex(c, 0), complex(-s, 0), complex(s, 0), complex(c, 0)]),
+    return _param(lambda: f"CRY({_fmt(theta)})", 2, [theta], _ctrl_u([complex(c, 0), complex(-s, 0), complex(s, 0), complex(c, 0)]),
                   _abi.GQ_OP_CTRL_U_2Q)
 
 
 def RXX(theta):
     c, s = math.cos(theta / 2), math.sin(theta / 2)
     cc, is_ = complex(c, 0), complex(0, -s)
-    return _param(f"RXX({_fmt(theta)})", 2, [theta], [cc, 0, 0, is_, 0, cc, is_, 0, 0, is_, cc, 0, is_, 0, 0, cc])
+    return _param(lambda: f"RXX({_fmt(theta)})", 2, [theta], [cc, 0, 0, is_, 0, cc, is_, 0, 0, is_, cc, 0, is_, 0, 0, cc])
 
 
 def RYY(theta):
     c, s = math.cos(theta / 2), math.sin(theta / 2)
     cc, is_, nis = complex(c, 0), complex(0, s), complex(0, -s)
-    return _param(f"RYY({_fmt(theta)})", 2, [theta], [cc, 0, 0, is_, 0, cc, nis, 0, 0, nis, cc, 0, is_, 0, 0, cc])
+    return _param(lambda: f"RYY({_fmt(theta)})", 2, [theta], [cc, 0, 0, is_, 0, cc, nis, 0, 0, nis, cc, 0, is_, 0, 0, cc])
 
 
 def RZZ(theta):
     em, ep = _e(-theta / 2), _e(theta / 2)
-    return _param(f"RZZ({_fmt(theta)})", 2, [theta], np.diag([em, ep, ep, em]).reshape(-1), _abi.GQ_OP_DIAG_2Q)
+    return _param(lambda: f"RZZ({_fmt(theta)})", 2, [theta], [em, 0, 0, 0, 0, ep, 0, 0, 0, 0, ep, 0, 0, 0, 0, em],
+                  _abi.GQ_OP_DIAG_2Q)
 
 
 def ZZ(theta):
     em, ep = _e(-theta / 2), _e(theta / 2)
-    return _param(f"ZZ({_fmt(theta)})", 2, [theta], np.diag([em, ep, ep, em]).reshape(-1), _abi.GQ_OP_DIAG_2Q)
+    return _param(lambda: f"ZZ({_fmt(theta)})", 2, [theta], np.diag([em, ep, ep, em]).reshape(-1), _abi.GQ_OP_DIAG_2Q)
 
 
 def GPI(phi):
-    return _param(f"GPI({_fmt(phi)})", 1, [phi], [0, _e(-phi), _e(phi), 0])
+    return _param(lambda: f"GPI({_fmt(phi)})", 1, [phi], [0, _e(-phi), _e(phi), 0])
 
 
 def GPI2(phi):
     inv = complex(_S2, 0)
-    return _param(f"GPI2({_fmt(phi)})", 1, [phi], [inv, inv * complex(0, -1) * _e(-phi), inv * complex(0, -1) * _e(phi), inv])
+    return _param(lambda: f"GPI2({_fmt(phi)})", 1, [phi], [inv, inv * complex(0, -1) * _e(-phi), inv * complex(0, -1) * _e(phi), inv])
 
 
 def MS(phi0, phi1):
     inv = complex(_S2, 0)
     ep, em = _e(phi0 + phi1), _e(phi0 - phi1)
     mi = complex(0, -1)
-    return _param(f"MS({_fmt(phi0, phi1)})", 2, [phi0, phi1],
+    return _param(lambda: f"MS({_fmt(phi0, phi1)})", 2, [phi0, phi1],
                   [inv, 0, 0, inv * mi * ep.conjugate(), 0, inv, inv * mi * em, 0,
                    0, inv * mi * em.conjugate(), inv, 0, inv * mi * ep, 0, 0, inv])
 
 
 def U1(lam):
-    return _param(f"U1({_fmt(lam)})", 1, [lam], [1, 0, 0, _e(lam)])
+    return _param(lambda: f"U1({_fmt(lam)})", 1, [lam], [1, 0, 0, _e(lam)])
 
 
 def U2(phi, lam):
     s = complex(_S2, 0)
-    return _param(f"U2({_fmt(phi, lam)})", 1, [phi, lam], [s, -_e(lam) * s, _e(phi) * s, _e(phi + lam) * s])
+    return _param(lambda: f"U2({_fmt(phi, lam)})", 1, [phi, lam], [s, -_e(lam) * s, _e(phi) * s, _e(phi + lam) * s])
 
 
 def Rot(phi, theta, omega):
     cth, sth = math.cos(theta / 2), math.sin(theta / 2)
     eipo, eimo = _e((phi + omega) / 2), _e((phi - omega) / 2)
-    return _param(f"Rot({_fmt(phi, theta, omega)})", 1, [phi, theta, omega],
+    return _param(lambda: f"Rot({_fmt(phi, theta, omega)})", 1, [phi, theta, omega],
                   [eipo.conjugate() * complex(cth, 0), -eimo.conjugate() * complex(sth, 0),
                    eimo * complex(sth, 0), eipo * complex(cth, 0)])
 
@@ -253,25 +256,25 @@ def Rot(phi, theta, omega):
 def PhasedXZ(x, z, a):
     cx, sx = math.cos(math.pi * x / 2), math.sin(math.pi * x / 2)
     ez, ea = _e(math.pi * z), _e(math.pi * a)
-    return _param(f"PhasedXZ({_fmt(x, z, a)})", 1, [x, z, a],
+    return _param(lambda: f"PhasedXZ({_fmt(x, z, a)})", 1, [x, z, a],
                   [complex(cx, 0), ea.conjugate() * complex(0, sx), ez * ea * complex(0, sx), ez * complex(cx, 0)])
 
 
 def GlobalPhase(phi):
     ep = _e(phi)
-    return _param(f"GlobalPhase({_fmt(phi)})", 1, [phi], [ep, 0, 0, ep])
+    return _param(lambda: f"GlobalPhase({_fmt(phi)})", 1, [phi], [ep, 0, 0, ep])
 
 
 def FSim(theta, phi):
     ct, st = math.cos(theta), math.sin(theta)
-    return _param(f"FSim({_fmt(theta, phi)})", 2, [theta, phi],
+    return _param(lambda: f"FSim({_fmt(theta, phi)})", 2, [theta, phi],
                   [1, 0, 0, 0, 0, complex(ct, 0), complex(0, -st), 0, 0, complex(0, -st), complex(ct, 0), 0,
                    0, 0, 0, _e(-phi)])
 
 
 def PSwap(phi):
     ep = _e(phi)
-    return _param(f"PSwap({_fmt(phi)})", 2, [phi], [1, 0, 0, 0, 0, 0, ep, 0, 0, ep, 0, 0, 0, 0, 0, 1])
+    return _param(lambda: f"PSwap({_fmt(phi)})", 2, [phi], [1, 0, 0, 0, 0, 0, ep, 0, 0, ep, 0, 0, 0, 0, 0, 1])
 
 
 class ControlledGate(Gate):
@@ -338,6 +341,7 @@ def MCP(phi, n_controls):
 class _Pseudo(Gate):
     def __init__(self, name, n, params=None):
         super().__init__(name, n, None, params)
+        self.directive = name  # what the simulators switch on, without formatting names
 
     def Inverse(self):
         return self

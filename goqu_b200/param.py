@@ -223,13 +223,16 @@ class SymbolicGate(_gate.Gate):
         return self.constructor(vals)
 
     def FreeParameters(self):
-        seen, names = set(), []
-        for e in self.exprs:
-            for p in e.Parameters():
-                if p.Name() not in seen:
-                    seen.add(p.Name())
-                    names.append(p.Name())
-        return names
+        names = self.__dict__.get("_free")
+        if names is None:  # expressions are immutable: computed once per gate
+            seen, names = set(), []
+            for e in self.exprs:
+                for p in e.Parameters():
+                    if p.Name() not in seen:
+                        seen.add(p.Name())
+                        names.append(p.Name())
+            self._free = names
+        return list(names)
 
     def IsBound(self):
         return all(e.IsNumeric() for e in self.exprs)

@@ -27,7 +27,7 @@ def _exec(ops, st, n, clbits, draw):
                 clbits[op.Clbits[0]] = orc.sv_measure(st, op.Qubits[0], draw())
             continue
         name = op.Gate.Name()
-        if name in ("barrier", "delay"):
+        if name in ("barrier", "delay"):  # the pseudo-gates' names (gate.go)
             continue
         if name == "reset":
             if orc.sv_measure(st, op.Qubits[0], draw()) == 1:
