@@ -288,8 +288,10 @@ def extra_qaoa():
         energies, grads = b.run_encoded(streams, terms, npar)
         ms.append(b.stats()["last_ms"])
     st = b.stats()
-    # error against the FP64 oracle on a sample of the batch: energies and
-    # parameter-shift gradients (exact for RZZ and RX generators)
+    # error against the FP64 oracle on a sample of the batch: energies, and
+    # gradients against central differences of the oracle energy (each QAOA
+    # angle drives every RZZ / RX of its layer, so the +-pi/2 shift rule of a
+    # single gate does not apply)
     from goqu_b200 import circuit as ir, encode, pauli
     from oracle import binding as orc
 
@@ -303,13 +305,13 @@ def extra_qaoa():
         e_err = max(e_err, abs(energies[k] - energy(c, names, h, x)))
         for i in range(len(names)):
             xp, xm = np.array(x, float), np.array(x, float)
-            xp[i] += math.pi / 2
-            xm[i] -= math.pi / 2
-            g_err = max(g_err, abs(grads[k][i] - (energy(c, names, h, xp) - energy(c, names, h, xm)) / 2))
+            xp[i] += 1e-6
+            xm[i] -= 1e-6
+            g_err = max(g_err, abs(grads[k][i] - (energy(c, names, h, xp) - energy(c, names, h, xm)) / 2e-6))
     return {"workload": "4096 QAOA MaxCut circuits (n 10..20, p 1..4), complex64, energies + gradients",
             "circuits_per_s": 4096 / (ms[-1] / 1000.0), "ms_device_first": ms[0], "ms_device_replay": ms[-1],
             "passes": st["passes"], "launches": st["kernel_launches"], "host_encode_s": host_s,
-            "max_abs_energy_error_vs_fp64_oracle": e_err, "max_abs_grad_error_vs_fp64_param_shift": g_err,
+            "max_abs_energy_error_vs_fp64_oracle": e_err, "max_abs_grad_error_vs_fp64_central_difference": g_err,
             "error_sample": "16 circuits (every 256th)"}
 
 
