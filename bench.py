@@ -54,7 +54,9 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def dist_setup():
+def dist_setup(backend=None):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): NCCL
+    when a GPU is present, gloo otherwise (the CPU tests of this plumbing)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -63,9 +65,12 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -74,7 +79,8 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -78,3 +78,48 @@ class Batch:
     def Run(self, evaluations, gradients=True):
         streams, terms = self.encode(evaluations)
         return self.run_encoded(streams, terms, [len(e[1]) for e in evaluations], gradients)
+
+
+def split_by_work(evaluations, world):
+    """Indices of each rank's share of a batch, balanced by state size: the
+    largest circuits first, each to the rank with the least work so far
+    (work = 2^n per circuit)."""
+    load = [0] * world
+    shares = [[] for _ in range(world)]
+    order = sorted(range(len(evaluations)), key=lambda i: -(1 << evaluations[i][0].NumQubits()))
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        shares[r].append(i)
+        load[r] += 1 << evaluations[i][0].NumQubits()
+    return [sorted(x) for x in shares]
+
+
+def run_sharded(evaluations, rank, world, precision=_abi.GQ_C64, gradients=True, runner=None):
+    """A batch split across ranks (one GPU each): every rank runs its share on
+    its own device and the energies and gradients are all-gathered; returns
+    the whole batch's results in input order on every rank. The gather of
+    scalars is the only collective (torch.distributed, any backend)."""
+    share = split_by_work(evaluations, world)[rank]
+    mine = [evaluations[i] for i in share]
+    if runner is None:
+        b = Batch(precision)
+        e, g = b.Run(mine, gradients) if mine else (np.empty(0), [])
+        b.Close()
+    else:
+        e, g = runner(mine, gradients)
+    local = (share, np.asarray(e, dtype=np.float64).tolist(),
+             [np.asarray(x, dtype=np.float64).tolist() for x in g] if gradients else None)
+    if world > 1:
+        import torch.distributed as dist
+        parts = [None] * world
+        dist.all_gather_object(parts, local)
+    else:
+        parts = [local]
+    energies = np.empty(len(evaluations), dtype=np.float64)
+    grads = [None] * len(evaluations) if gradients else None
+    for idx, es, gs in parts:
+        for j, i in enumerate(idx):
+            energies[i] = es[j]
+            if gradients:
+                grads[i] = np.asarray(gs[j], dtype=np.float64)
+    return energies, grads

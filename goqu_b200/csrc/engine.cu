@@ -125,6 +125,10 @@ using AdjKernelD = void (*)(cplx<double>*, cplx<double>*, const PassDesc*, const
 using AdjKernelF = void (*)(cplx<float>*, cplx<float>*, const PassDesc*, const PhaseDesc*, const KOp*,
                             const cplx<float>*, double*, int);
 constexpr int kAdjThreads = 128;
+// CTAs per SM of the batched reverse pass: complex64 keeps both states'
+// 16 amplitudes in 64 registers and fits 3.
+template <class T>
+constexpr int kAdjBatchMinB = sizeof(T) == 4 ? 3 : 2;
 const AdjKernelD kAdjD = k_adjoint_pass<double, kAdjThreads, 2>;
 const AdjKernelF kAdjF = k_adjoint_pass<float, kAdjThreads, 3>;
 template <class T>
@@ -1299,7 +1303,7 @@ int set_batch_attrs() {
         err = cudaFuncSetAttribute(BatchTile<T>::kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(sizeof(cplx<T>) << mt));
         if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(k_adjoint_pass_batch<T, kAdjThreads, 2>,
+            err = cudaFuncSetAttribute(k_adjoint_pass_batch<T, kAdjThreads, kAdjBatchMinB<T>>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)adj_smem(sizeof(cplx<T>), log2i(kAdjThreads) + RQ));
     });
@@ -1520,7 +1524,8 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
                     (const PhaseDesc*)(d + o.phase), (const KOp*)(d + o.ops), (const cplx<T>*)(d + o.pool));
                 ++launches;
             } else {
-                k_adjoint_pass_batch<T, kAdjThreads, 2><<<L.count, threads, adj_smem(sizeof(cplx<T>), L.m), e.stream>>>(
+                k_adjoint_pass_batch<T, kAdjThreads, kAdjBatchMinB<T>><<<L.count, threads, adj_smem(sizeof(cplx<T>), L.m),
+                                                                         e.stream>>>(
                     states, lams, (const BItem*)(d + o.items) + L.item0, (const uint64_t*)(d + o.part) + L.item0,
                     (const int*)(d + o.nslots), (const PassDesc*)(d + o.pass), (const PhaseDesc*)(d + o.phase),
                     (const KOp*)(d + o.ops), (const cplx<T>*)(d + o.pool), partial);

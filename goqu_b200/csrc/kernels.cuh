@@ -161,21 +161,40 @@ __device__ __forceinline__ void adjoint_pass_body(cplx<T>* __restrict__ psi, cpl
         sa[s] = psi[g];
         sb[s] = lam[g];
     }
+    const int nwarps = (int)((blockDim.x + 31) >> 5);
+    for (int i = (int)t; i < nwarps * MAX_GRAD_SLOTS; i += (int)blockDim.x) gsm[i] = 0.0;
     __syncthreads();
     const int warp = t >> 5, lane = t & 31;
     // Tiles below 2^9 amplitudes have fewer than 32 threads: reduce over the
     // lanes that exist (the mask of a shuffle must name only live lanes).
     const unsigned nlanes = blockDim.x < 32 ? blockDim.x : 32u;
     const unsigned lanes = nlanes == 32 ? 0xffffffffu : ((1u << nlanes) - 1u);
-    auto grad = [&](uint32_t slot, double v) {
+    // A slot is a parameter of the pass: consecutive gradient ops of one
+    // parameter (every RZZ of a QAOA layer, say) add up in a register, and
+    // the warp reduces once per run (all lanes call grad() in the same order).
+    double acc = 0.0;
+    int cur = -1;
+    auto flush = [&]() {
+        if (cur < 0) return;
+        double v = acc;
         for (unsigned o = 16; o > 0; o >>= 1) {
             const double y = __shfl_xor_sync(lanes, v, o);
             if ((lane ^ o) < (int)nlanes) v += y;
         }
-        if (lane == 0) gsm[warp * MAX_GRAD_SLOTS + slot] = v;
+        if (lane == 0) gsm[warp * MAX_GRAD_SLOTS + cur] += v;
+        acc = 0.0;
+        cur = -1;
+    };
+    auto grad = [&](uint32_t slot, double v) {
+        if ((int)slot != cur) {
+            flush();
+            cur = (int)slot;
+        }
+        acc += v;
     };
     for (int p = 0; p < pd.n_phases; ++p) {
         run_phase_dual<T>(sa, sb, phases[pd.phase0 + p], ops, pool, t, base, grad);
+        flush();
         __syncthreads();
     }
     for (int it = 0; it < NREG; ++it) {
@@ -191,9 +210,9 @@ __device__ __forceinline__ void adjoint_pass_body(cplx<T>* __restrict__ psi, cpl
     }
     __syncthreads();
     for (int sl = (int)t; sl < nslots; sl += (int)blockDim.x) {  // tiles may have fewer threads than slots
-        double acc = 0.0;
-        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) acc += gsm[w * MAX_GRAD_SLOTS + sl];
-        partial_out[sl] = acc;
+        double tot = 0.0;
+        for (int w = 0; w < nwarps; ++w) tot += gsm[w * MAX_GRAD_SLOTS + sl];
+        partial_out[sl] = tot;
     }
 }
 

@@ -611,9 +611,10 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                 std::memset(&op, 0, sizeof(op));
                 op.type = g.type;
                 const KType kind = g.type == K_GRAD ? g.grad_kind : g.type;
-                if (g.type == K_GRAD) {
-                    op.slot = (uint32_t)slot_params.size();
-                    slot_params.push_back(g.param);
+                if (g.type == K_GRAD) {  // one slot per parameter of the pass
+                    const auto at = std::find(slot_params.begin(), slot_params.end(), g.param);
+                    op.slot = (uint32_t)(at - slot_params.begin());
+                    if (at == slot_params.end()) slot_params.push_back(g.param);
                 }
                 for (int k = 0; k < RQ; ++k)
                     if (g.ctrl & (1ull << rq[k])) op.creg |= (uint8_t)(1u << k);

@@ -52,7 +52,7 @@ def test_qaoa_gradients_match_oracle_central_differences():
     # adjoint gradient against central differences of the FP64 oracle energy
     from oracle import binding as orc
     evals = workloads.qaoa_batch(6, seed=21, n_values=(10, 12))
-    for prec, tol in ((_abi.GQ_C128, 1e-8), (_abi.GQ_C64, 2e-3)):
+    for prec, tol in ((_abi.GQ_C128, 1e-6), (_abi.GQ_C64, 2e-3)):  # central differences: ~1e-7 roundoff
         b = batch.Batch(prec)
         energies, grads = b.Run(evals)
         for k, (c, names, h, x) in enumerate(evals):
