@@ -187,7 +187,8 @@ static int emulate_sv_impl(int nq, int precision, double* state, const gq_op* op
 }
 
 // Schedule only: out = {passes, phases, ops, sum over ops of their FMA-per-
-// amplitude cost}, for comparing scheduler settings without running anything.
+// amplitude cost, K_PAIRSUM ops}, for comparing scheduler settings without
+// running anything.
 int gqx_schedule_stats(int nq, int precision, const gq_op* ops, size_t n_ops, int tile_qubits, int budget, int fuse,
                        int64_t* out) {
     const int nphys = nq < gq::RQ ? gq::RQ : nq;
@@ -204,15 +205,17 @@ int gqx_schedule_stats(int nq, int precision, const gq_op* ops, size_t n_ops, in
     opt.fuse_dense = fuse != 0;
     gq::Program prog;
     gq::schedule(gates, nphys, opt, prog);
-    int64_t cost = 0;
+    int64_t cost = 0, pairsums = 0;
     for (const gq::KOp& op : prog.ops) {
-        static const int c[] = {0, 8, 16, 32, 64, 1, 1, 3, 1, 4, 16};
+        static const int c[] = {0, 8, 16, 32, 64, 1, 1, 3, 1, 4, 16, 6};
         cost += c[op.type] + 6;
+        pairsums += op.type == gq::K_PAIRSUM;
     }
     out[0] = (int64_t)prog.passes.size();
     out[1] = (int64_t)prog.phases.size();
     out[2] = (int64_t)prog.ops.size();
     out[3] = cost;
+    out[4] = pairsums;
     return GQ_OK;
 }
 

@@ -312,7 +312,7 @@ struct Engine {
         const size_t np = pr.passes.size();
         std::vector<const void*> jfn(np, nullptr);
         std::vector<const CachedPlan*> plans(np, nullptr);
-        if (jit_mode != 0 && nphys >= jit_min_qubits && jit_available()) {
+        if (jit_on()) {
             // One tile per CTA: 4 CTAs of 128 threads per SM (128 registers)
             // measured fastest for both precisions. Persistent: as many CTAs
             // per SM as two tile buffers each allow (3 for complex128).
@@ -432,9 +432,13 @@ struct Engine {
         return prec == GQ_C64 ? run_adjoint_t<float>(pr) : run_adjoint_t<double>(pr);
     }
 
+    bool jit_on() const { return jit_mode != 0 && nphys >= jit_min_qubits && jit_available(); }
+
     int run_gates(const std::vector<NGate>& gates) {
         Program pr;
-        schedule(gates, nphys, opt, pr);
+        SchedOptions o = opt;
+        o.fuse_pairs = !jit_on();  // specialised kernels take diagonals as free pending factors
+        schedule(gates, nphys, o, pr);
         stats.gates_in += pr.gates;
         return prec == GQ_C64 ? run_program_t<float>(pr) : run_program_t<double>(pr);
     }

@@ -2,6 +2,7 @@
 #include "schedule.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <random>
 
@@ -54,6 +55,7 @@ int cost_of(KType t) {
         case K_U4: return 64;
         case K_DIAG: return 3;
         case K_RESET: return 4;
+        case K_PAIRSUM: return 6;
         default: return 1;
     }
 }
@@ -415,6 +417,124 @@ std::vector<NGate> fuse_phase(const std::vector<NGate>& gates, const std::vector
     return out;
 }
 
+// Runs of commuting diagonal ops (phases, diagonals, and their gradient ops)
+// in a phase's op list: identical parity-symmetric 2-qubit diagonals
+// (d00 = d11, d01 = d10, no controls: RZZ(g), ZZ(g) of one layer) fold into
+// one K_PAIRSUM with T[c] = d00^(K-c) d01^c; gradient ops of one parameter
+// with such a G fold into one K_GRAD(K_PAIRSUM) with T[c] = (K-c) g00 + c g01.
+// Inside such a run every op commutes with every other, and a gradient op
+// measures the same Re <lambda|G|psi> anywhere in it when the run's
+// diagonals are unitary (<D lambda|G|D psi> = <lambda|G|psi>), so gradient
+// ops are moved ahead of the run's unitaries only when all of them are.
+bool pair_sym(const NGate& g) {
+    const KType k = g.type == K_GRAD ? g.grad_kind : g.type;
+    return k == K_DIAG && g.ctrl == 0 && g.targets.size() == 2 && g.data.size() == 4 && eq(g.data[0], g.data[3]) &&
+           eq(g.data[1], g.data[2]);
+}
+
+bool diag_class(const NGate& g) {
+    const KType k = g.type == K_GRAD ? g.grad_kind : g.type;
+    return (k == K_DIAG || k == K_PHASE) && !g.barrier;
+}
+
+bool unit_modulus(const NGate& g) {
+    for (const Z& z : g.data)
+        if (std::fabs(z.re * z.re + z.im * z.im - 1.0) > 1e-12) return false;
+    return true;
+}
+
+std::vector<NGate> fuse_pairsums(const std::vector<NGate>& in, uint64_t R, const int* rq) {
+    auto code = [&](int q) {
+        for (int k = 0; k < RQ; ++k)
+            if (rq[k] == q && (R >> q & 1ull)) return (double)k;
+        return (double)(16 + q);
+    };
+    std::vector<NGate> out;
+    size_t i = 0;
+    while (i < in.size()) {
+        if (!diag_class(in[i])) {
+            out.push_back(in[i++]);
+            continue;
+        }
+        size_t j = i;
+        bool has_grad = false, unitary = true;
+        while (j < in.size() && diag_class(in[j])) {
+            if (in[j].type == K_GRAD)
+                has_grad = true;
+            else if (!unit_modulus(in[j]))
+                unitary = false;
+            ++j;
+        }
+        if (has_grad && !unitary) {  // keep the run as it is
+            for (size_t k = i; k < j; ++k) out.push_back(in[k]);
+            i = j;
+            continue;
+        }
+        // groups of fusable ops, in first-appearance order
+        std::vector<std::vector<size_t>> groups;
+        std::vector<size_t> singles;
+        for (size_t k = i; k < j; ++k) {
+            const NGate& g = in[k];
+            if (!pair_sym(g)) {
+                singles.push_back(k);
+                continue;
+            }
+            bool placed = false;
+            for (auto& grp : groups) {
+                const NGate& h = in[grp[0]];
+                if (h.type == g.type && h.param == g.param && eq(h.data[0], g.data[0]) && eq(h.data[1], g.data[1]) &&
+                    grp.size() < 200) {
+                    grp.push_back(k);
+                    placed = true;
+                    break;
+                }
+            }
+            if (!placed) groups.push_back({k});
+        }
+        std::vector<NGate> grads, units;
+        for (size_t k : singles) (in[k].type == K_GRAD ? grads : units).push_back(in[k]);
+        for (const auto& grp : groups) {
+            const NGate& h = in[grp[0]];
+            if (grp.size() < 2) {
+                (h.type == K_GRAD ? grads : units).push_back(h);
+                continue;
+            }
+            const int K = (int)grp.size();
+            NGate f;
+            f.type = h.type == K_GRAD ? K_GRAD : K_PAIRSUM;
+            f.grad_kind = h.type == K_GRAD ? K_PAIRSUM : K_NONE;
+            f.param = h.param;
+            f.src = h.src;
+            for (size_t k : grp) {
+                f.targets.push_back(in[k].targets[0]);
+                f.targets.push_back(in[k].targets[1]);
+                f.data.push_back(Z{code(in[k].targets[0]), code(in[k].targets[1])});
+            }
+            const Z e = h.data[0], o = h.data[1];
+            if (h.type == K_GRAD) {
+                for (int c = 0; c <= K; ++c)
+                    f.data.push_back(Z{(K - c) * e.re + c * o.re, (K - c) * e.im + c * o.im});
+            } else {
+                std::vector<Z> pe(K + 1), po(K + 1);
+                pe[0] = po[0] = Z{1, 0};
+                for (int c = 1; c <= K; ++c) {
+                    pe[c] = Z{pe[c - 1].re * e.re - pe[c - 1].im * e.im, pe[c - 1].re * e.im + pe[c - 1].im * e.re};
+                    po[c] = Z{po[c - 1].re * o.re - po[c - 1].im * o.im, po[c - 1].re * o.im + po[c - 1].im * o.re};
+                }
+                for (int c = 0; c <= K; ++c) {
+                    const Z a = pe[K - c], b = po[c];
+                    f.data.push_back(Z{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re});
+                }
+            }
+            (h.type == K_GRAD ? grads : units).push_back(f);
+        }
+        out.insert(out.end(), grads.begin(), grads.end());
+        out.insert(out.end(), units.begin(), units.end());
+        i = j;
+    }
+    return out;
+}
+
 int rank_gf2(std::vector<uint32_t> v) {
     int r = 0;
     for (int bit = 31; bit >= 0; --bit) {
@@ -605,7 +725,8 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                 return -1;
             };
             ph.op_begin = (int32_t)prog.ops.size();
-            const std::vector<NGate> fused = fuse_phase(gates, groups[p], R, rq, opt.fuse_dense);
+            std::vector<NGate> fused = fuse_phase(gates, groups[p], R, rq, opt.fuse_dense);
+            if (opt.fuse_pairs) fused = fuse_pairsums(fused, R, rq);
             for (const NGate& g : fused) {
                 KOp op;
                 std::memset(&op, 0, sizeof(op));
@@ -644,6 +765,9 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                 } else if (kind == K_X || kind == K_RESET) {
                     op.t0 = (uint8_t)kbit(g.targets[0]);
                     op.flags = g.pure ? 1 : 0;
+                    prog.pool.insert(prog.pool.end(), g.data.begin(), g.data.end());
+                } else if (kind == K_PAIRSUM) {
+                    op.nreg = (uint8_t)((g.data.size() - 1) / 2);
                     prog.pool.insert(prog.pool.end(), g.data.begin(), g.data.end());
                 } else if (kind == K_SWAP) {
                     int a = kbit(g.targets[0]), b = kbit(g.targets[1]);

@@ -44,6 +44,9 @@ struct SchedOptions {
     int low_qubits = 3;    // lowest qubits always in a tile (coalesced runs)
     int budget = 96;       // FMA-per-amplitude budget of a pass
     int swizzle_width = 3; // log2 of the 16-byte (c128) / 8-byte (c64) slots of one bank sweep
+    bool fuse_pairs = true;   // fold runs of identical parity-symmetric 2-qubit diagonals into one
+                              // K_PAIRSUM (the interpreted kernels; the specialised kernels keep
+                              // diagonals as pending factors at no cost and take K_PAIRSUM off)
     bool fuse_dense = false;  // fold runs of register-local gates of a phase into one dense block
                               // (measured slower on the layered benchmark: dense blocks reload
                               // their matrix per amplitude group)

@@ -59,7 +59,12 @@ enum KType : uint8_t {
     K_PHASE = 8, // scalar factor when all controls are set
     K_RESET = 9, // deterministic reset of register bit t0 (sim/statevector/sim.go:168-186)
     K_GRAD = 10, // adjoint: Re <lambda| G |psi> into gradient slot `slot`; flags = the
-                 // structure of G (K_U1..K_U4 dense on t0.., K_DIAG, K_PHASE)
+                 // structure of G (K_U1..K_U4 dense on t0.., K_DIAG, K_PHASE, K_PAIRSUM)
+    K_PAIRSUM = 11, // nreg = K qubit pairs: factor T[c] where c is the number of pairs
+                    // whose two bits differ at the amplitude (a run of identical
+                    // parity-symmetric 2-qubit diagonals, e.g. the RZZ(gamma) of a QAOA
+                    // layer). Pool: K pair codes (re, im = code of each qubit: register
+                    // bit 0..3, or 16 + global qubit), then T[0..K].
 };
 
 constexpr int MAX_GRAD_SLOTS = 64;  // gradient ops per pass
@@ -382,6 +387,45 @@ GQ_HD void k_phase(cplx<T> (&a)[NREG], const cplx<T> s, uint32_t creg) {
         if ((j & creg) == creg) a[j] = cmul(s, a[j]);
 }
 
+// Per-slot counts of a K_PAIRSUM's odd pairs, one byte per register slot
+// (slots 0..7 in lo, 8..15 in hi): each pair adds 1 to the slots where its
+// two bits differ. slot_bits(r, h): byte j = bit r of slot j (h: of j + 8).
+GQ_HD uint64_t slot_bits(int r, bool h) {
+    return r == 0 ? 0x0100010001000100ull
+                  : (r == 1 ? 0x0101000001010000ull : (r == 2 ? 0x0101010100000000ull : (h ? 0x0101010101010101ull : 0ull)));
+}
+
+// Byte mask of a pair code: a register bit's slot pattern, or a global
+// qubit's bit of g0 broadcast to every slot.
+GQ_HD uint64_t code_bits(int code, uint64_t g0, bool h) {
+    if (code < 16) return slot_bits(code, h);
+    return ((g0 >> (code - 16)) & 1ull) ? 0x0101010101010101ull : 0ull;
+}
+
+template <class T, class MP>
+GQ_HD void pair_counts(MP codes, uint32_t K, uint64_t g0, uint64_t& lo, uint64_t& hi) {
+    lo = hi = 0;
+    for (uint32_t k = 0; k < K; ++k) {
+        const cplx<T> cd = ldc(codes, k);
+        const int c0 = (int)cd.x, c1 = (int)cd.y;
+        lo += code_bits(c0, g0, false) ^ code_bits(c1, g0, false);
+        hi += code_bits(c0, g0, true) ^ code_bits(c1, g0, true);
+    }
+}
+
+GQ_HD uint32_t slot_count(uint64_t lo, uint64_t hi, int j) {
+    return (uint32_t)(((j < 8 ? lo : hi) >> (8 * (j & 7))) & 0xffull);
+}
+
+template <class T>
+GQ_HD void k_pairsum(cplx<T> (&a)[NREG], const cplx<T>* d, uint32_t K, uint64_t g0) {
+    uint64_t lo, hi;
+    pair_counts<T>(d, K, g0, lo, hi);
+    const cplx<T>* table = d + K;
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) a[j] = cmul(ldc(table, slot_count(lo, hi, j)), a[j]);
+}
+
 // Applies one op to the thread's 16 amplitudes. g0 is the global index of the
 // thread's register slot 0 (its thread bits and the CTA's base).
 template <class T>
@@ -475,6 +519,9 @@ GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint
         case K_PHASE:
             k_phase<T>(a, ldc(m, 0), creg);
             break;
+        case K_PAIRSUM:
+            k_pairsum<T>(a, m, op.nreg, g0);
+            break;
         case K_RESET:
             switch (op.t0) {
                 case 0: k_reset<T, 0>(a); break;
@@ -561,6 +608,14 @@ GQ_HD double grad_partial(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], co
             }
             return acc;
         }
+        case K_PAIRSUM: {  // G = sum of the pairs' generators: T[c] per slot
+            uint64_t lo, hi;
+            pair_counts<T>(m, op.nreg, g0, lo, hi);
+            const cplx<T>* table = m + op.nreg;
+#pragma unroll
+            for (int j = 0; j < NREG; ++j) acc += cdot_re(b[j], cmul(ldc(table, slot_count(lo, hi, j)), a[j]));
+            return acc;
+        }
         default: {
             // dense G on the target register bits: apply it to a copy of psi
             // (the amplitudes whose controls are unset keep psi's values and
@@ -615,7 +670,7 @@ GQ_HD void run_phase_dual(cplx<T>* sm_a, cplx<T>* sm_b, const PhaseDesc& ph, con
     for (int o = ob; o < oe; ++o) {
         const KOp& op = ops[o];
         if (op.type == K_GRAD) {
-            const double v = (op.flags == K_PHASE || op.flags == K_DIAG)
+            const double v = (op.flags == K_PHASE || op.flags == K_DIAG || op.flags == K_PAIRSUM)
                                  ? grad_partial<T>(a, b, op, pool, g0)
                                  : grad_partial_dense<T>(a, b, op, pool, g0, sm_a, sbase, ph.rslot);
             grad(op.slot, v);

@@ -11,7 +11,7 @@ import os
 import numpy as np
 import pytest
 
-from goqu_b200 import _abi, encode
+from goqu_b200 import _abi, circuit as ir, encode, workloads
 from oracle import binding as orc
 
 from kat_util import build_circuit, cplx, load_kats, random_circuit
@@ -212,3 +212,29 @@ def test_emulated_dense_fusion_matches_oracle(emu, n, seed, tile):
                                   ops.ptr(), len(ops), tile, 400, ctypes.byref(p), ctypes.byref(q))
     assert rc == 0
     np.testing.assert_allclose(st, want, atol=1e-12, rtol=0)
+
+
+def test_qaoa_layers_fuse_into_pair_sums(emu):
+    # QAOA: the RZZ(gamma) of a layer fold into K_PAIRSUM ops (one table lookup
+    # per amplitude); the result and the adjoint gradient stay exact
+    from goqu_b200 import pauli as P
+    emu.gqx_schedule_stats.restype = ctypes.c_int
+    emu.gqx_schedule_stats.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_abi.gq_op), ctypes.c_size_t,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    for c, names, h, x in workloads.qaoa_batch(4, seed=17, n_values=(8, 10, 12)):
+        n = c.NumQubits()
+        bound = ir.Bind(c, {nm: float(x[i]) for i, nm in enumerate(names)})
+        ops = encode.statevector_ops(bound)
+        out = (ctypes.c_int64 * 5)()
+        assert emu.gqx_schedule_stats(n, 0, ops.ptr(), len(ops), 0, 0, 0, out) == 0
+        assert out[4] >= 1  # fused
+        got, _, _ = run_emu(emu, ops)
+        np.testing.assert_allclose(got, orc.sv_evolve(ops), atol=1e-12, rtol=0)
+        e, g = _emu_adjoint(emu, c, names, x, h)
+        assert abs(e - _oracle_energy(c, names, x, h)) < 1e-12
+        for i in range(len(names)):
+            xp, xm = np.array(x, float), np.array(x, float)
+            xp[i] += 1e-5
+            xm[i] -= 1e-5
+            fd = (_oracle_energy(c, names, xp, h) - _oracle_energy(c, names, xm, h)) / 2e-5
+            assert abs(g[i] - fd) < 1e-6
