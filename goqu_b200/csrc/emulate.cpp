@@ -242,8 +242,30 @@ int gqx_emulate_dm(int nq, double* rho, const gq_op* ops, size_t n_ops, int tile
 // Adjoint gradient on the host through the same reverse program and dual
 // tile code as the device: psi forward, lambda = sum_t Re(c_t) P_t psi, then
 // the reverse passes accumulating 2 Re <lambda| G |psi> per parameter.
+static int emulate_adjoint_impl(int nq, const gq_op* ops, size_t n_ops, const gq_pauli_term* terms, size_t n_terms,
+                                size_t n_params, int tile_qubits, int budget, double* grad_out, double* energy_out,
+                                const char* csrc, const char* work, int64_t* jitted);
+
 int gqx_emulate_adjoint(int nq, const gq_op* ops, size_t n_ops, const gq_pauli_term* terms, size_t n_terms,
                         size_t n_params, int tile_qubits, int budget, double* grad_out, double* energy_out) {
+    return emulate_adjoint_impl(nq, ops, n_ops, terms, n_terms, n_params, tile_qubits, budget, grad_out, energy_out,
+                                nullptr, nullptr, nullptr);
+}
+
+// The same gradient with the reverse passes run through the host form of the
+// specialised dual kernels (jit_plan_dual): the generated code is compiled
+// with the host compiler in `work` (tile_core.cuh from `csrc`).
+// *jitted = reverse passes that ran generated code.
+int gqx_jit_emulate_adjoint(int nq, const gq_op* ops, size_t n_ops, const gq_pauli_term* terms, size_t n_terms,
+                            size_t n_params, int tile_qubits, int budget, double* grad_out, double* energy_out,
+                            const char* csrc, const char* work, int64_t* jitted) {
+    return emulate_adjoint_impl(nq, ops, n_ops, terms, n_terms, n_params, tile_qubits, budget, grad_out, energy_out,
+                                csrc, work, jitted);
+}
+
+static int emulate_adjoint_impl(int nq, const gq_op* ops, size_t n_ops, const gq_pauli_term* terms, size_t n_terms,
+                                size_t n_params, int tile_qubits, int budget, double* grad_out, double* energy_out,
+                                const char* csrc, const char* work, int64_t* jitted) {
     const int nphys = nq < gq::RQ ? gq::RQ : nq;
     std::vector<gq::NGate> fwd, rev;
     std::vector<int> fo, ro;
@@ -280,8 +302,68 @@ int gqx_emulate_adjoint(int nq, const gq_op* ops, size_t n_ops, const gq_pauli_t
     std::vector<double> grad(n_params, 0.0);
     std::vector<gq::cplx<double>> pool(pr.pool.size());
     for (size_t i = 0; i < pool.size(); ++i) pool[i] = {pr.pool[i].re, pr.pool[i].im};
+    // generated dual passes (host form), when asked for
+    typedef void (*DualFn)(gq::cplx<double>*, gq::cplx<double>*, const gq::cplx<double>*, const gq::cplx<double>*,
+                           const gq::PhaseDesc*, double*, int, gq::cplx<double>*, double*);
+    std::vector<gq::JitPlan> plans(csrc ? pr.passes.size() : 0);
+    std::vector<char> planned(plans.size(), 0);
+    void* lib = nullptr;
+    if (csrc) {
+        std::string src;
+        for (size_t i = 0; i < pr.passes.size(); ++i) {
+            const int threads = 1 << (pr.passes[i].m - gq::RQ);
+            if (!gq::jit_plan_dual(pr, i, false, threads, 1, plans[i], true)) continue;
+            planned[i] = 1;
+            src += plans[i].host_source;
+        }
+        const std::string dir = work;
+        const std::string cpp = dir + "/gqj_hostdual.cpp", so = dir + "/gqj_hostdual.so";
+        FILE* f = std::fopen(cpp.c_str(), "w");
+        if (!f) {
+            g_err = "cannot write " + cpp;
+            return GQ_EINVAL;
+        }
+        std::fwrite(src.data(), 1, src.size(), f);
+        std::fclose(f);
+        const std::string cmd = "g++ -O1 -std=c++17 -shared -fPIC -w -I'" + std::string(csrc) + "' '" + cpp +
+                                "' -o '" + so + "' 2>'" + dir + "/gqj_hostdual.log'";
+        if (std::system(cmd.c_str()) != 0) {
+            g_err = "host compile of the generated dual passes failed (" + dir + "/gqj_hostdual.log)";
+            return GQ_EINVAL;
+        }
+        lib = dlopen(so.c_str(), RTLD_NOW | RTLD_LOCAL);
+        if (!lib) {
+            g_err = dlerror();
+            return GQ_EINVAL;
+        }
+        *jitted = 0;
+    }
     for (size_t pi = 0; pi < pr.passes.size(); ++pi) {
         const gq::PassDesc& pd = pr.passes[pi];
+        DualFn fn = nullptr;
+        std::vector<gq::cplx<double>> block;
+        if (lib && planned[pi]) {
+            block.resize(plans[pi].n_param);
+            if (gq::jit_pack(pr, pi, plans[pi], false, block.data()))
+                fn = (DualFn)dlsym(lib, ("gqj_hostdual_" + std::to_string(pi)).c_str());
+        }
+        if (fn) {
+            const int nslots = (int)pr.pass_params[pi].size();
+            const uint64_t nc = 1ull << pd.n_outer;
+            std::vector<double> part(nc * (size_t)std::max(1, nslots)), gsm(4 * gq::MAX_GRAD_SLOTS);
+            std::vector<gq::cplx<double>> smem(2u << pd.m);
+            uint32_t op_base, pool_base;
+            gq::jit_bases(pr, pi, &op_base, &pool_base);
+            fn(psi.data(), lam.data(), block.data(), pool.data() + pool_base, pr.phases.data() + pd.phase0,
+               part.data(), nslots, smem.data(), gsm.data());
+            for (int sl = 0; sl < nslots; ++sl) {
+                double tot = 0.0;
+                for (uint64_t c = 0; c < nc; ++c) tot += part[c * nslots + sl];
+                grad[pr.pass_params[pi][sl]] += 2.0 * tot;
+            }
+            ++*jitted;
+            continue;
+        }
         const int m = pd.m;
         const uint32_t tpb = 1u << (m - gq::RQ);
         std::vector<gq::cplx<double>> sa(1u << m), sb(1u << m);
@@ -309,6 +391,7 @@ int gqx_emulate_adjoint(int nq, const gq_op* ops, size_t n_ops, const gq_pauli_t
         }
         for (size_t sl = 0; sl < pr.pass_params[pi].size(); ++sl) grad[pr.pass_params[pi][sl]] += 2.0 * slots[sl];
     }
+    if (lib) dlclose(lib);
     for (size_t i = 0; i < n_params; ++i) grad_out[i] = grad[i];
     if (energy_out) *energy_out = energy;
     return GQ_OK;
@@ -417,6 +500,50 @@ int gqx_jit_emulate(int nq, int precision, double* state, const gq_op* ops, size
     out[0] = (int64_t)prog.passes.size();
     out[1] = jitted;
     return rc;
+}
+
+// The reverse sweep of an adjoint gradient as specialised dual kernels: the
+// reverse program of `ops` scheduled as the engine does (11-qubit tiles),
+// each pass's dual kernel text compiled with NVRTC at the engine's launch
+// bounds. out: [passes, passes with a kernel text, compiled].
+int gqx_jit_check_dual(int nq, int precision, const gq_op* ops, size_t n_ops, size_t n_params, int max_compile,
+                       int64_t* out) {
+    if (!gq::jit_available()) {
+        g_err = "libnvrtc not found";
+        return GQ_EUNSUPPORTED;
+    }
+    const int nphys = nq < gq::RQ ? gq::RQ : nq;
+    std::vector<gq::NGate> fwd, rev;
+    std::vector<int> fo, ro;
+    int rc = gq::adjoint_gates(nq, ops, n_ops, n_params, fwd, rev, fo, ro, g_err);
+    if (rc != GQ_OK) return rc;
+    gq::SchedOptions opt;
+    opt.tile_qubits = 11;
+    opt.budget = 320;
+    opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
+    opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    gq::Program pr;
+    gq::schedule(rev, nphys, opt, pr);
+    std::set<std::string> texts;
+    int64_t planned = 0, compiled = 0;
+    for (size_t i = 0; i < pr.passes.size(); ++i) {
+        gq::JitPlan pl;
+        const int threads = 1 << (pr.passes[i].m - gq::RQ);
+        if (!gq::jit_plan_dual(pr, i, precision == GQ_C64, threads, 2, pl)) continue;
+        ++planned;
+        if (!texts.insert(pl.source).second || compiled >= max_compile) continue;
+        std::string log;
+        const std::string err = gq::jit_compile_only(pl.source, nullptr, &log);
+        if (!err.empty()) {
+            g_err = err.substr(0, 4000);
+            return GQ_ECUDA;
+        }
+        ++compiled;
+    }
+    out[0] = (int64_t)pr.passes.size();
+    out[1] = planned;
+    out[2] = compiled;
+    return GQ_OK;
 }
 
 }  // extern "C"

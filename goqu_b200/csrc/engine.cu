@@ -189,6 +189,7 @@ struct Engine {
     cudaStream_t stream = nullptr;
     DevBuf state, prog, scratch, scratch2, aux;
     DevBuf lam, ckpt, adj_partial, adj_grad;  // adjoint differentiation
+    int adj_nparams = 0;                      // parameters of the current gradient
     int adj_segments = 0;                     // forward checkpoints (0: automatic)
     PinnedBuf staging, hostio;
     cudaEvent_t staged = nullptr, ev0 = nullptr, ev1 = nullptr, ev_pass0 = nullptr, ev_pass1 = nullptr;
@@ -375,51 +376,129 @@ struct Engine {
     template <class T>
     int run_adjoint_t(const Program& pr) {
         if (pr.passes.empty()) return GQ_OK;
+        const size_t np = pr.passes.size();
         size_t nslot_total = 0;
         for (const auto& v : pr.pass_params) nslot_total += v.size();
+        const size_t ns1 = std::max<size_t>(1, nslot_total);
         const size_t o_pass = 0;
-        const size_t o_phase = align16(o_pass + sizeof(PassDesc) * pr.passes.size());
+        const size_t o_phase = align16(o_pass + sizeof(PassDesc) * np);
         const size_t o_ops = align16(o_phase + sizeof(PhaseDesc) * pr.phases.size());
         const size_t o_pool = align16(o_ops + sizeof(KOp) * pr.ops.size());
         const size_t o_slots = align16(o_pool + sizeof(cplx<T>) * std::max<size_t>(1, pr.pool.size()));
-        const size_t total = align16(o_slots + sizeof(int) * std::max<size_t>(1, nslot_total));
+        const size_t o_soff = align16(o_slots + sizeof(int) * ns1);
+        const size_t o_sn = align16(o_soff + sizeof(uint64_t) * ns1);
+        const size_t o_sst = align16(o_sn + sizeof(uint64_t) * ns1);
+        const size_t total = align16(o_sst + sizeof(uint32_t) * ns1);
         void* hp = nullptr;
         GQ_TRY(stage(total, &hp));
         char* h = (char*)hp;
-        std::memcpy(h + o_pass, pr.passes.data(), sizeof(PassDesc) * pr.passes.size());
+        std::memcpy(h + o_pass, pr.passes.data(), sizeof(PassDesc) * np);
         std::memcpy(h + o_phase, pr.phases.data(), sizeof(PhaseDesc) * pr.phases.size());
         if (!pr.ops.empty()) std::memcpy(h + o_ops, pr.ops.data(), sizeof(KOp) * pr.ops.size());
         cplx<T>* pool = (cplx<T>*)(h + o_pool);
         for (size_t i = 0; i < pr.pool.size(); ++i) pool[i] = {(T)pr.pool[i].re, (T)pr.pool[i].im};
+        // Gradient partials of consecutive passes share one buffer (up to
+        // kPartialCap doubles) and are reduced by two launches per group of
+        // passes (k_slot_sums, k_param_sums) instead of one per pass.
+        constexpr uint64_t kPartialCap = 16ull << 20;
         int* slots = (int*)(h + o_slots);
+        uint64_t* soff = (uint64_t*)(h + o_soff);
+        uint64_t* sn = (uint64_t*)(h + o_sn);
+        uint32_t* sst = (uint32_t*)(h + o_sst);
+        std::vector<uint64_t> pass_off(np);
+        std::vector<size_t> pass_slot0(np);
+        std::vector<size_t> group_end;  // last pass of each group
+        uint64_t used = 0, max_group = 1;
         size_t k = 0;
-        uint64_t max_part = 1;
-        for (size_t i = 0; i < pr.passes.size(); ++i) {
-            for (int v : pr.pass_params[i]) slots[k++] = v;
-            max_part = std::max<uint64_t>(max_part, (1ull << pr.passes[i].n_outer) * pr.pass_params[i].size());
+        for (size_t i = 0; i < np; ++i) {
+            const uint64_t grid = 1ull << pr.passes[i].n_outer;
+            const uint64_t ns = pr.pass_params[i].size();
+            if (used && used + grid * ns > kPartialCap) {
+                group_end.push_back(i - 1);
+                used = 0;
+            }
+            pass_off[i] = used;
+            pass_slot0[i] = k;
+            for (uint64_t sl = 0; sl < ns; ++sl, ++k) {
+                slots[k] = pr.pass_params[i][sl];
+                soff[k] = used + sl;
+                sn[k] = grid;
+                sst[k] = (uint32_t)ns;
+            }
+            used += grid * ns;
+            max_group = std::max(max_group, used);
         }
+        group_end.push_back(np - 1);
         GQ_TRY(upload(prog, total));
-        GQ_TRY(adj_partial.ensure(max_part * sizeof(double)));
+        GQ_TRY(adj_partial.ensure((max_group + ns1) * sizeof(double)));
+        double* partial = (double*)adj_partial.p;
+        double* sums = partial + max_group;
         char* d = (char*)prog.p;
-        size_t slot_off = 0;
-        for (size_t i = 0; i < pr.passes.size(); ++i) {
+        // specialised dual kernels for the passes whose compilation has
+        // finished (or, with GQ_OPT_JIT = 2, once it has)
+        std::vector<const void*> jfn(np, nullptr);
+        std::vector<const CachedPlan*> plans(np, nullptr);
+        if (jit_on()) {
+            const int minb = 2;  // both states' 16 amplitudes and a gradient copy in registers
+            for (size_t i = 0; i < np; ++i) {
+                const PassDesc& pd = pr.passes[i];
+                plans[i] = jit_cached_plan(pr, i, prec == GQ_C64, 1 << (pd.m - RQ), minb, false, true);
+                if (plans[i]->ok) jfn[i] = jit_plan_kernel(plans[i], adj_smem(sizeof(cplx<T>), pd.m));
+            }
+            if (jit_mode == 2) {
+                jit_wait(600000.0);
+                for (size_t i = 0; i < np; ++i)
+                    if (plans[i]->ok && !jfn[i])
+                        jfn[i] = jit_plan_kernel(plans[i], adj_smem(sizeof(cplx<T>), pr.passes[i].m));
+            }
+        }
+        std::vector<cplx<T>> pblock;
+        int64_t jitted = 0;
+        size_t gi = 0, slot_lo = 0;
+        for (size_t i = 0; i < np; ++i) {
             const PassDesc& pd = pr.passes[i];
             const int nslots = (int)pr.pass_params[i].size();
             const unsigned threads = 1u << (pd.m - RQ);
             const unsigned grid = 1u << pd.n_outer;
-            AdjTable<T>::get()<<<grid, threads, adj_smem(sizeof(cplx<T>), pd.m), stream>>>(
-                (cplx<T>*)state.p, (cplx<T>*)lam.p, (const PassDesc*)(d + o_pass) + i, (const PhaseDesc*)(d + o_phase),
-                (const KOp*)(d + o_ops), (const cplx<T>*)(d + o_pool), (double*)adj_partial.p, nslots);
-            ++stats.kernel_launches;
-            if (nslots > 0) {
-                k_grad_reduce<<<1, 1024, 0, stream>>>((const double*)adj_partial.p, grid, nslots,
-                                                      (const int*)(d + o_slots) + slot_off, (double*)adj_grad.p);
-                ++stats.kernel_launches;
+            const size_t smem = adj_smem(sizeof(cplx<T>), pd.m);
+            double* part = partial + pass_off[i];
+            if (jfn[i]) pblock.resize(plans[i]->plan.n_param);
+            if (jfn[i] && jit_pack(pr, i, plans[i]->plan, prec == GQ_C64, pblock.data())) {
+                uint32_t op_base, pool_base;
+                jit_bases(pr, i, &op_base, &pool_base);
+                cplx<T>* psi = (cplx<T>*)state.p;
+                cplx<T>* lm = (cplx<T>*)lam.p;
+                const cplx<T>* poolp = (const cplx<T>*)(d + o_pool) + pool_base;
+                const PhaseDesc* php = (const PhaseDesc*)(d + o_phase) + pd.phase0;
+                int ns = nslots;
+                void* args[7] = {&psi, &lm, pblock.data(), &poolp, &php, &part, &ns};
+                GQ_CUDA(cudaLaunchKernel(jfn[i], dim3(grid), dim3(threads), args, smem, stream));
+                ++jitted;
+            } else {
+                AdjTable<T>::get()<<<grid, threads, smem, stream>>>(
+                    (cplx<T>*)state.p, (cplx<T>*)lam.p, (const PassDesc*)(d + o_pass) + i,
+                    (const PhaseDesc*)(d + o_phase), (const KOp*)(d + o_ops), (const cplx<T>*)(d + o_pool), part,
+                    nslots);
             }
-            slot_off += nslots;
+            ++stats.kernel_launches;
+            if (i == group_end[gi]) {
+                const size_t slot_hi = pass_slot0[i] + nslots;
+                const int ns = (int)(slot_hi - slot_lo);
+                if (ns > 0) {
+                    k_slot_sums<<<ns, 256, 0, stream>>>(partial, (const uint64_t*)(d + o_soff) + slot_lo,
+                                                         (const uint64_t*)(d + o_sn) + slot_lo,
+                                                         (const uint32_t*)(d + o_sst) + slot_lo, sums);
+                    k_param_sums<<<(adj_nparams + 255) / 256, 256, 0, stream>>>(
+                        sums, (const int*)(d + o_slots) + slot_lo, ns, adj_nparams, (double*)adj_grad.p);
+                    stats.kernel_launches += 2;
+                }
+                slot_lo = slot_hi;
+                ++gi;
+            }
         }
         GQ_CUDA(cudaGetLastError());
-        stats.passes += (int64_t)pr.passes.size();
+        stats.jit_passes += jitted;
+        stats.passes += (int64_t)np;
         stats.phases += (int64_t)pr.phases.size();
         return GQ_OK;
     }
@@ -890,6 +969,7 @@ int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_p
     const size_t sbytes = e.n_amps * e.amp_bytes();
     GQ_TRY(e.lam.ensure(sbytes));
     GQ_TRY(e.adj_grad.ensure(std::max<size_t>(1, n_params) * sizeof(double)));
+    e.adj_nparams = (int)n_params;
     // Forward segments (checkpoints bound the drift of un-applying gates).
     int segs = e.adj_segments;
     if (segs <= 0) segs = (e.prec == GQ_C64 && n_ops > 256) ? (int)std::min<size_t>(8, n_ops / 128) : 1;

@@ -117,7 +117,8 @@ JitState jit_lookup(const std::string& source, size_t smem_bytes, bool queue, co
     if (e.state == JIT_PENDING && !e.cubin.empty()) {
         // libraries and kernels are context independent: one load serves every device
         cudaError_t err = cudaLibraryLoadData(&e.lib, e.cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-        if (err == cudaSuccess) err = cudaLibraryGetKernel(&e.kernel, e.lib, "gqj_pass");
+        const char* name = source.find("\ngqj_dual(") != std::string::npos ? "gqj_dual" : "gqj_pass";
+        if (err == cudaSuccess) err = cudaLibraryGetKernel(&e.kernel, e.lib, name);
         if (err != cudaSuccess) {
             e.state = JIT_FAILED;
             e.log = cudaGetErrorString(err);
@@ -164,7 +165,7 @@ void put(std::string& k, const V& v) {
 }  // namespace
 
 const CachedPlan* jit_cached_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks,
-                                  bool persistent) {
+                                  bool persistent, bool dual) {
     const PassDesc& pd = pr.passes[pi];
     uint32_t op_base, pool_base;
     jit_bases(pr, pi, &op_base, &pool_base);
@@ -174,6 +175,7 @@ const CachedPlan* jit_cached_plan(const Program& pr, size_t pi, bool c64, int th
     put(key, threads);
     put(key, min_blocks);
     put(key, (int)persistent);
+    put(key, (int)dual);
     put(key, pd.m);
     put(key, pd.n_outer);
     put(key, pd.n_phases);
@@ -190,7 +192,7 @@ const CachedPlan* jit_cached_plan(const Program& pr, size_t pi, bool c64, int th
         put(key, ph.op_end - ph.op_begin);
         for (int o = ph.op_begin; o < ph.op_end; ++o) {
             const KOp& op = pr.ops[o];
-            const uint8_t b[8] = {op.type, op.t0, op.t1, op.t2, op.creg, op.nreg, op.flags, 0};
+            const uint8_t b[8] = {op.type, op.t0, op.t1, op.t2, op.creg, op.nreg, op.flags, (uint8_t)op.slot};
             key.append((const char*)b, 8);
             put(key, op.mat - pool_base);
             put(key, op.cmask);
@@ -209,7 +211,8 @@ const CachedPlan* jit_cached_plan(const Program& pr, size_t pi, bool c64, int th
     if (it != pc.map.end()) return it->second.get();
     if (pc.map.size() >= 8192) pc.map.clear();  // bound the cache; plans are regenerated on demand
     std::unique_ptr<CachedPlan> cp(new CachedPlan());
-    cp->ok = jit_plan(pr, pi, c64, threads, min_blocks, persistent, cp->plan);
+    cp->ok = dual ? jit_plan_dual(pr, pi, c64, threads, min_blocks, cp->plan)
+                  : jit_plan(pr, pi, c64, threads, min_blocks, persistent, cp->plan);
     const CachedPlan* r = cp.get();
     pc.map.emplace(std::move(key), std::move(cp));
     return r;

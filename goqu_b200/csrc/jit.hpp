@@ -68,6 +68,13 @@ struct JitPlan {
 // parameter block over the kernel-parameter limit): they stay interpreted.
 bool jit_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks, bool persistent, JitPlan& out,
               bool host = false);
+// The reverse (adjoint) pass on psi and lambda at once (kernel gqj_dual):
+// every op on both states, gradient ops adding Re <lambda|G|psi> into
+// per-warp slots that each CTA sums into partial[cta * nslots + slot], as
+// k_adjoint_pass does. Dense ops stay dense (no pending factors). With
+// `host`, host_source holds the same pass as a host function (CPU tests).
+bool jit_plan_dual(const Program& pr, size_t pass, bool c64, int threads, int min_blocks, JitPlan& out,
+                   bool host = false);
 // Op and pool indices in a plan and its kernel text are relative to the
 // pass: to its first op and that op's first pool entry (jit_bases). The
 // kernel is launched with `pool` advanced by pool_base and `phases` by the
@@ -95,7 +102,7 @@ struct CachedPlan {
     bool failed = false;    // compilation or loading failed
 };
 const CachedPlan* jit_cached_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks,
-                                  bool persistent);
+                                  bool persistent, bool dual = false);
 // The compiled kernel of a cached plan (queues its compilation on first call);
 // nullptr until it is ready.
 const void* jit_plan_kernel(const CachedPlan* cp, size_t smem_bytes);

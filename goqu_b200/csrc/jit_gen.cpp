@@ -447,6 +447,243 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
     return true;
 }
 
+bool jit_plan_dual(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, JitPlan& out, bool host) {
+    const PassDesc& pd = pr.passes[pi];
+    uint32_t op_base, pool_base;
+    jit_bases(pr, pi, &op_base, &pool_base);
+    const int m = pd.m, tbits = m - RQ;
+    if (tbits < 0 || (1 << tbits) != threads) return false;
+    out.atoms.clear();
+    out.entries.clear();
+    out.phase_shears.clear();
+    Gen gen(pr, out, c64 ? 3900u : 1950u);
+
+    std::string pro = "    uint64_t base = 0;\n";
+    emit_deposit(pro, "    ", "base", "cta", pd.outer_q, pd.n_outer);
+    pro += "    uint64_t gt = base;\n    uint32_t stt = 0;\n";
+    emit_deposit(pro, "    ", "gt", "t", pd.tile_q, tbits);
+    for (int k = 0; k < tbits; ++k)
+        pro += "    stt ^= (0u - ((t >> " + num(k) + ") & 1u)) & " + hex32(pd.acol[k]) + ";\n";
+    pro += "    (void)gt;\n    (void)stt;\n";
+    uint64_t G[NREG];
+    uint32_t S[NREG];
+    for (int it = 0; it < NREG; ++it) {
+        G[it] = 0;
+        S[it] = 0;
+        for (int k = 0; k < RQ; ++k)
+            if ((it >> k) & 1) {
+                G[it] |= 1ull << pd.tile_q[tbits + k];
+                S[it] ^= pd.acol[tbits + k];
+            }
+    }
+    std::string seg_in = "    {\n        cplx<T> v[16], w[16];\n";
+    for (int it = 0; it < NREG; ++it)
+        seg_in += "        v[" + num(it) + "] = psi[gt | " + hex64(G[it]) + "];\n        w[" + num(it) + "] = lam[gt | " +
+                  hex64(G[it]) + "];\n";
+    for (int it = 0; it < NREG; ++it)
+        seg_in += "        sa[stt ^ " + hex32(S[it]) + "] = v[" + num(it) + "];\n        sbuf[stt ^ " + hex32(S[it]) +
+                  "] = w[" + num(it) + "];\n";
+    seg_in += "    }\n";
+    std::string seg_out = "    {\n";
+    for (int it = 0; it < NREG; ++it)
+        seg_out += "        psi[gt | " + hex64(G[it]) + "] = sa[stt ^ " + hex32(S[it]) + "];\n        lam[gt | " +
+                   hex64(G[it]) + "] = sbuf[stt ^ " + hex32(S[it]) + "];\n";
+    seg_out += "    }\n";
+    const std::string SL = num(MAX_GRAD_SLOTS);
+    // per-warp slot sums: the device reduces a warp's lanes with shuffles;
+    // the host form (threads in turn) adds each thread's value
+    auto flush = [&](int slot, bool hst) -> std::string {
+        if (hst) return "        gsm[(t >> 5) * " + SL + " + " + num(slot) + "] += gacc; gacc = 0.0;\n";
+        return "        { double fv = gacc; for (unsigned o = 16; o > 0; o >>= 1) { const double y = "
+               "__shfl_xor_sync(lanes, fv, o); if ((lane ^ o) < (int)nlanes) fv += y; } if (lane == 0) gsm[warp * " +
+               SL + " + " + num(slot) + "] += fv; gacc = 0.0; }\n";
+    };
+    std::vector<std::string> ph_dev, ph_host;
+    for (int p = 0; p < pd.n_phases; ++p) {
+        const PhaseDesc& ph = pr.phases[pd.phase0 + p];
+        uint32_t tslot[MAX_TILE];
+        int tq[MAX_TILE];
+        for (int k = 0; k < tbits; ++k) {
+            const uint32_t sv = k < 4 ? ph.tlo_slot[1u << k] : ph.thi_slot[1u << (k - 4)];
+            const uint64_t g = k < 4 ? ph.tlo_glob[1u << k] : ph.thi_glob[1u << (k - 4)];
+            if (g == 0 || (g & (g - 1))) return false;
+            tslot[k] = sv;
+            tq[k] = ctz64(g);
+        }
+        for (int v = 0; v < TLO && v < (1 << tbits); ++v) {
+            uint32_t sv = 0;
+            uint64_t g = 0;
+            for (int k = 0; k < 4 && k < tbits; ++k)
+                if ((v >> k) & 1) {
+                    sv ^= tslot[k];
+                    g |= 1ull << tq[k];
+                }
+            if (sv != ph.tlo_slot[v] || g != ph.tlo_glob[v]) return false;
+        }
+        std::string head = "    {\n        uint32_t sb = 0;\n        uint64_t g0 = base;\n";
+        for (int k = 0; k < tbits; ++k)
+            head += "        sb ^= (0u - ((t >> " + num(k) + ") & 1u)) & " + hex32(tslot[k]) + ";\n";
+        emit_deposit(head, "        ", "g0", "t", tq, tbits);
+        head += "        (void)g0;\n        cplx<T> a[16], bb[16];\n        double gacc = 0.0;\n        (void)gacc;\n";
+        for (int j = 0; j < NREG; ++j)
+            head += "        a[" + num(j) + "] = sa[sb ^ " + hex32(ph.rslot[j]) + "];\n        bb[" + num(j) +
+                    "] = sbuf[sb ^ " + hex32(ph.rslot[j]) + "];\n";
+        std::string bd, bh;  // op bodies, device / host flush
+        int cur = -1;
+        for (int oa = ph.op_begin; oa < ph.op_end; ++oa) {
+            const KOp& op = pr.ops[oa];
+            const uint32_t rm = op.mat - pool_base;
+            const bool grad = op.type == K_GRAD;
+            const uint8_t kind = grad ? op.flags : op.type;
+            if (kind == K_NONE || kind == K_RESET || kind == K_GRAD || kind > K_PAIRSUM) return false;
+            const std::string creg = num(op.creg) + "u";
+            const std::string C = op.creg ? "true" : "false";
+            const std::string S0 = num(op.t0), S1 = num(op.t1), S2 = num(op.t2);
+            std::string cond;
+            if (op.cmask) cond = "if ((g0 & " + hex64(op.cmask) + ") == " + hex64(op.cmask) + ") ";
+            auto pm = [&](uint32_t off) { return "PMat<T>{p.m + " + num(off) + "}"; };
+            const bool pure_x = kind == K_X && !grad && (op.flags & 1);
+            // the op's body on register array x (xs: its shared-memory tile, U4's scratch)
+            auto body = [&](const std::string& x, const std::string& xs) -> std::string {
+                switch (kind) {
+                    case K_U1:
+                        return "k_u1<T, " + S0 + ", " + C + ">(" + x + ", " + pm(gen.copy(rm, 4)) + ", " + creg + ");";
+                    case K_U2:
+                        return "k_u2<T, " + S0 + ", " + S1 + ", " + C + ">(" + x + ", " + pm(gen.copy(rm, 16)) + ", " +
+                               creg + ");";
+                    case K_U3:
+                        return "k_u3<T, " + S0 + ", " + S1 + ", " + S2 + ">(" + x + ", " + pm(gen.copy(rm, 64)) +
+                               ", " + creg + ");";
+                    case K_U4:
+                        return "k_u4<T>(" + x + ", " + pm(gen.copy(rm, 256)) + ", " + xs + ", sb, phases[" + num(p) +
+                               "].rslot);";
+                    case K_X:
+                        return "k_x<T, " + S0 + ", " + C + ">(" + x + ", " +
+                               (pure_x ? std::string("pool") : pm(gen.copy(rm, 2))) + ", " + creg + ", " +
+                               (pure_x ? "true" : "false") + ");";
+                    case K_SWAP: return "k_swap<T, " + S0 + ", " + S1 + ">(" + x + ", " + creg + ");";
+                    case K_PHASE: return "k_phase<T>(" + x + ", p.m[" + num(gen.copy(rm, 1)) + "], " + creg + ");";
+                    case K_PAIRSUM:
+                        return "k_pairsum<T>(" + x + ", pool + " + num(rm) + "u, " + num(op.nreg) + "u, g0);";
+                    case K_DIAG: {
+                        std::string h = "{ uint32_t hi = 0; ";
+                        int k = 0;
+                        for (uint64_t dm = op.dmask; dm; dm &= dm - 1, ++k)
+                            h += "hi |= (uint32_t)((g0 >> " + num(ctz64(dm)) + ") & 1ull) << " + num(k) + "; ";
+                        h += "k_diag_hi<T>(" + x + ", pool + " + num(rm) + "u, hi << " + num(op.nreg) + ", " +
+                             num(op.nreg) + "u, " + creg + ", " + hex64(op.ridx) + "); }";
+                        return h;
+                    }
+                    default: return "";
+                }
+            };
+            if (!grad) {
+                const std::string line = "        " + cond + body("a", "sa") + "\n        " + cond + body("bb", "sbuf") + "\n";
+                bd += line;
+                bh += line;
+                continue;
+            }
+            if ((int)op.slot != cur) {  // slot runs: reduce once per run
+                if (cur >= 0) {
+                    bd += flush(cur, false);
+                    bh += flush(cur, true);
+                }
+                cur = (int)op.slot;
+            }
+            std::string e;
+            if (kind == K_PHASE) {
+                e = "gv = grad_phase_c<T>(a, bb, p.m[" + num(gen.copy(rm, 1)) + "], " + creg + ");";
+            } else if (kind == K_DIAG) {
+                std::string h = "uint32_t hi = 0; ";
+                int k = 0;
+                for (uint64_t dm = op.dmask; dm; dm &= dm - 1, ++k)
+                    h += "hi |= (uint32_t)((g0 >> " + num(ctz64(dm)) + ") & 1ull) << " + num(k) + "; ";
+                e = h + "gv = grad_diag_c<T>(a, bb, pool + " + num(rm) + "u, hi << " + num(op.nreg) + ", " + creg +
+                    ", " + hex64(op.ridx) + ");";
+            } else if (kind == K_PAIRSUM) {
+                e = "gv = grad_pairsum_c<T>(a, bb, pool + " + num(rm) + "u, " + num(op.nreg) + "u, g0);";
+            } else {  // dense G, applied to a copy of psi
+                e = "cplx<T> v[16]; for (int j = 0; j < 16; ++j) v[j] = a[j]; " + body("v", "sa") +
+                    " gv = dot_re_creg<T>(bb, v, " + creg + ");";
+            }
+            const std::string line = "        { double gv = 0.0; " + cond + "{ " + e + " } gacc += gv; }\n";
+            bd += line;
+            bh += line;
+        }
+        if (cur >= 0) {
+            bd += flush(cur, false);
+            bh += flush(cur, true);
+        }
+        std::string tail;
+        for (int j = 0; j < NREG; ++j)
+            tail += "        sa[sb ^ " + hex32(ph.rslot[j]) + "] = a[" + num(j) + "];\n        sbuf[sb ^ " +
+                    hex32(ph.rslot[j]) + "] = bb[" + num(j) + "];\n";
+        tail += "    }\n";
+        ph_dev.push_back(head + bd + tail);
+        ph_host.push_back(head + bh + tail);
+        if (gen.overflow) return false;
+    }
+
+    out.n_param = gen.np > 0 ? gen.np : 1;
+    const std::string T = c64 ? "float" : "double";
+    const std::string tile = num(1ll << m);
+    std::string& s = out.source;
+    s.clear();
+    s += "// goqu_b200 specialised reverse (adjoint) pass\n";
+    s += "typedef unsigned char uint8_t;\ntypedef int int32_t;\ntypedef unsigned int uint32_t;\n";
+    s += "typedef long long int64_t;\ntypedef unsigned long long uint64_t;\n";
+    s += "#include \"tile_core.cuh\"\n";
+    s += "namespace gq {\nstruct JP {\n    cplx<" + T + "> m[" + num(out.n_param) + "];\n};\n}\n";
+    s += "extern \"C\" __global__ void __launch_bounds__(" + num(threads) + ", " + num(min_blocks) + ")\n";
+    s += "gqj_dual(gq::cplx<" + T + ">* __restrict__ psi, gq::cplx<" + T + ">* __restrict__ lam, const "
+         "__grid_constant__ gq::JP p, const gq::cplx<" + T + ">* __restrict__ pool, const gq::PhaseDesc* __restrict__ "
+         "phases, double* __restrict__ partial, int nslots) {\n";
+    s += "    using namespace gq;\n    using T = " + T + ";\n";
+    s += "    extern __shared__ __align__(16) unsigned char smraw[];\n";
+    s += "    cplx<T>* const sa = reinterpret_cast<cplx<T>*>(smraw);\n";
+    s += "    cplx<T>* const sbuf = sa + " + tile + ";\n";
+    s += "    double* const gsm = reinterpret_cast<double*>(sbuf + " + tile + ");\n";
+    s += "    (void)pool;\n    (void)phases;\n";
+    s += "    const uint32_t t = threadIdx.x;\n    const uint64_t cta = blockIdx.x;\n";
+    s += "    const int nwarps = (int)((blockDim.x + 31) >> 5);\n";
+    s += "    const int warp = (int)(t >> 5), lane = (int)(t & 31);\n";
+    s += "    const unsigned nlanes = blockDim.x < 32 ? blockDim.x : 32u;\n";
+    s += "    const unsigned lanes = nlanes == 32 ? 0xffffffffu : ((1u << nlanes) - 1u);\n";
+    s += pro + seg_in;
+    s += "    for (int i = (int)t; i < nwarps * " + SL + "; i += (int)blockDim.x) gsm[i] = 0.0;\n";
+    s += "    __syncthreads();\n";
+    for (const std::string& ph : ph_dev) s += ph + "    __syncthreads();\n";
+    s += seg_out;
+    s += "    for (int sl = (int)t; sl < nslots; sl += (int)blockDim.x) {\n        double tot = 0.0;\n"
+         "        for (int w = 0; w < nwarps; ++w) tot += gsm[w * " + SL + " + sl];\n"
+         "        partial[cta * (uint64_t)nslots + sl] = tot;\n    }\n}\n";
+    if (host) {
+        std::string& h = out.host_source;
+        h.clear();
+        h += "#include \"tile_core.cuh\"\n";
+        h += "extern \"C\" void gqj_hostdual_" + num((long long)pi) + "(gq::cplx<" + T + ">* psi, gq::cplx<" + T +
+             ">* lam, const gq::cplx<" + T + ">* pm, const gq::cplx<" + T + ">* pool, const gq::PhaseDesc* phases, "
+             "double* partial, int nslots, gq::cplx<" + T + ">* sa, double* gsm) {\n";
+        h += "    using namespace gq;\n    using T = " + T + ";\n    (void)pool;\n    (void)phases;\n";
+        h += "    const struct {\n        const cplx<T>* m;\n    } p{pm};\n";
+        h += "    cplx<T>* const sbuf = sa + " + tile + ";\n";
+        h += "    const int nwarps = " + num((threads + 31) >> 5) + ";\n";
+        h += "    for (uint64_t cta = 0; cta < (1ull << " + num(pd.n_outer) + "); ++cta) {\n";
+        auto loop = [&](const std::string& seg) {
+            h += "    for (uint32_t t = 0; t < " + num(threads) + "u; ++t) {\n" + pro + seg + "    }\n";
+        };
+        loop(seg_in);
+        h += "    for (int i = 0; i < nwarps * " + SL + "; ++i) gsm[i] = 0.0;\n";
+        for (const std::string& ph : ph_host) loop(ph);
+        loop(seg_out);
+        h += "    for (int sl = 0; sl < nslots; ++sl) {\n        double tot = 0.0;\n"
+             "        for (int w = 0; w < nwarps; ++w) tot += gsm[w * " + SL + " + sl];\n"
+             "        partial[cta * (uint64_t)nslots + sl] = tot;\n    }\n";
+        h += "    }\n}\n";
+    }
+    return true;
+}
+
 bool jit_pack(const Program& pr, size_t pi, const JitPlan& plan, bool c64, void* block) {
     uint32_t op_base, pool_base;
     jit_bases(pr, pi, &op_base, &pool_base);

@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 // Adjoint reverse pass: the tile pass on two states (psi, lambda) at once,
 // with gradient ops. Each warp writes its sum for every gradient slot once
 // per pass into shared memory; the CTA's per-slot totals go to
-// partial[cta * nslots + slot] (summed per slot by k_grad_reduce).
+// partial[cta * nslots + slot] (summed per slot by k_slot_sums).
 template <class T>
 __device__ __forceinline__ void adjoint_pass_body(cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam,
                                                   const PassDesc& pd, const PhaseDesc* __restrict__ phases,
@@ -240,25 +240,41 @@ __global__ void __launch_bounds__(THREADS, MINB)
                          partial + part_off[blockIdx.x], pass_nslots[it.pass], smraw);
 }
 
-// grad[slot_param[s]] += 2 * sum over CTAs of partial[cta][s], slots in order
-// (single CTA of 1024 threads: deterministic).
-__global__ void k_grad_reduce(const double* __restrict__ partial, uint64_t nctas, int nslots,
-                              const int* __restrict__ slot_param, double* __restrict__ grad) {
-    __shared__ double red[32];
-    for (int s = 0; s < nslots; ++s) {
-        double v = 0.0;
-        for (uint64_t c = threadIdx.x; c < nctas; c += blockDim.x) v += partial[c * nslots + s];
+// Gradient reduction of many reverse passes at once: block s sums slot s
+// over its pass's CTAs, partial[off[s] + c * stride[s]] for c < nctas[s],
+// into sums[s]; then k_param_sums adds 2 x (the sums of each parameter's
+// slots, in slot order) to grad[param]. Both orders are fixed
+// (deterministic).
+__global__ void k_slot_sums(const double* __restrict__ partial, const uint64_t* __restrict__ off,
+                            const uint64_t* __restrict__ nctas, const uint32_t* __restrict__ stride,
+                            double* __restrict__ sums) {
+    const uint64_t s = blockIdx.x;
+    double v = 0.0;
+    for (uint64_t c = threadIdx.x; c < nctas[s]; c += blockDim.x) v += partial[off[s] + c * stride[s]];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (unsigned w = 0; w < (blockDim.x >> 5); ++w) tot += red[w];
-            grad[slot_param[s]] += 2.0 * tot;
-        }
-        __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (unsigned w = 0; w < (blockDim.x >> 5); ++w) tot += red[w];
+        sums[s] = tot;
     }
+}
+
+__global__ void k_param_sums(const double* __restrict__ sums, const int* __restrict__ slot_param, int nslots,
+                             int nparams, double* __restrict__ grad) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nparams) return;
+    double acc = 0.0;
+    bool any = false;
+    for (int s = 0; s < nslots; ++s)
+        if (slot_param[s] == p) {
+            acc += sums[s];
+            any = true;
+        }
+    if (any) grad[p] += 2.0 * acc;
 }
 
 template <class T>

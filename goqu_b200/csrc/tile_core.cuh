@@ -575,9 +575,55 @@ GQ_HD void run_phase(cplx<T>* sm, const PhaseDesc& ph, const KOp* ops, const cpl
 
 // ---- adjoint differentiation ----------------------------------------------
 
+
 template <class T>
 GQ_HD double cdot_re(cplx<T> b, cplx<T> v) {  // Re(conj(b) * v) in FP64
     return (double)b.x * (double)v.x + (double)b.y * (double)v.y;
+}
+
+// Gradient partials with the op's fields as arguments (the specialised dual
+// kernels pass literals; grad_partial below passes the op record's).
+template <class T>
+GQ_HD double dot_re_creg(const cplx<T> (&b)[NREG], const cplx<T> (&v)[NREG], uint32_t creg) {
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < NREG; ++j)
+        if ((j & creg) == creg) acc += cdot_re(b[j], v[j]);
+    return acc;
+}
+
+template <class T>
+GQ_HD double grad_phase_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], cplx<T> sc, uint32_t creg) {
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < NREG; ++j)
+        if ((j & creg) == creg) acc += cdot_re(b[j], cmul(sc, a[j]));
+    return acc;
+}
+
+template <class T>
+GQ_HD double grad_diag_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const cplx<T>* d, uint32_t hi,
+                         uint32_t creg, uint64_t ridx) {
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if ((j & creg) != creg) continue;
+        const uint32_t idx = hi | (uint32_t)((ridx >> (4 * j)) & 15u);
+        acc += cdot_re(b[j], cmul(ldc(d, idx), a[j]));
+    }
+    return acc;
+}
+
+template <class T>
+GQ_HD double grad_pairsum_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const cplx<T>* d, uint32_t K,
+                            uint64_t g0) {
+    uint64_t lo, hi;
+    pair_counts<T>(d, K, g0, lo, hi);
+    const cplx<T>* table = d + K;
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) acc += cdot_re(b[j], cmul(ldc(table, slot_count(lo, hi, j)), a[j]));
+    return acc;
 }
 
 // Re sum_j conj(lambda_j) (G psi)_j over the thread's amplitudes, G being the
@@ -589,33 +635,13 @@ GQ_HD double grad_partial(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], co
     if ((g0 & op.cmask) != op.cmask) return 0.0;
     const cplx<T>* m = pool + op.mat;
     const uint32_t creg = op.creg;
-    double acc = 0.0;
     switch (op.flags) {
-        case K_PHASE: {
-            const cplx<T> sc = ldc(m, 0);
-#pragma unroll
-            for (int j = 0; j < NREG; ++j)
-                if ((j & creg) == creg) acc += cdot_re(b[j], cmul(sc, a[j]));
-            return acc;
-        }
-        case K_DIAG: {
-            const uint32_t hi = (uint32_t)(pext64(g0, op.dmask) << op.nreg);
-#pragma unroll
-            for (int j = 0; j < NREG; ++j) {
-                if ((j & creg) != creg) continue;
-                const uint32_t idx = hi | (uint32_t)((op.ridx >> (4 * j)) & 15u);
-                acc += cdot_re(b[j], cmul(ldc(m, idx), a[j]));
-            }
-            return acc;
-        }
-        case K_PAIRSUM: {  // G = sum of the pairs' generators: T[c] per slot
-            uint64_t lo, hi;
-            pair_counts<T>(m, op.nreg, g0, lo, hi);
-            const cplx<T>* table = m + op.nreg;
-#pragma unroll
-            for (int j = 0; j < NREG; ++j) acc += cdot_re(b[j], cmul(ldc(table, slot_count(lo, hi, j)), a[j]));
-            return acc;
-        }
+        case K_PHASE:
+            return grad_phase_c<T>(a, b, ldc(m, 0), creg);
+        case K_DIAG:
+            return grad_diag_c<T>(a, b, m, (uint32_t)(pext64(g0, op.dmask) << op.nreg), creg, op.ridx);
+        case K_PAIRSUM:  // G = sum of the pairs' generators: T[c] per slot
+            return grad_pairsum_c<T>(a, b, m, op.nreg, g0);
         default: {
             // dense G on the target register bits: apply it to a copy of psi
             // (the amplitudes whose controls are unset keep psi's values and

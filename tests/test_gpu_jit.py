@@ -86,3 +86,57 @@ def test_density_matrix_matches_oracle():
     st = dm.stats()
     assert st["jit_passes"] == st["passes"] >= 1
     np.testing.assert_allclose(dm.DensityMatrix().reshape(-1), want, atol=1e-12, rtol=0)
+
+
+@pytest.mark.parametrize("n,layers", [(9, 3), (12, 2), (20, 2)])
+def test_specialised_reverse_passes_match_interpreted(n, layers):
+    # the adjoint's reverse sweep on specialised dual kernels (GQ_OPT_JIT = 2,
+    # every size) against the interpreted one (GQ_OPT_JIT = 0) and parameter shift
+    from goqu_b200 import gradient
+    c, names = workloads.hardware_efficient_ansatz(n, layers)
+    h = workloads.ising_hamiltonian(n)
+    x = np.random.default_rng(n).uniform(0, 2 * np.pi, len(names))
+    ev_j = gradient.AdjointEvaluator(c, h, names)
+    ev_j.sim.set_option(_abi.GQ_OPT_JIT, 2)
+    ev_j.sim.set_option(_abi.GQ_OPT_JIT_MIN_QUBITS, 0)
+    ev_i = gradient.AdjointEvaluator(c, h, names)
+    ev_i.sim.set_option(_abi.GQ_OPT_JIT, 0)
+    e_j, g_j = ev_j(x)
+    st = ev_j.sim.stats()
+    assert st["jit_passes"] == st["passes"]  # forward and reverse passes all specialised
+    e_i, g_i = ev_i(x)
+    assert ev_i.sim.stats()["jit_passes"] == 0
+    assert abs(e_j - e_i) < 1e-12
+    np.testing.assert_allclose(g_j, g_i, atol=1e-11, rtol=0)
+    if n <= 12:
+        ps = gradient.ParameterShift(gradient.CostFunc(c, h, names))(x)
+        np.testing.assert_allclose(g_j, ps, atol=1e-9, rtol=0)
+
+
+def test_specialised_reverse_passes_general_gates():
+    # U3 / CP / RXX / RYY / RZZ / CCX and expressions: dense, diagonal, phase
+    # and controlled gradient generators on the dual kernels, complex128 and complex64
+    from goqu_b200 import circuit as ir, gradient, param as prm, pauli as P
+    th = prm.NewVector("t", 6)
+    b = ir.Builder("g", 10)
+    for q in range(10):
+        b.H(q)
+    b.SymU3(th.At(0), prm.Mul(2.0, th.At(1)), th.At(2), 3).SymCP(th.At(3), 0, 9).SymRXX(th.At(4), 1, 2)
+    b.SymRZZ(th.At(0), 2, 8).SymRX(prm.Neg(th.At(1)), 7).CNOT(3, 0).SymRY(th.At(5), 5).CCX(1, 2, 6)
+    b.SymPhase(th.At(2), 4).SymRZ(th.At(4), 9).SymRYY(th.At(3), 4, 5)
+    c = b.Build()
+    names = ir.FreeParameters(c)
+    h = P.NewPauliSum([P.NewPauliString(0.7, {0: P.Z, 3: P.X}, 10), P.NewPauliString(-0.4, {1: P.Y, 2: P.Y}, 10),
+                       P.NewPauliString(0.25, {9: P.X, 6: P.Z}, 10)])
+    x = np.random.default_rng(3).uniform(0, 2 * np.pi, len(names))
+    for prec, tol in ((_abi.GQ_C128, 1e-11), (_abi.GQ_C64, 1e-4)):
+        ev_j = gradient.AdjointEvaluator(c, h, names, prec)
+        ev_j.sim.set_option(_abi.GQ_OPT_JIT, 2)
+        ev_j.sim.set_option(_abi.GQ_OPT_JIT_MIN_QUBITS, 0)
+        ev_i = gradient.AdjointEvaluator(c, h, names, prec)
+        ev_i.sim.set_option(_abi.GQ_OPT_JIT, 0)
+        e_j, g_j = ev_j(x)
+        e_i, g_i = ev_i(x)
+        assert ev_j.sim.stats()["jit_passes"] == ev_j.sim.stats()["passes"]
+        assert abs(e_j - e_i) < tol
+        np.testing.assert_allclose(g_j, g_i, atol=tol, rtol=0)

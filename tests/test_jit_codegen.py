@@ -131,3 +131,85 @@ def test_generated_code_density_matrix(emu, tmp_path):
     c, nm = workloads.noisy_brickwork(5, layers=3, seed=1)
     ops = encode.density_ops(c, nm)
     np.testing.assert_allclose(jit_emulate(emu, ops, 5, tmp_path, dm=1), orc.dm_evolve(ops), atol=1e-12, rtol=0)
+
+
+# ---- specialised reverse (adjoint) passes, host form -------------------------
+
+def _adjoint(emu, circuit, names, x, h, tmp_path=None, tile=0):
+    from goqu_b200 import pauli as P
+    stream = encode.statevector_ops(circuit, {nm: float(x[i]) for i, nm in enumerate(names)}, names)
+    terms = P.to_terms(h)
+    grad = np.zeros(len(names))
+    energy = ctypes.c_double()
+    common = [circuit.NumQubits(), stream.ptr(), len(stream), ctypes.cast(terms, ctypes.POINTER(_abi.gq_pauli_term)),
+              len(terms), len(names), tile, 0, grad.ctypes.data_as(_D), ctypes.byref(energy)]
+    base = [ctypes.c_int, ctypes.POINTER(_abi.gq_op), ctypes.c_size_t, ctypes.POINTER(_abi.gq_pauli_term),
+            ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, _D, _D]
+    if tmp_path is None:
+        emu.gqx_emulate_adjoint.restype = ctypes.c_int
+        emu.gqx_emulate_adjoint.argtypes = base
+        rc = emu.gqx_emulate_adjoint(*common)
+        jitted = None
+    else:
+        emu.gqx_jit_emulate_adjoint.restype = ctypes.c_int
+        emu.gqx_jit_emulate_adjoint.argtypes = base + [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
+        j = ctypes.c_int64()
+        rc = emu.gqx_jit_emulate_adjoint(*common, CSRC, str(tmp_path).encode(), ctypes.byref(j))
+        jitted = j.value
+    assert rc == 0, emu.gqx_last_error().decode()
+    return energy.value, grad, jitted
+
+
+def _general_circuit():
+    from goqu_b200 import circuit as ir, param as prm, pauli as P
+    th = prm.NewVector("t", 6)
+    b = ir.Builder("g", 9)
+    for q in range(9):
+        b.H(q)
+    b.SymU3(th.At(0), prm.Mul(2.0, th.At(1)), th.At(2), 3).SymCP(th.At(3), 0, 8).SymRXX(th.At(4), 1, 2)
+    b.SymRZZ(th.At(0), 2, 7).SymRX(prm.Neg(th.At(1)), 6).CNOT(3, 0).SymRY(th.At(5), 5).CCX(1, 2, 6)
+    b.SymPhase(th.At(2), 4).SymRZ(th.At(4), 8).SymRYY(th.At(3), 4, 5)
+    c = b.Build()
+    h = P.NewPauliSum([P.NewPauliString(0.7, {0: P.Z, 3: P.X}, 9), P.NewPauliString(-0.4, {1: P.Y, 2: P.Y}, 9),
+                       P.NewPauliString(0.25, {8: P.X, 6: P.Z}, 9)])
+    from goqu_b200 import circuit as ir2
+    return c, ir2.FreeParameters(c), h
+
+
+@pytest.mark.parametrize("which,tile", [("hea6", 0), ("hea9", 6), ("general", 0), ("general", 5), ("qaoa", 0)])
+def test_generated_dual_passes_match_interpreted_adjoint(emu, tmp_path, which, tile):
+    if which.startswith("hea"):
+        n = int(which[3:])
+        c, names = workloads.hardware_efficient_ansatz(n, 3)
+        h = workloads.ising_hamiltonian(n)
+    elif which == "general":
+        c, names, h = _general_circuit()
+    else:
+        c, names, h, x0 = workloads.qaoa_batch(1, seed=8, n_values=(10,))[0]
+    x = np.random.default_rng(4).uniform(0, 2 * np.pi, len(names))
+    e0, g0, _ = _adjoint(emu, c, names, x, h, tile=tile)
+    e1, g1, jitted = _adjoint(emu, c, names, x, h, tmp_path, tile=tile)
+    assert jitted >= 1
+    assert abs(e0 - e1) < 1e-13
+    np.testing.assert_allclose(g1, g0, atol=1e-12, rtol=0)
+
+
+@pytest.mark.parametrize("precision", [_abi.GQ_C128, _abi.GQ_C64])
+def test_dual_kernels_compile(emu, precision):
+    # device text of the dual kernels (hardware-efficient ansatz; QAOA with
+    # pair sums) compiles with NVRTC for sm_100a
+    emu.gqx_jit_check_dual.restype = ctypes.c_int
+    emu.gqx_jit_check_dual.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_abi.gq_op), ctypes.c_size_t,
+                                       ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    c, names = workloads.hardware_efficient_ansatz(12, 3)
+    qc, qn, _, _ = workloads.qaoa_batch(1, seed=3, n_values=(12,))[0]
+    for circ, nm in ((c, names), (qc, qn)):
+        xv = np.random.default_rng(1).uniform(0, 6.2, len(nm))
+        ops = encode.statevector_ops(circ, {k: float(xv[i]) for i, k in enumerate(nm)}, nm)
+        out = (ctypes.c_int64 * 3)()
+        rc = emu.gqx_jit_check_dual(circ.NumQubits(), precision, ops.ptr(), len(ops), len(nm), 2, out)
+        if rc == _abi.GQ_EUNSUPPORTED:
+            pytest.skip("libnvrtc not available")
+        assert rc == 0, emu.gqx_last_error().decode()[:3000]
+        passes, planned, compiled = list(out)
+        assert planned == passes >= 1 and compiled >= 1
