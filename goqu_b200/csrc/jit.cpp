@@ -205,6 +205,8 @@ const CachedPlan* jit_cached_plan(const Program& pr, size_t pi, bool c64, int th
             }
         }
     }
+    if (!dual)  // which one-qubit chains the forward kernel fuses
+        for (const ChainCand& cc : jit_chains(pr, pi)) put(key, (int)cc.fusable);
     PlanCache& pc = plan_cache();
     std::lock_guard<std::mutex> lk(pc.mu);
     auto it = pc.map.find(key);

@@ -34,19 +34,33 @@
 namespace gq {
 
 // A factor value: pool[ref] (kind 0), or for the one-qubit unitary at
-// ops[ref]: e^{i lambda} (1), g cos(theta/2) (2), g cos(theta/2) e^{i phi} (3).
+// ops[ref]: e^{i lambda} (1), g cos(theta/2) (2), g cos(theta/2) e^{i phi} (3);
+// kinds 4-6 are the same three for the product of chain ref / 4 under the
+// predicate values ref % 4 (JitChain).
 struct JitAtom {
     uint8_t kind;
     uint32_t ref;
 };
 
 // One parameter-block entry: `count` pool values from pool[ref] (kind 0), the
-// shear t of the one-qubit unitary ops[ref] (kind 1, real part), or the
-// product of atoms `num` divided by the product of atoms `den` (kind 2).
+// shear t of the one-qubit unitary ops[ref] (kind 1, real part), the product
+// of atoms `num` divided by the product of atoms `den` (kind 2), or the shear
+// t of chain ref / 4 under predicate values ref % 4 (kind 3).
 struct JitEntry {
     uint8_t kind;
     uint32_t ref, count;
     std::vector<uint32_t> num, den;
+};
+
+// A chain of one-qubit ops on one register bit inside a phase: uncontrolled
+// one-qubit unitaries and X-type ops, each X either unconditional (pred -1)
+// or controlled by CTA-uniform predicate `pred` (0 or 1, local to the chain).
+// No other op of the phase touches the bit between them, so the chain acts as
+// one unitary per combination of its (at most two) predicates. Ops are pass
+// relative, in order of application.
+struct JitChain {
+    std::vector<uint32_t> ops;
+    std::vector<int8_t> pred;
 };
 
 struct JitPlan {
@@ -54,8 +68,10 @@ struct JitPlan {
     std::string host_source;  // the same pass as a host function (CPU tests), when asked for
     std::vector<JitAtom> atoms;
     std::vector<JitEntry> entries;
+    std::vector<JitChain> chains;
     uint32_t n_param = 0;                             // complex entries of the parameter block (>= 1)
     std::vector<std::vector<uint32_t>> phase_shears;  // shear ops of each phase (range check)
+    std::vector<std::vector<uint32_t>> phase_chains;  // chains of each phase (range check)
 };
 
 // Kernel text for pass `pass` of `pr` at precision c64 / c128 with the given
@@ -89,6 +105,18 @@ bool jit_pack(const Program& pr, size_t pass, const JitPlan& plan, bool c64, voi
 // above. False when m is not unitary to 1e-12 or cos / sin(theta/2) is below
 // 1e-150 (the generator then keeps the dense 2x2).
 bool u1_decompose(const Z* m, double* t, Z* lam, Z* post0, Z* post1);
+
+// Candidate chains (JitChain) of pass `pass`, per phase, with the outer-qubit
+// control mask of each predicate, and whether every product of the chain
+// decomposes into the shear form with the program's current numbers. A chain
+// holds at least two one-qubit unitaries.
+struct ChainCand {
+    int phase;
+    JitChain chain;
+    uint64_t pmask[2];
+    bool fusable;
+};
+std::vector<ChainCand> jit_chains(const Program& pr, size_t pass);
 
 // A pass's plan as cached per process, keyed by the pass's structure (launch
 // shape, tile and phase tables, op kinds, bits, controls, relative pool

@@ -53,6 +53,7 @@ void emit_deposit(std::string& s, const char* ind, const char* dst, const char* 
 }
 
 Z zmul(Z a, Z b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+Z zadd(Z a, Z b) { return {a.re + b.re, a.im + b.im}; }
 Z zdiv(Z a, Z b) {
     const double d = b.re * b.re + b.im * b.im;
     return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
@@ -99,21 +100,66 @@ struct Gen {
         return add_entry("C" + num(ref) + ":" + num(count), JitEntry{0, ref, count, {}, {}});
     }
     uint32_t shear_t(uint32_t op) { return add_entry("T" + num(op), JitEntry{1, op, 1, {}, {}}); }
-    // Offset of prod(num) / prod(den) after cancelling common atoms; -1 if 1.
-    long ratio(const Pend& n0, const Pend& d0) {
-        Pend n, d;
+    // Offset of the 2^nl shear values of chain `fid` (one per predicate combination).
+    uint32_t chain_t(uint32_t fid, int nl) {
+        const std::string key = "F" + num(fid);
+        auto it = entry_ids.find(key);
+        if (it != entry_ids.end()) return it->second;
+        const uint32_t n = 1u << nl;
+        if (np + n > cap) {
+            overflow = true;
+            return 0;
+        }
+        const uint32_t off = np;
+        for (uint32_t e = 0; e < n; ++e) out.entries.push_back(JitEntry{3, fid * 4 + e, 1, {}, {}});
+        np += n;
+        entry_ids[key] = off;
+        return off;
+    }
+    // prod(n0) / prod(d0) with common atoms cancelled, and its dedupe key.
+    static std::string reduce(const Pend& n0, const Pend& d0, Pend& n, Pend& d) {
+        n.clear();
+        d.clear();
         std::set_difference(n0.begin(), n0.end(), d0.begin(), d0.end(), std::back_inserter(n));
         std::set_difference(d0.begin(), d0.end(), n0.begin(), n0.end(), std::back_inserter(d));
-        if (n.empty() && d.empty()) return -1;
-        std::string key = "P";
+        std::string key;
         for (uint32_t a : n) key += num(a) + ",";
         key += "/";
         for (uint32_t a : d) key += num(a) + ",";
-        return add_entry(key, JitEntry{2, 0, 1, n, d});
+        return key;
+    }
+    // Offset of prod(num) / prod(den) after cancelling common atoms; -1 if 1.
+    long ratio(const Pend& n0, const Pend& d0) {
+        Pend n, d;
+        const std::string key = reduce(n0, d0, n, d);
+        if (n.empty() && d.empty()) return -1;
+        return add_entry("P" + key, JitEntry{2, 0, 1, n, d});
+    }
+    // Offset of a block of consecutive ratios prod(nums[e]) / prod(dens[e]).
+    uint32_t ratio_table(const std::vector<Pend>& nums, const std::vector<Pend>& dens) {
+        std::vector<Pend> ns(nums.size()), ds(nums.size());
+        std::string key = "Q";
+        for (size_t e = 0; e < nums.size(); ++e) key += reduce(nums[e], dens[e], ns[e], ds[e]) + ";";
+        auto it = entry_ids.find(key);
+        if (it != entry_ids.end()) return it->second;
+        if (np + nums.size() > cap) {
+            overflow = true;
+            return 0;
+        }
+        const uint32_t off = np;
+        for (size_t e = 0; e < nums.size(); ++e) out.entries.push_back(JitEntry{2, 0, 1, ns[e], ds[e]});
+        np += (uint32_t)nums.size();
+        entry_ids[key] = off;
+        return off;
     }
 };
 
 void pend_add(Pend& p, uint32_t a) { p.insert(std::upper_bound(p.begin(), p.end(), a), a); }
+
+// A register slot's pending factor as a function of the phase's uniform
+// predicates: entry c holds the atoms that apply when predicate k holds for
+// exactly the bits k set in c.
+using PendT = std::vector<Pend>;
 
 }  // namespace
 
@@ -143,17 +189,151 @@ void jit_bases(const Program& pr, size_t pi, uint32_t* op_base, uint32_t* pool_b
     *pool_base = ob < pr.ops.size() ? pr.ops[ob].mat : 0;
 }
 
-bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, bool persistent, JitPlan& out,
-              bool host) {
+namespace {
+
+// Register bits an op reads or mixes in any way (targets, controls, the
+// register part of a diagonal's table index).
+uint32_t op_reg_bits(const KOp& op) {
+    uint32_t b = op.creg;
+    const uint8_t kind = op.type == K_GRAD ? op.flags : op.type;
+    switch (kind) {
+        case K_U1: case K_X: b |= 1u << op.t0; break;
+        case K_U2: case K_SWAP: b |= (1u << op.t0) | (1u << op.t1); break;
+        case K_U3: b |= (1u << op.t0) | (1u << op.t1) | (1u << op.t2); break;
+        case K_U4: case K_PAIRSUM: b = 15u; break;
+        case K_RESET: b = 15u; break;  // nonlinear: commutes with no unitary on any register bit
+        case K_DIAG:
+            for (int k = 0; k < RQ; ++k)
+                for (int j = 0; j < NREG; ++j)
+                    if (((op.ridx >> (4 * j)) & 15u) != ((op.ridx >> (4 * (j ^ (1 << k)))) & 15u)) b |= 1u << k;
+            break;
+        default: break;
+    }
+    return b;
+}
+
+// The product of a chain's ops (row major) when its predicates take the
+// values of the bits of e.
+void chain_matrix(const Program& pr, uint32_t op_base, const JitChain& ch, int e, Z* out) {
+    Z m[4] = {{1, 0}, {0, 0}, {0, 0}, {1, 0}};
+    for (size_t i = 0; i < ch.ops.size(); ++i) {
+        const KOp& op = pr.ops[op_base + ch.ops[i]];
+        Z f[4];
+        if (op.type == K_U1) {
+            for (int k = 0; k < 4; ++k) f[k] = pr.pool[op.mat + k];
+        } else {
+            if (ch.pred[i] >= 0 && !((e >> ch.pred[i]) & 1)) continue;
+            const bool pure = op.flags & 1;
+            f[0] = f[3] = Z{0, 0};
+            f[1] = pure ? Z{1, 0} : pr.pool[op.mat];
+            f[2] = pure ? Z{1, 0} : pr.pool[op.mat + 1];
+        }
+        const Z r[4] = {zadd(zmul(f[0], m[0]), zmul(f[1], m[2])), zadd(zmul(f[0], m[1]), zmul(f[1], m[3])),
+                        zadd(zmul(f[2], m[0]), zmul(f[3], m[2])), zadd(zmul(f[2], m[1]), zmul(f[3], m[3]))};
+        for (int k = 0; k < 4; ++k) m[k] = r[k];
+    }
+    for (int k = 0; k < 4; ++k) out[k] = m[k];
+}
+
+}  // namespace
+
+std::vector<ChainCand> jit_chains(const Program& pr, size_t pi) {
+    const PassDesc& pd = pr.passes[pi];
+    uint32_t op_base, pool_base;
+    jit_bases(pr, pi, &op_base, &pool_base);
+    uint64_t outer = 0;
+    for (int k = 0; k < pd.n_outer; ++k) outer |= 1ull << pd.outer_q[k];
+    std::vector<ChainCand> res;
+    for (int p = 0; p < pd.n_phases; ++p) {
+        const PhaseDesc& ph = pr.phases[pd.phase0 + p];
+        for (int r = 0; r < RQ; ++r) {
+            auto element = [&](const KOp& op) {
+                if (op.t0 != r || op.creg) return false;
+                if (op.type == K_U1) return op.cmask == 0;
+                return op.type == K_X && (op.cmask & ~outer) == 0;
+            };
+            std::vector<int> run;
+            auto finish = [&]() {
+                int first = -1, last = -1, nu = 0;
+                for (size_t i = 0; i < run.size(); ++i)
+                    if (pr.ops[run[i]].type == K_U1) {
+                        if (first < 0) first = (int)i;
+                        last = (int)i;
+                        ++nu;
+                    }
+                if (nu >= 2) {
+                    ChainCand cc;
+                    cc.phase = p;
+                    cc.pmask[0] = cc.pmask[1] = 0;
+                    int np = 0;
+                    bool ok = true;
+                    for (int i = first; i <= last; ++i) {
+                        const KOp& op = pr.ops[run[i]];
+                        int8_t pv = -1;
+                        if (op.cmask) {
+                            int k = 0;
+                            while (k < np && cc.pmask[k] != op.cmask) ++k;
+                            if (k == np) {
+                                if (np == 2) {
+                                    ok = false;
+                                    break;
+                                }
+                                cc.pmask[np++] = op.cmask;
+                            }
+                            pv = (int8_t)k;
+                        }
+                        cc.chain.ops.push_back((uint32_t)run[i] - op_base);
+                        cc.chain.pred.push_back(pv);
+                    }
+                    if (ok) {
+                        cc.fusable = true;
+                        for (int e = 0; e < (1 << np) && cc.fusable; ++e) {
+                            Z mm[4], l, a0, a1;
+                            double t;
+                            chain_matrix(pr, op_base, cc.chain, e, mm);
+                            cc.fusable = u1_decompose(mm, &t, &l, &a0, &a1);
+                        }
+                        res.push_back(cc);
+                    }
+                }
+                run.clear();
+            };
+            for (int o = ph.op_begin; o < ph.op_end; ++o) {
+                const KOp& op = pr.ops[o];
+                if (!(op_reg_bits(op) & (1u << r))) continue;
+                if (element(op)) {
+                    run.push_back(o);
+                } else {
+                    finish();
+                }
+            }
+            finish();
+        }
+    }
+    return res;
+}
+
+namespace {
+
+enum PlanResult { PLAN_OK = 0, PLAN_UNCOVERED = 1, PLAN_OVERFLOW = 2 };
+
+// jit_plan with at most `kmax` uniform predicates per phase.
+PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, bool persistent,
+                        JitPlan& out, bool host, int kmax) {
     const PassDesc& pd = pr.passes[pi];
     uint32_t op_base, pool_base;
     jit_bases(pr, pi, &op_base, &pool_base);
     const int m = pd.m, tbits = m - RQ;
-    if (tbits < 0 || (1 << tbits) != threads) return false;
+    if (tbits < 0 || (1 << tbits) != threads) return PLAN_UNCOVERED;
     out.atoms.clear();
     out.entries.clear();
     out.phase_shears.clear();
+    out.chains.clear();
+    out.phase_chains.clear();
     Gen gen(pr, out, c64 ? 3900u : 1950u);  // 32 KB of kernel parameters
+    uint64_t outer_mask = 0;
+    for (int k = 0; k < pd.n_outer; ++k) outer_mask |= 1ull << pd.outer_q[k];
+    const std::vector<ChainCand> cands = jit_chains(pr, pi);
 
     // ---- prologue: CTA base, staging columns (thread bits = tile bits [0, tbits))
     auto make_pro = [&](const char* ctav) {
@@ -197,7 +377,7 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
         for (int k = 0; k < tbits; ++k) {
             const uint32_t sv = k < 4 ? ph.tlo_slot[1u << k] : ph.thi_slot[1u << (k - 4)];
             const uint64_t g = k < 4 ? ph.tlo_glob[1u << k] : ph.thi_glob[1u << (k - 4)];
-            if (g == 0 || (g & (g - 1))) return false;
+            if (g == 0 || (g & (g - 1))) return PLAN_UNCOVERED;
             tslot[k] = sv;
             tq[k] = ctz64(g);
         }
@@ -209,18 +389,103 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                     sv ^= tslot[k];
                     g |= 1ull << tq[k];
                 }
-            if (sv != ph.tlo_slot[v] || g != ph.tlo_glob[v]) return false;
+            if (sv != ph.tlo_slot[v] || g != ph.tlo_glob[v]) return PLAN_UNCOVERED;
         }
+        // Uniform predicates: controls of X-type and phase ops that lie in the
+        // CTA's outer bits hold for a whole CTA. Such an op costs no arithmetic:
+        // the X swaps registers under a CTA-uniform branch, and both become
+        // predicate-dependent pending factors, read from a table indexed by
+        // the predicates' values when they are applied.
+        std::vector<uint64_t> upred;
+        for (int oa = ph.op_begin; oa < ph.op_end && (int)upred.size() < kmax; ++oa) {
+            const KOp& op = pr.ops[oa];
+            if (op.type != K_X || !op.cmask || (op.cmask & ~outer_mask)) continue;
+            if (std::find(upred.begin(), upred.end(), op.cmask) == upred.end()) upred.push_back(op.cmask);
+        }
+        const int K = (int)upred.size(), NC = 1 << K;
+        auto upred_of = [&](uint64_t cmask) {
+            for (int k = 0; k < K; ++k)
+                if (upred[k] == cmask) return k;
+            return -1;
+        };
+        // Chains fused into one unitary per predicate combination, applied
+        // at the chain's last op; its other ops are skipped.
+        out.phase_chains.emplace_back();
+        struct Fused {
+            uint32_t fid;
+            int nl, ubit[2];
+        };
+        std::map<int, Fused> fused_at;
+        std::vector<char> skip(ph.op_end - ph.op_begin, 0);
+        for (const ChainCand& cc : cands) {
+            if (cc.phase != p || !cc.fusable) continue;
+            Fused f;
+            f.nl = 0;
+            bool ok = true;
+            for (int k = 0; k < 2 && cc.pmask[k]; ++k) {
+                f.ubit[k] = upred_of(cc.pmask[k]);
+                ok = ok && f.ubit[k] >= 0;
+                ++f.nl;
+            }
+            if (!ok) continue;
+            f.fid = (uint32_t)out.chains.size();
+            out.chains.push_back(cc.chain);
+            out.phase_chains.back().push_back(f.fid);
+            for (size_t i = 0; i + 1 < cc.chain.ops.size(); ++i) skip[op_base + cc.chain.ops[i] - ph.op_begin] = 1;
+            fused_at[(int)(op_base + cc.chain.ops.back())] = f;
+        }
+
         std::string b = "    {\n        uint32_t sb = 0;\n        uint64_t g0 = base;\n";
         for (int k = 0; k < tbits; ++k)
             b += "        sb ^= (0u - ((t >> " + num(k) + ") & 1u)) & " + hex32(tslot[k]) + ";\n";
         emit_deposit(b, "        ", "g0", "t", tq, tbits);
-        b += "        (void)g0;\n        cplx<T> a[16];\n";
+        b += "        (void)g0;\n";
+        if (K > 0) {
+            b += "        const uint32_t pc = 0u";
+            for (int k = 0; k < K; ++k)
+                b += " | (((base & " + hex64(upred[k]) + ") == " + hex64(upred[k]) + ") ? " + hex32(1u << k) + " : 0u)";
+            b += ";\n";
+        }
+        b += "        cplx<T> a[16];\n";
         for (int j = 0; j < NREG; ++j) b += "        a[" + num(j) + "] = sm[sb ^ " + hex32(ph.rslot[j]) + "];\n";
 
-        Pend pend[NREG];
-        auto scale = [&](int j, long off) {
-            if (off >= 0) b += "        a[" + num(j) + "] = cmul(p.m[" + num(off) + "], a[" + num(j) + "]);\n";
+        PendT pend[NREG];
+        for (int j = 0; j < NREG; ++j) pend[j].assign(NC, Pend());
+        auto add_all = [&](int j, uint32_t atom) {
+            for (Pend& e : pend[j]) pend_add(e, atom);
+        };
+        // Multiplies a[j] by num[c] / den[c] for the current predicate values c.
+        auto scale_by = [&](int j, const PendT& nm, const PendT& dn) {
+            uint32_t dep = 0;  // predicates the ratio depends on
+            Pend n0, d0, n1, d1;
+            std::vector<std::string> keys(NC);
+            for (int c = 0; c < NC; ++c) keys[c] = Gen::reduce(nm[c], dn[c], n0, d0);
+            for (int c = 0; c < NC; ++c)
+                for (int k = 0; k < K; ++k)
+                    if (keys[c] != keys[c ^ (1 << k)]) dep |= 1u << k;
+            if (dep == 0) {
+                const long off = gen.ratio(nm[0], dn[0]);
+                if (off >= 0) b += "        a[" + num(j) + "] = cmul(p.m[" + num(off) + "], a[" + num(j) + "]);\n";
+                return;
+            }
+            std::vector<int> bits;
+            for (int k = 0; k < K; ++k)
+                if ((dep >> k) & 1) bits.push_back(k);
+            PendT tn, td;
+            for (int e = 0; e < (1 << (int)bits.size()); ++e) {
+                int c = 0;
+                for (size_t i = 0; i < bits.size(); ++i)
+                    if ((e >> i) & 1) c |= 1 << bits[i];
+                tn.push_back(nm[c]);
+                td.push_back(dn[c]);
+            }
+            const uint32_t off = gen.ratio_table(tn, td);
+            std::string idx;
+            for (size_t i = 0; i < bits.size(); ++i) {
+                if (i) idx += " | ";
+                idx += "(((pc >> " + num(bits[i]) + ") & 1u) << " + num((long long)i) + ")";
+            }
+            b += "        a[" + num(j) + "] = cmul(p.m[" + num(off) + " + (" + idx + ")], a[" + num(j) + "]);\n";
         };
         // Groups of an op on target bits `tm` under register controls `creg`.
         auto groups = [&](uint32_t tm, uint32_t creg) {
@@ -237,19 +502,36 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
         auto normalize = [&](const std::vector<int>& g) {
             for (size_t i = 1; i < g.size(); ++i)
                 if (pend[g[i]] != pend[g[0]]) {
-                    scale(g[i], gen.ratio(pend[g[i]], pend[g[0]]));
+                    scale_by(g[i], pend[g[i]], pend[g[0]]);
                     pend[g[i]] = pend[g[0]];
                 }
         };
+        // Other phases with run-time controls accumulate per register-control
+        // pattern M into a per-thread factor rq<M> (one complex multiply per
+        // thread and op), applied to the slots of M before an op that mixes
+        // them with other slots, and at the end of the phase.
+        uint32_t racc = 0, rdecl = 0;  // bit M: rq<M> pending / declared
+        auto flush = [&](uint32_t mixed) {
+            for (uint32_t M = 0; M < NREG; ++M) {
+                if (!((racc >> M) & 1u) || ((M & mixed) == 0 && mixed != 0xffffffffu)) continue;
+                for (int j = 0; j < NREG; ++j)
+                    if ((j & (int)M) == (int)M)
+                        b += "        a[" + num(j) + "] = cmul(rq" + num(M) + ", a[" + num(j) + "]);\n";
+                racc &= ~(1u << M);
+            }
+        };
         auto resolve = [&](int j) {
-            if (pend[j].empty()) return;
-            scale(j, gen.ratio(pend[j], {}));
-            pend[j].clear();
+            bool any = false;
+            for (const Pend& e : pend[j]) any = any || !e.empty();
+            if (!any) return;
+            scale_by(j, pend[j], PendT(NC));
+            pend[j].assign(NC, Pend());
         };
 
         for (int oa = ph.op_begin; oa < ph.op_end; ++oa) {
             const KOp& op = pr.ops[oa];
-            if (op.type == K_GRAD || op.type == K_NONE || op.type > K_RESET) return false;
+            if (op.type == K_GRAD || op.type == K_NONE || op.type > K_RESET) return PLAN_UNCOVERED;
+            if (skip[oa - ph.op_begin]) continue;
             // indices relative to the pass (its first op and first pool entry),
             // so the kernel text and plan do not depend on the pass's position
             const uint32_t o = (uint32_t)oa - op_base, rm = op.mat - pool_base;
@@ -257,27 +539,62 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
             const std::string C = op.creg ? "true" : "false";
             std::string cond;
             if (op.cmask) cond = "if ((g0 & " + hex64(op.cmask) + ") == " + hex64(op.cmask) + ") ";
+            const int uk = op.cmask ? upred_of(op.cmask) : -1;
             const std::string S0 = num(op.t0), S1 = num(op.t1), S2 = num(op.t2);
             auto pm = [&](uint32_t off) { return "PMat<T>{p.m + " + num(off) + "}"; };
+            switch (op.type) {  // register bits the op mixes
+                case K_U1: case K_X: flush(1u << op.t0); break;
+                case K_U2: case K_SWAP: flush((1u << op.t0) | (1u << op.t1)); break;
+                case K_U3: flush((1u << op.t0) | (1u << op.t1) | (1u << op.t2)); break;
+                case K_U4: case K_RESET: flush(0xffffffffu); break;
+                default: break;
+            }
             switch (op.type) {
                 case K_U1: {
                     const uint32_t tm = 1u << op.t0;
                     double tv;
                     Z lam, p0, p1;
-                    if (!op.cmask && u1_decompose(&pr.pool[op.mat], &tv, &lam, &p0, &p1)) {
+                    const auto fu = fused_at.find(oa);
+                    if (fu != fused_at.end()) {
+                        // the chain's product under this CTA's predicate values:
+                        // atoms and shear read at index e (the chain's predicates)
+                        const Fused& f = fu->second;
+                        auto local = [&](int c) {
+                            int e = 0;
+                            for (int k = 0; k < f.nl; ++k) e |= ((c >> f.ubit[k]) & 1) << k;
+                            return (uint32_t)e;
+                        };
+                        const auto gs = groups(tm, 0u);
+                        for (const auto& g : gs) {
+                            for (int c = 0; c < NC; ++c) pend_add(pend[g[1]][c], gen.atom(4, f.fid * 4 + local(c)));
+                            normalize(g);
+                        }
+                        std::string idx = "0u";
+                        for (int k = 0; k < f.nl; ++k)
+                            idx += " | (((pc >> " + num(f.ubit[k]) + ") & 1u) << " + num(k) + ")";
+                        b += "        k_shear<T, " + S0 + ", false>(a, p.m[" + num(gen.chain_t(f.fid, f.nl)) + " + (" +
+                             idx + ")].x, 0u);\n";
+                        for (const auto& g : gs) {
+                            pend[g[1]] = pend[g[0]];
+                            for (int c = 0; c < NC; ++c) {
+                                pend_add(pend[g[1]][c], gen.atom(6, f.fid * 4 + local(c)));
+                                pend_add(pend[g[0]][c], gen.atom(5, f.fid * 4 + local(c)));
+                            }
+                        }
+                    } else if (!op.cmask && u1_decompose(&pr.pool[op.mat], &tv, &lam, &p0, &p1)) {
                         const uint32_t a_l = gen.atom(1, (uint32_t)o), a_0 = gen.atom(2, (uint32_t)o),
                                        a_1 = gen.atom(3, (uint32_t)o);
                         const auto gs = groups(tm, op.creg);
                         for (const auto& g : gs) {
-                            pend_add(pend[g[1]], a_l);
+                            add_all(g[1], a_l);
                             normalize(g);
                         }
                         b += "        k_shear<T, " + S0 + ", " + C + ">(a, p.m[" + num(gen.shear_t((uint32_t)o)) +
                              "].x, " + creg + ");\n";
                         for (const auto& g : gs) {
                             pend[g[1]] = pend[g[0]];
-                            pend_add(pend[g[1]], a_1);
-                            pend_add(pend[g[0]], a_0);
+                            add_all(g[1], a_1);
+                            add_all(g[0], a_0);
                         }
                         out.phase_shears.back().push_back((uint32_t)o);
                     } else {
@@ -305,21 +622,25 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                 case K_X: {
                     const uint32_t tm = 1u << op.t0;
                     const bool pure = op.flags & 1;
-                    if (op.cmask) {
+                    if (op.cmask && uk < 0) {
                         for (const auto& g : groups(tm, op.creg)) normalize(g);
                         b += "        " + cond + "k_x<T, " + S0 + ", " + C + ">(a, " +
                              (pure ? std::string("pool") : pm(gen.copy(rm, 2))) + ", " + creg + ", " +
                              (pure ? "true" : "false") + ");\n";
                     } else {
-                        // a compile-time permutation; the phases p0, p1 become pending factors
-                        b += "        k_x<T, " + S0 + ", " + C + ">(a, pool, " + creg + ", true);\n";
-                        for (const auto& g : groups(tm, op.creg)) {
-                            std::swap(pend[g[0]], pend[g[1]]);
-                            if (!pure) {
-                                pend_add(pend[g[0]], gen.atom(0, rm));
-                                pend_add(pend[g[1]], gen.atom(0, rm + 1));
+                        // a permutation (for a uniform predicate, under a CTA-uniform
+                        // branch); the phases p0, p1 become pending factors
+                        b += "        " + std::string(uk >= 0 ? "if ((pc >> " + num(uk) + ") & 1u) " : "") + "k_x<T, " +
+                             S0 + ", " + C + ">(a, pool, " + creg + ", true);\n";
+                        for (const auto& g : groups(tm, op.creg))
+                            for (int c = 0; c < NC; ++c) {
+                                if (uk >= 0 && !((c >> uk) & 1)) continue;
+                                std::swap(pend[g[0]][c], pend[g[1]][c]);
+                                if (!pure) {
+                                    pend_add(pend[g[0]][c], gen.atom(0, rm));
+                                    pend_add(pend[g[1]][c], gen.atom(0, rm + 1));
+                                }
                             }
-                        }
                     }
                     break;
                 }
@@ -338,13 +659,23 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                     break;
                 }
                 case K_PHASE:
-                    if (op.cmask) {
-                        b += "        " + cond + "k_phase<T>(a, p.m[" + num(gen.copy(rm, 1)) + "], " + creg +
-                             ");\n";
+                    if (op.cmask && uk < 0) {
+                        const uint32_t M = op.creg;
+                        const std::string rv = "rq" + num(M), v = "p.m[" + num(gen.copy(rm, 1)) + "]";
+                        if ((racc >> M) & 1u) {
+                            b += "        " + cond + rv + " = cmul(" + v + ", " + rv + ");\n";
+                        } else {
+                            b += "        " + std::string((rdecl >> M) & 1u ? "" : "cplx<T> ") + rv +
+                                 " = cplx<T>{T(1), T(0)};\n        " + cond + rv + " = " + v + ";\n";
+                            racc |= 1u << M;
+                            rdecl |= 1u << M;
+                        }
                     } else {
                         const uint32_t a_s = gen.atom(0, rm);
                         for (int j = 0; j < NREG; ++j)
-                            if ((j & op.creg) == op.creg) pend_add(pend[j], a_s);
+                            if ((j & op.creg) == op.creg)
+                                for (int c = 0; c < NC; ++c)
+                                    if (uk < 0 || ((c >> uk) & 1)) pend_add(pend[j][c], a_s);
                     }
                     break;
                 case K_DIAG:
@@ -358,8 +689,7 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                         b += "        " + cond + h + "\n";
                     } else {
                         for (int j = 0; j < NREG; ++j)
-                            if ((j & op.creg) == op.creg)
-                                pend_add(pend[j], gen.atom(0, rm + (uint32_t)((op.ridx >> (4 * j)) & 15u)));
+                            if ((j & op.creg) == op.creg) add_all(j, gen.atom(0, rm + (uint32_t)((op.ridx >> (4 * j)) & 15u)));
                     }
                     break;
                 case K_RESET:
@@ -367,12 +697,13 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
                     b += "        " + cond + "k_reset<T, " + S0 + ">(a);\n";
                     break;
                 default:
-                    return false;
+                    return PLAN_UNCOVERED;
             }
-            if (gen.overflow) return false;
+            if (gen.overflow) return PLAN_OVERFLOW;
         }
+        flush(0xffffffffu);
         for (int j = 0; j < NREG; ++j) resolve(j);
-        if (gen.overflow) return false;
+        if (gen.overflow) return PLAN_OVERFLOW;
         for (int j = 0; j < NREG; ++j) b += "        sm[sb ^ " + hex32(ph.rslot[j]) + "] = a[" + num(j) + "];\n";
         b += "    }\n";
         seg_ph.push_back(b);
@@ -444,7 +775,20 @@ bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_block
         loop(seg_out);
         h += "    }\n}\n";
     }
-    return true;
+    return PLAN_OK;
+}
+
+}  // namespace
+
+bool jit_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, bool persistent, JitPlan& out,
+              bool host) {
+    // predicate tables grow the parameter block: fewer predicates per phase
+    // when it does not fit
+    for (int kmax : {4, 2, 0}) {
+        const PlanResult r = plan_forward(pr, pi, c64, threads, min_blocks, persistent, out, host, kmax);
+        if (r != PLAN_OVERFLOW) return r == PLAN_OK;
+    }
+    return false;
 }
 
 bool jit_plan_dual(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, JitPlan& out, bool host) {
@@ -699,10 +1043,34 @@ bool jit_pack(const Program& pr, size_t pi, const JitPlan& plan, bool c64, void*
         have[o] = 1;
         return true;
     };
+    // chain products under each predicate combination
+    struct ChainDec {
+        double t;
+        Z lam, p0, p1;
+        bool have = false;
+    };
+    std::vector<ChainDec> cd(plan.chains.size() * 4);
+    auto cdec = [&](uint32_t ref) -> const ChainDec* {
+        if (ref / 4 >= plan.chains.size()) return nullptr;
+        ChainDec& d = cd[ref];
+        if (!d.have) {
+            Z mm[4];
+            chain_matrix(pr, op_base, plan.chains[ref / 4], (int)(ref % 4), mm);
+            if (!u1_decompose(mm, &d.t, &d.lam, &d.p0, &d.p1)) return nullptr;
+            d.have = true;
+        }
+        return &d;
+    };
     for (size_t i = 0; i < plan.atoms.size(); ++i) {
         const JitAtom& a = plan.atoms[i];
         if (a.kind == 0) {
             av[i] = pr.pool[pool_base + a.ref];
+            continue;
+        }
+        if (a.kind >= 4) {
+            const ChainDec* d = cdec(a.ref);
+            if (!d) return false;
+            av[i] = a.kind == 4 ? d->lam : (a.kind == 5 ? d->p0 : d->p1);
             continue;
         }
         Z lam, p0, p1;
@@ -711,9 +1079,9 @@ bool jit_pack(const Program& pr, size_t pi, const JitPlan& plan, bool c64, void*
     }
     // range check: within a phase the amplitudes grow by at most prod(1 + |t|)
     const double limit = c64 ? 60.0 : 600.0;  // log2 bound
-    for (const auto& ph : plan.phase_shears) {
+    for (size_t p = 0; p < plan.phase_shears.size(); ++p) {
         double lg = 0;
-        for (uint32_t o : ph) {
+        for (uint32_t o : plan.phase_shears[p]) {
             if (o >= nops) return false;
             if (!have[o]) {
                 Z l, a, b;
@@ -721,6 +1089,18 @@ bool jit_pack(const Program& pr, size_t pi, const JitPlan& plan, bool c64, void*
             }
             lg += std::log2(1.0 + std::fabs(tv[o]));
         }
+        if (p < plan.phase_chains.size())
+            for (uint32_t f : plan.phase_chains[p]) {
+                double tmax = 0;
+                int npred = 0;
+                for (int8_t k : plan.chains[f].pred) npred = std::max(npred, k + 1);
+                for (int e = 0; e < (1 << npred); ++e) {
+                    const ChainDec* d = cdec(f * 4 + (uint32_t)e);
+                    if (!d) return false;
+                    tmax = std::max(tmax, std::fabs(d->t));
+                }
+                lg += std::log2(1.0 + tmax);
+            }
         if (lg > limit) return false;
     }
     std::vector<Z> vals;
@@ -734,6 +1114,10 @@ bool jit_pack(const Program& pr, size_t pi, const JitPlan& plan, bool c64, void*
                 if (!dec(e.ref, &l, &a, &b)) return false;
             }
             vals.push_back({tv[e.ref], 0.0});
+        } else if (e.kind == 3) {
+            const ChainDec* d = cdec(e.ref);
+            if (!d) return false;
+            vals.push_back({d->t, 0.0});
         } else {
             Z nv = {1, 0}, dv = {1, 0};
             for (uint32_t a : e.num) nv = zmul(nv, av[a]);
