@@ -502,6 +502,44 @@ int gqx_jit_emulate(int nq, int precision, double* state, const gq_op* ops, size
     return rc;
 }
 
+// What the specialised statevector kernels of `ops` use, scheduled as the
+// engine does: out = [passes, passes with a kernel text, fused one-qubit
+// chains, chain candidates, phases with CTA-uniform predicates, phases with
+// run-time phase accumulators].
+int gqx_jit_plan_stats(int nq, int precision, const gq_op* ops, size_t n_ops, int tile_qubits, int budget,
+                       int64_t* out) {
+    std::vector<gq::NGate> gates;
+    const int nphys = nq < gq::RQ ? gq::RQ : nq;
+    for (size_t i = 0; i < n_ops; ++i) {
+        const int rc = gq::normalize_op(ops[i], nphys, gates, g_err);
+        if (rc != GQ_OK) return rc;
+    }
+    gq::SchedOptions opt;
+    opt.tile_qubits = tile_qubits > 0 ? tile_qubits : 11;
+    opt.budget = budget > 0 ? budget : 320;
+    opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
+    opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    gq::Program prog;
+    gq::schedule(gates, nphys, opt, prog);
+    int64_t planned = 0, chains = 0, cands = 0, pred_phases = 0, acc_phases = 0;
+    for (size_t i = 0; i < prog.passes.size(); ++i) {
+        gq::JitPlan pl;
+        cands += (int64_t)gq::jit_chains(prog, i).size();
+        if (!gq::jit_plan(prog, i, precision == GQ_C64, 1 << (prog.passes[i].m - gq::RQ), 4, false, pl)) continue;
+        ++planned;
+        chains += (int64_t)pl.chains.size();
+        for (size_t at = 0; (at = pl.source.find("const uint32_t pc =", at)) != std::string::npos; ++at) ++pred_phases;
+        for (size_t at = 0; (at = pl.source.find("cplx<T> rq", at)) != std::string::npos; ++at) ++acc_phases;
+    }
+    out[0] = (int64_t)prog.passes.size();
+    out[1] = planned;
+    out[2] = chains;
+    out[3] = cands;
+    out[4] = pred_phases;
+    out[5] = acc_phases;
+    return GQ_OK;
+}
+
 // The reverse sweep of an adjoint gradient as specialised dual kernels: the
 // reverse program of `ops` scheduled as the engine does (11-qubit tiles),
 // each pass's dual kernel text compiled with NVRTC at the engine's launch

@@ -140,3 +140,37 @@ def dense_unitary_state(circuit):
         t = np.moveaxis(t, list(range(k)), axes)
         psi = t.reshape(-1)
     return psi
+
+
+def chain_circuit(n, seed, low=5):
+    """One-qubit chains on low qubits through X-type gates controlled from high
+    qubits (CTA-index bits at small tiles): CNOT, CY (phased X), H-CNOT-H
+    (a diagonal product: not fused), two controls on one target, and
+    controlled phases from high qubits (run-time accumulators)."""
+    rng = np.random.default_rng(seed)
+    b = ir.Builder("chains", n)
+    for layer in range(10):
+        for q in range(low):
+            b.U3(*rng.uniform(0, 2 * np.pi, 3), q)
+        for q in range(low):
+            c = int(rng.integers(low, n))
+            kind = (layer + q) % 5
+            if kind == 0:
+                b.CNOT(c, q)
+            elif kind == 1:
+                b.Ctrl(G.Y, [c], q)
+            elif kind == 2:
+                b.H(q)
+                b.CNOT(c, q)
+                b.H(q)
+            elif kind == 3:
+                b.CNOT(c, q)
+                b.U3(*rng.uniform(0, 2 * np.pi, 3), q)
+                b.CNOT(int(rng.integers(low, n)), q)
+            else:
+                for c2 in rng.choice(np.arange(low, n), 3, replace=False):
+                    b.MCP(rng.uniform(0, 2 * np.pi), [int(c2)], q)
+        for q in range(low, n):
+            if layer % 3 == 0:
+                b.U3(*rng.uniform(0, 2 * np.pi, 3), q)
+    return b.Build()

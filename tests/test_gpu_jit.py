@@ -11,7 +11,7 @@ import pytest
 from goqu_b200 import _abi, densitymatrix, encode, statevector, workloads
 from oracle import binding as orc
 
-from kat_util import random_circuit
+from kat_util import chain_circuit, random_circuit
 
 pytestmark = pytest.mark.gpu
 
@@ -33,6 +33,20 @@ def test_random_circuits_match_oracle(n, seed):
     st = sim.stats()
     assert st["jit_passes"] == st["passes"] >= 1
     np.testing.assert_allclose(sim.StateVector(), want, atol=1e-12, rtol=0)
+
+
+@pytest.mark.parametrize("n,seed", [(14, 21), (16, 22)])
+def test_uniform_predicates_and_chains_match_oracle(n, seed):
+    # X-type gates and phases controlled from CTA-index qubits: predicate
+    # tables, fused one-qubit chains, run-time phase accumulators
+    c = chain_circuit(n, seed, low=6)
+    want = orc.sv_evolve(encode.statevector_ops(c))
+    for prec, tol in ((_abi.GQ_C128, 1e-12), (_abi.GQ_C64, 2e-5)):
+        sim = jit_sim(n, prec)
+        sim.Evolve(c)
+        st = sim.stats()
+        assert st["jit_passes"] == st["passes"] >= 1
+        assert np.max(np.abs(sim.StateVector() - want)) < tol
 
 
 def test_complex64_matches_oracle():

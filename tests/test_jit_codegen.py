@@ -11,7 +11,7 @@ import os
 import pytest
 
 from goqu_b200 import _abi, encode, workloads
-from kat_util import random_circuit
+from kat_util import chain_circuit, random_circuit
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EMU = os.path.join(ROOT, "goqu_b200", "libgqb200_emu.so")
@@ -125,6 +125,54 @@ def test_generated_code_extreme_angles(emu, tmp_path):
             b.CNOT(q, q + 1)
     ops = encode.statevector_ops(b.Build())
     np.testing.assert_allclose(jit_emulate(emu, ops, 12, tmp_path), orc.sv_evolve(ops), atol=1e-12, rtol=0)
+
+
+def plan_stats(emu, stream, n, tile=0, precision=_abi.GQ_C128):
+    emu.gqx_jit_plan_stats.restype = ctypes.c_int
+    out = (ctypes.c_int64 * 6)()
+    rc = emu.gqx_jit_plan_stats(n, precision, stream.ptr(), len(stream), tile, 0, out)
+    assert rc == 0, emu.gqx_last_error().decode()
+    return dict(zip(["passes", "planned", "chains", "candidates", "pred_phases", "acc_decls"], list(out)))
+
+
+@pytest.mark.parametrize("n,seed,tile", [(12, 11, 7), (13, 12, 8), (14, 13, 0)])
+def test_generated_code_uniform_predicates_and_chains(emu, tmp_path, n, seed, tile):
+    # pending factors indexed by CTA-uniform predicates, fused one-qubit chains
+    # and run-time phase accumulators, each checked to be in use
+    ops = encode.statevector_ops(chain_circuit(n, seed))
+    st = plan_stats(emu, ops, n, tile)
+    assert st["planned"] == st["passes"]
+    assert st["chains"] >= 1 and st["pred_phases"] >= 1 and st["acc_decls"] >= 1, st
+    want = orc.sv_evolve(ops)
+    np.testing.assert_allclose(jit_emulate(emu, ops, n, tmp_path, tile=tile), want, atol=1e-12, rtol=0)
+    assert np.max(np.abs(jit_emulate(emu, ops, n, tmp_path, precision=_abi.GQ_C64, tile=tile) - want)) < 2e-5
+
+
+def test_generated_code_unfusable_chains(emu, tmp_path):
+    # H CNOT H with the control on a CTA-index bit: the chain's products are
+    # I and Z (diagonal), which have no shear form, so the chain stays unfused
+    from goqu_b200 import circuit as ir
+    n = 12
+    b = ir.Builder("hxh", n)
+    rng = np.random.default_rng(4)
+    for q in range(4, n):
+        b.U3(*rng.uniform(0, 2 * np.pi, 3), q)
+    for q in range(4):
+        b.H(q)
+        b.CNOT(8 + q, q)
+        b.H(q)
+    ops = encode.statevector_ops(b.Build())
+    st = plan_stats(emu, ops, n, 7)
+    assert st["planned"] == st["passes"] and st["candidates"] > st["chains"], st
+    np.testing.assert_allclose(jit_emulate(emu, ops, n, tmp_path, tile=7), orc.sv_evolve(ops), atol=1e-12, rtol=0)
+
+
+def test_layered_benchmark_uses_chains(emu):
+    # the 28-qubit benchmark's brickwork: most CNOT targets fuse with their U3s
+    c = workloads.random_layers_qft(28, layers=40, seed=2028)
+    st = plan_stats(emu, encode.statevector_ops(c), 28)
+    assert st["planned"] == st["passes"]
+    assert st["chains"] >= 400, st
 
 
 def test_generated_code_density_matrix(emu, tmp_path):
