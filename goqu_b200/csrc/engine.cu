@@ -10,8 +10,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gqb200.h"
@@ -1287,14 +1289,16 @@ int gq_dm_stats(const gq_dm* dm, gq_stats* out) {
 // sweep/run.go:27-171, and the QAOA / VQE evaluations of algorithm/*): every
 // circuit's forward and reverse programs are concatenated into one device
 // program. Wave w runs pass w of every circuit in one launch per tile size
-// (work items = state, pass, CTA), so no kernel waits on another; lambda,
+// (a descriptor per state and pass, runs of descriptors with equal CTA
+// counts), so no kernel waits on another; lambda,
 // energies and gradients are reduced per circuit in fixed order. The launch
 // sequence is captured in a CUDA graph and replayed while the circuits'
 // structure (not their angles) stays the same.
 namespace {
 
 struct BLaunch {
-    uint32_t item0, count;  // into the item array
+    uint32_t run0, nrun;  // into the run array
+    uint32_t count;       // blocks
     int m;
     bool adjoint;
     uint32_t grp0, ngrp;    // gradient groups reduced after an adjoint launch
@@ -1305,8 +1309,8 @@ struct BatchPlan {
     std::vector<int> pass_nslots;  // gradient slots per pass
     std::vector<uint32_t> slot_grad;
     std::vector<uint32_t> pass_slot0;
-    std::vector<BItem> items;
-    std::vector<uint64_t> part_off;
+    std::vector<BDesc> descs;
+    std::vector<BRun> runs;
     std::vector<BLaunch> launches;  // forward waves, then reverse waves
     size_t n_forward_launches = 0;
     std::vector<BGradGroup> ggroups;
@@ -1321,9 +1325,18 @@ struct BatchPlan {
     uint64_t signature = 0;
 };
 
+// Structure signature (graph replay): a 64-bit multiply-xorshift hash over
+// 8-byte words.
 uint64_t fnv(uint64_t h, const void* p, size_t n) {
     const unsigned char* b = (const unsigned char*)p;
-    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, b + i, 8);
+        h = (h ^ w) * 0x9E3779B97F4A7C15ull;
+        h ^= h >> 29;
+    }
+    for (; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
     return h;
 }
 
@@ -1395,20 +1408,35 @@ int set_batch_attrs() {
     return GQ_OK;
 }
 
-// Builds the concatenated program, work items and reduction tables.
+// Builds the concatenated program, launch descriptors and reduction tables.
 int build_batch_plan(int prec, const gq_batch_item* items, size_t n, bool grads, const SchedOptions& base_opt,
                      BatchPlan& P) {
     P = BatchPlan();
-    std::string err;
     std::vector<std::vector<int>> fwd_passes(n), rev_passes(n);
     std::vector<uint64_t> grad_off(n);
-    for (size_t c = 0; c < n; ++c) {
+    // Each circuit is analysed and scheduled on its own (worker threads);
+    // the results are concatenated in order below.
+    struct CircPlan {
+        Program pf, pr;
+        std::vector<DGroup> groups;  // term indices local to the circuit
+        std::vector<DTerm> terms;
+        int rc = GQ_OK;
+        std::string err;
+    };
+    std::vector<CircPlan> cp(n);
+    auto plan_one = [&](size_t c) {
+        CircPlan& q = cp[c];
         const gq_batch_item& it = items[c];
-        if (it.num_qubits < 1 || it.num_qubits > 30) return fail(GQ_EINVAL, "batch item " + std::to_string(c) + ": qubits out of range");
-        if ((it.n_ops && !it.ops) || (it.n_terms && !it.terms)) return fail(GQ_EINVAL, "batch item " + std::to_string(c) + ": null ops or terms");
+        auto bad = [&](int rc, const std::string& why) {
+            q.rc = rc;
+            q.err = "batch item " + std::to_string(c) + ": " + why;
+        };
+        if (it.num_qubits < 1 || it.num_qubits > 30) return bad(GQ_EINVAL, "qubits out of range");
+        if ((it.n_ops && !it.ops) || (it.n_terms && !it.terms)) return bad(GQ_EINVAL, "null ops or terms");
         const int nphys = std::max(it.num_qubits, RQ);
         std::vector<NGate> fwd, rev;
         std::vector<int> fo, ro;
+        std::string err;
         int rc;
         if (grads) {
             rc = adjoint_gates(it.num_qubits, it.ops, it.n_ops, it.n_params, fwd, rev, fo, ro, err);
@@ -1416,54 +1444,80 @@ int build_batch_plan(int prec, const gq_batch_item* items, size_t n, bool grads,
             rc = GQ_OK;
             for (size_t k = 0; k < it.n_ops && rc == GQ_OK; ++k) rc = normalize_op(it.ops[k], it.num_qubits, fwd, err);
         }
-        if (rc != GQ_OK) return fail(rc, "batch item " + std::to_string(c) + ": " + err);
-        grad_off[c] = P.total_params;
-        P.total_params += it.n_params;
-        P.state_off.push_back(P.total_amps);
-        P.total_amps += 1ull << nphys;
-        SchedOptions o = base_opt;
-        Program pf;
-        schedule(fwd, nphys, o, pf);
-        const size_t pb = P.prog.passes.size();
-        append_program(pf, P, grad_off[c]);
-        for (size_t i = 0; i < pf.passes.size(); ++i) fwd_passes[c].push_back((int)(pb + i));
-        if (grads) {
-            o.tile_qubits = std::min(o.tile_qubits, log2i(kAdjThreads) + RQ);
-            Program pr;
-            schedule(rev, nphys, o, pr);
-            const size_t rb = P.prog.passes.size();
-            append_program(pr, P, grad_off[c]);
-            for (size_t i = 0; i < pr.passes.size(); ++i) rev_passes[c].push_back((int)(rb + i));
-        }
+        if (rc != GQ_OK) return bad(rc, err);
         // Pauli terms of this circuit: Re(c_t) only (lambda for the gradient
         // and Re <psi|H|psi>), grouped by x mask
         const uint64_t qmask = (1ull << it.num_qubits) - 1;
         std::vector<size_t> order(it.n_terms);
         for (size_t i = 0; i < it.n_terms; ++i) {
-            if ((it.terms[i].x_mask | it.terms[i].z_mask) & ~qmask)
-                return fail(GQ_EINVAL, "batch item " + std::to_string(c) + ": Pauli term out of range");
+            if ((it.terms[i].x_mask | it.terms[i].z_mask) & ~qmask) return bad(GQ_EINVAL, "Pauli term out of range");
             order[i] = i;
+        }
+        SchedOptions o = base_opt;
+        schedule(fwd, nphys, o, q.pf);
+        if (grads) {
+            o.tile_qubits = std::min(o.tile_qubits, log2i(kAdjThreads) + RQ);
+            schedule(rev, nphys, o, q.pr);
         }
         std::stable_sort(order.begin(), order.end(),
                          [&](size_t a, size_t b) { return it.terms[a].x_mask < it.terms[b].x_mask; });
-        BCircuit bc;
-        bc.state = P.state_off[c];
-        bc.n_amps = 1ull << it.num_qubits;
-        bc.group0 = (int32_t)P.groups.size();
         for (size_t k = 0; k < it.n_terms; ++k) {
             const gq_pauli_term& t = it.terms[order[k]];
-            if (P.groups.size() == (size_t)bc.group0 || P.groups.back().x != t.x_mask)
-                P.groups.push_back({t.x_mask, (int32_t)P.terms.size(), (int32_t)P.terms.size()});
+            if (q.groups.empty() || q.groups.back().x != t.x_mask)
+                q.groups.push_back({t.x_mask, (int32_t)q.terms.size(), (int32_t)q.terms.size()});
             const int ny = __builtin_popcountll(t.x_mask & t.z_mask) & 3;
             double wr = t.coeff_re, wi = 0.0;
             if (ny == 1) wr = 0.0, wi = t.coeff_re;
             if (ny == 2) wr = -t.coeff_re;
             if (ny == 3) wr = 0.0, wi = -t.coeff_re;
-            P.terms.push_back({wr, wi, t.z_mask});
-            P.groups.back().t1 = (int32_t)P.terms.size();
+            q.terms.push_back({wr, wi, t.z_mask});
+            q.groups.back().t1 = (int32_t)q.terms.size();
         }
-        bc.ngroups = (int32_t)P.groups.size() - bc.group0;
+    };
+    {
+        unsigned nt = std::thread::hardware_concurrency();
+        nt = std::max(1u, std::min(nt == 0 ? 1u : nt, 32u));
+        if (n < 64) nt = 1;
+        std::atomic<size_t> next{0};
+        auto worker = [&]() {
+            for (size_t c; (c = next.fetch_add(1)) < n;) plan_one(c);
+        };
+        std::vector<std::thread> pool;
+        for (unsigned k = 1; k < nt; ++k) pool.emplace_back(worker);
+        worker();
+        for (std::thread& t : pool) t.join();
+    }
+    for (size_t c = 0; c < n; ++c) {
+        CircPlan& q = cp[c];
+        if (q.rc != GQ_OK) return fail(q.rc, q.err);
+        const gq_batch_item& it = items[c];
+        const int nphys = std::max(it.num_qubits, RQ);
+        grad_off[c] = P.total_params;
+        P.total_params += it.n_params;
+        P.state_off.push_back(P.total_amps);
+        P.total_amps += 1ull << nphys;
+        const size_t pb = P.prog.passes.size();
+        append_program(q.pf, P, grad_off[c]);
+        for (size_t i = 0; i < q.pf.passes.size(); ++i) fwd_passes[c].push_back((int)(pb + i));
+        if (grads) {
+            const size_t rb = P.prog.passes.size();
+            append_program(q.pr, P, grad_off[c]);
+            for (size_t i = 0; i < q.pr.passes.size(); ++i) rev_passes[c].push_back((int)(rb + i));
+        }
+        BCircuit bc;
+        bc.state = P.state_off[c];
+        bc.n_amps = 1ull << it.num_qubits;
+        bc.group0 = (int32_t)P.groups.size();
+        const int32_t t0 = (int32_t)P.terms.size();
+        for (DGroup g : q.groups) {
+            g.t0 += t0;
+            g.t1 += t0;
+            P.groups.push_back(g);
+        }
+        P.terms.insert(P.terms.end(), q.terms.begin(), q.terms.end());
+        bc.ngroups = (int32_t)q.groups.size();
         P.circ.push_back(bc);
+        q = CircPlan();  // release the circuit's program
     }
     // chunks of the lambda / energy kernel
     const uint32_t chunk_len = 4096;
@@ -1472,28 +1526,35 @@ int build_batch_plan(int prec, const gq_batch_item* items, size_t n, bool grads,
         for (uint64_t b = 0; b < P.circ[c].n_amps; b += chunk_len) P.chunks.push_back({(uint32_t)c, (uint32_t)b});
         P.chunk_seg.push_back(P.chunks.size());
     }
-    // waves
+    // waves: pass w of every circuit, one launch per tile size; inside a
+    // launch, circuits with the same CTA count form one run
     auto add_waves = [&](const std::vector<std::vector<int>>& passes, bool adjoint) {
         size_t W = 0;
         for (auto& v : passes) W = std::max(W, v.size());
+        std::vector<std::vector<size_t>> by_outer(64);
         for (size_t w = 0; w < W; ++w) {
             for (int m = RQ; m <= MAX_TILE; ++m) {
-                BLaunch L{(uint32_t)P.items.size(), 0, m, adjoint, (uint32_t)P.ggroups.size(), 0};
+                for (auto& v : by_outer) v.clear();
                 for (size_t c = 0; c < n; ++c) {
                     if (w >= passes[c].size()) continue;
-                    const int gp = passes[c][w];
-                    const PassDesc& pd = P.prog.passes[gp];
-                    if (pd.m != m) continue;
-                    const uint32_t first = (uint32_t)P.items.size();
-                    for (uint64_t cta = 0; cta < (1ull << pd.n_outer); ++cta) {
-                        P.items.push_back({P.state_off[c], (uint32_t)gp, (uint32_t)cta});
-                        P.part_off.push_back(P.total_partials);
-                        P.total_partials += P.pass_nslots[gp];
-                    }
-                    if (adjoint && P.pass_nslots[gp] > 0)
-                        P.ggroups.push_back({first, (uint32_t)P.items.size(), P.pass_slot0[gp], (uint32_t)P.pass_nslots[gp]});
+                    const PassDesc& pd = P.prog.passes[passes[c][w]];
+                    if (pd.m == m) by_outer[pd.n_outer].push_back(c);
                 }
-                L.count = (uint32_t)P.items.size() - L.item0;
+                BLaunch L{(uint32_t)P.runs.size(), 0, 0, m, adjoint, (uint32_t)P.ggroups.size(), 0};
+                for (int k = 63; k >= 0; --k) {
+                    if (by_outer[k].empty()) continue;
+                    P.runs.push_back({L.count, (uint32_t)P.descs.size(), (uint32_t)k, 0u});
+                    for (size_t c : by_outer[k]) {
+                        const int gp = passes[c][w];
+                        const uint32_t ns = (uint32_t)P.pass_nslots[gp];
+                        P.descs.push_back({P.state_off[c], P.total_partials, (uint32_t)gp, ns});
+                        if (adjoint && ns > 0)
+                            P.ggroups.push_back({P.total_partials, 1u << k, P.pass_slot0[gp], ns, 0u});
+                        P.total_partials += (uint64_t)ns << k;
+                        L.count += 1u << k;
+                    }
+                }
+                L.nrun = (uint32_t)P.runs.size() - L.run0;
                 L.ngrp = (uint32_t)P.ggroups.size() - L.grp0;
                 if (L.count) P.launches.push_back(L);
             }
@@ -1507,7 +1568,8 @@ int build_batch_plan(int prec, const gq_batch_item* items, size_t n, bool grads,
     h = fnv(h, P.prog.passes.data(), P.prog.passes.size() * sizeof(PassDesc));
     h = fnv(h, P.prog.phases.data(), P.prog.phases.size() * sizeof(PhaseDesc));
     h = fnv(h, P.prog.ops.data(), P.prog.ops.size() * sizeof(KOp));
-    h = fnv(h, P.items.data(), P.items.size() * sizeof(BItem));
+    h = fnv(h, P.descs.data(), P.descs.size() * sizeof(BDesc));
+    h = fnv(h, P.runs.data(), P.runs.size() * sizeof(BRun));
     h = fnv(h, P.groups.data(), P.groups.size() * sizeof(DGroup));
     const size_t ps = P.prog.pool.size(), nt = P.terms.size();
     h = fnv(h, &ps, sizeof(ps));
@@ -1523,9 +1585,9 @@ template <class T>
 int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* grad_out) {
     Engine& e = b->e;
     BatchPlan& P = b->plan;
-    // ---- one upload: program | items | part_off | groups... (tables)
+    // ---- one upload: program, descriptors, runs, reduction tables
     struct Off {
-        size_t pass, phase, ops, pool, items, part, nslots, ggroups, slotg, bcirc, chunks, seg, groups, terms, soff, total;
+        size_t pass, phase, ops, pool, descs, runs, ggroups, slotg, bcirc, chunks, seg, groups, terms, soff, total;
     } o{};
     size_t at = 0;
     auto put = [&](size_t bytes) {
@@ -1537,9 +1599,8 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
     o.phase = put(P.prog.phases.size() * sizeof(PhaseDesc));
     o.ops = put(P.prog.ops.size() * sizeof(KOp));
     o.pool = put(P.prog.pool.size() * sizeof(cplx<T>));
-    o.items = put(P.items.size() * sizeof(BItem));
-    o.part = put(P.part_off.size() * sizeof(uint64_t));
-    o.nslots = put(P.pass_nslots.size() * sizeof(int));
+    o.descs = put(P.descs.size() * sizeof(BDesc));
+    o.runs = put(P.runs.size() * sizeof(BRun));
     o.ggroups = put(P.ggroups.size() * sizeof(BGradGroup));
     o.slotg = put(P.slot_grad.size() * sizeof(uint32_t));
     o.bcirc = put(P.circ.size() * sizeof(BCircuit));
@@ -1562,9 +1623,8 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
         cplx<T>* pool = (cplx<T>*)(h + o.pool);
         for (size_t i = 0; i < P.prog.pool.size(); ++i) pool[i] = {(T)P.prog.pool[i].re, (T)P.prog.pool[i].im};
     }
-    cp(o.items, P.items.data(), P.items.size() * sizeof(BItem));
-    cp(o.part, P.part_off.data(), P.part_off.size() * sizeof(uint64_t));
-    cp(o.nslots, P.pass_nslots.data(), P.pass_nslots.size() * sizeof(int));
+    cp(o.descs, P.descs.data(), P.descs.size() * sizeof(BDesc));
+    cp(o.runs, P.runs.data(), P.runs.size() * sizeof(BRun));
     cp(o.ggroups, P.ggroups.data(), P.ggroups.size() * sizeof(BGradGroup));
     cp(o.slotg, P.slot_grad.data(), P.slot_grad.size() * sizeof(uint32_t));
     cp(o.bcirc, P.circ.data(), P.circ.size() * sizeof(BCircuit));
@@ -1604,18 +1664,19 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
             const unsigned threads = 1u << (L.m - RQ);
             if (!L.adjoint) {
                 BatchTile<T>::kernel<<<L.count, threads, sizeof(cplx<T>) << L.m, e.stream>>>(
-                    states, (const BItem*)(d + o.items) + L.item0, (const PassDesc*)(d + o.pass),
-                    (const PhaseDesc*)(d + o.phase), (const KOp*)(d + o.ops), (const cplx<T>*)(d + o.pool));
+                    states, (const BRun*)(d + o.runs) + L.run0, (int)L.nrun, (const BDesc*)(d + o.descs),
+                    (const PassDesc*)(d + o.pass), (const PhaseDesc*)(d + o.phase), (const KOp*)(d + o.ops),
+                    (const cplx<T>*)(d + o.pool));
                 ++launches;
             } else {
                 k_adjoint_pass_batch<T, kAdjThreads, kAdjBatchMinB<T>><<<L.count, threads, adj_smem(sizeof(cplx<T>), L.m),
                                                                          e.stream>>>(
-                    states, lams, (const BItem*)(d + o.items) + L.item0, (const uint64_t*)(d + o.part) + L.item0,
-                    (const int*)(d + o.nslots), (const PassDesc*)(d + o.pass), (const PhaseDesc*)(d + o.phase),
-                    (const KOp*)(d + o.ops), (const cplx<T>*)(d + o.pool), partial);
+                    states, lams, (const BRun*)(d + o.runs) + L.run0, (int)L.nrun, (const BDesc*)(d + o.descs),
+                    (const PassDesc*)(d + o.pass), (const PhaseDesc*)(d + o.phase), (const KOp*)(d + o.ops),
+                    (const cplx<T>*)(d + o.pool), partial);
                 ++launches;
                 if (L.ngrp) {
-                    k_grad_reduce_batch<<<L.ngrp, 256, 0, e.stream>>>(partial, (const uint64_t*)(d + o.part),
+                    k_grad_reduce_batch<<<L.ngrp, 256, 0, e.stream>>>(partial,
                                                                       (const BGradGroup*)(d + o.ggroups) + L.grp0,
                                                                       (const uint32_t*)(d + o.slotg),
                                                                       (double*)b->grads.p);
@@ -1645,7 +1706,13 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
         GQ_CUDA(cudaGetLastError());
         return GQ_OK;
     };
+    // the batch's device work alone (pass_ms): from the first launch on
+    auto mark0 = [&]() -> int {
+        if (e.timing) GQ_CUDA(cudaEventRecord(e.ev_pass0, e.stream));
+        return GQ_OK;
+    };
     if (replay) {
+        GQ_TRY(mark0());
         GQ_CUDA(cudaGraphLaunch(b->graph, e.stream));
         launches = b->graph_launches;  // the recorded sequence
     } else if (b->use_graph) {
@@ -1670,9 +1737,15 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
         }
         b->graph_sig = P.signature;
         b->graph_launches = launches;
+        GQ_TRY(mark0());
         GQ_CUDA(cudaGraphLaunch(b->graph, e.stream));
     } else {
+        GQ_TRY(mark0());
         GQ_TRY(record());
+    }
+    if (e.timing) {
+        GQ_CUDA(cudaEventRecord(e.ev_pass1, e.stream));
+        e.pass_timed = true;
     }
     e.stats.kernel_launches = launches;
     if (energies) GQ_CUDA(cudaMemcpyAsync(energies, b->energies.p, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));

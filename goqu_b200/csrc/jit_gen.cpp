@@ -946,6 +946,9 @@ bool jit_plan_dual(const Program& pr, size_t pi, bool c64, int threads, int min_
                     ", " + hex64(op.ridx) + ");";
             } else if (kind == K_PAIRSUM) {
                 e = "gv = grad_pairsum_c<T>(a, bb, pool + " + num(rm) + "u, " + num(op.nreg) + "u, g0);";
+            } else if (kind == K_X) {
+                const uint32_t px = gen.copy(rm, 2);
+                e = "gv = grad_x_c<T, " + S0 + ">(a, bb, p.m[" + num(px) + "], p.m[" + num(px + 1) + "], " + creg + ");";
             } else {  // dense G, applied to a copy of psi
                 e = "cplx<T> v[16]; for (int j = 0; j < 16; ++j) v[j] = a[j]; " + body("v", "sa") +
                     " gv = dot_re_creg<T>(bb, v, " + creg + ");";

@@ -107,22 +107,43 @@ __global__ void __launch_bounds__(THREADS, MINB)
     tile_pass_body<T>(st, *pdp, phases, ops, pool, blockIdx.x, reinterpret_cast<cplx<T>*>(smraw));
 }
 
-// A batch of independent states: block b runs CTA items[b].cta of pass
-// items[b].pass on the state starting at amplitude items[b].state.
-struct BItem {
-    uint64_t state;
+// A batch of independent states. A batched launch runs one pass of many
+// states: descriptor d (state, pass) takes 2^n_outer consecutive blocks.
+// Descriptors with the same CTA count form a run, so block b finds its
+// descriptor arithmetically after a scan over the launch's few runs.
+struct BDesc {
+    uint64_t state;  // first amplitude of the state
+    uint64_t part0;  // reverse passes: its gradient partials start here (cta * nslots + slot)
     uint32_t pass;
-    uint32_t cta;
+    uint32_t nslots;
 };
+struct BRun {
+    uint32_t block0;     // first block of the run in the launch
+    uint32_t desc0;      // its first descriptor
+    uint32_t log2_ctas;  // CTAs per descriptor
+    uint32_t pad;
+};
+
+__device__ __forceinline__ BDesc batch_desc(const BRun* __restrict__ runs, int nruns, const BDesc* __restrict__ descs,
+                                            uint32_t b, uint32_t& cta) {
+    int r = 0;
+    while (r + 1 < nruns && runs[r + 1].block0 <= b) ++r;
+    const BRun R = runs[r];
+    const uint32_t off = b - R.block0;
+    cta = off & ((1u << R.log2_ctas) - 1u);
+    return descs[R.desc0 + (off >> R.log2_ctas)];
+}
 
 template <class T, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB)
-    k_tile_pass_batch(cplx<T>* __restrict__ states, const BItem* __restrict__ items, const PassDesc* __restrict__ passes,
+    k_tile_pass_batch(cplx<T>* __restrict__ states, const BRun* __restrict__ runs, int nruns,
+                      const BDesc* __restrict__ descs, const PassDesc* __restrict__ passes,
                       const PhaseDesc* __restrict__ phases, const KOp* __restrict__ ops,
                       const cplx<T>* __restrict__ pool) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    const BItem it = items[blockIdx.x];
-    tile_pass_body<T>(states + it.state, passes[it.pass], phases, ops, pool, it.cta, reinterpret_cast<cplx<T>*>(smraw));
+    uint32_t cta;
+    const BDesc d = batch_desc(runs, nruns, descs, blockIdx.x, cta);
+    tile_pass_body<T>(states + d.state, passes[d.pass], phases, ops, pool, cta, reinterpret_cast<cplx<T>*>(smraw));
 }
 
 // ---------------------------------------------------------------------------
@@ -226,18 +247,19 @@ __global__ void __launch_bounds__(THREADS, MINB)
                          nslots, smraw);
 }
 
-// Batched reverse passes: item b's gradient partials go to
-// partial[part_off[b] .. + nslots of its pass].
+// Batched reverse passes: CTA c of descriptor d writes its gradient partials
+// to partial[d.part0 + c * d.nslots .. + d.nslots].
 template <class T, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB)
-    k_adjoint_pass_batch(cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam, const BItem* __restrict__ items,
-                         const uint64_t* __restrict__ part_off, const int* __restrict__ pass_nslots,
-                         const PassDesc* __restrict__ passes, const PhaseDesc* __restrict__ phases,
-                         const KOp* __restrict__ ops, const cplx<T>* __restrict__ pool, double* __restrict__ partial) {
+    k_adjoint_pass_batch(cplx<T>* __restrict__ psi, cplx<T>* __restrict__ lam, const BRun* __restrict__ runs,
+                         int nruns, const BDesc* __restrict__ descs, const PassDesc* __restrict__ passes,
+                         const PhaseDesc* __restrict__ phases, const KOp* __restrict__ ops,
+                         const cplx<T>* __restrict__ pool, double* __restrict__ partial) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    const BItem it = items[blockIdx.x];
-    adjoint_pass_body<T>(psi + it.state, lam + it.state, passes[it.pass], phases, ops, pool, it.cta,
-                         partial + part_off[blockIdx.x], pass_nslots[it.pass], smraw);
+    uint32_t cta;
+    const BDesc d = batch_desc(runs, nruns, descs, blockIdx.x, cta);
+    adjoint_pass_body<T>(psi + d.state, lam + d.state, passes[d.pass], phases, ops, pool, cta,
+                         partial + d.part0 + (uint64_t)cta * d.nslots, (int)d.nslots, smraw);
 }
 
 // Gradient reduction of many reverse passes at once: block s sums slot s
@@ -910,22 +932,23 @@ __global__ void k_segment_reduce(const double* __restrict__ partial, const uint6
     }
 }
 
-// Gradient partials of one reverse wave: group g covers items [ib, ie) of
-// one circuit's pass, each item holding nslots partials from part_off[item];
-// grad[slot_grad[slot0 + s]] += 2 * sum over the group's items.
+// Gradient partials of one reverse wave: group g is one circuit's pass, its
+// nctas CTAs holding nslots partials each from part0;
+// grad[slot_grad[slot0 + s]] += 2 * sum over the group's CTAs.
 struct BGradGroup {
-    uint32_t item_begin, item_end;
+    uint64_t part0;   // partials of one reverse pass of one state: part0 + cta * nslots + slot
+    uint32_t nctas;
     uint32_t slot0;   // into slot_grad
     uint32_t nslots;
+    uint32_t pad;
 };
-__global__ void k_grad_reduce_batch(const double* __restrict__ partial, const uint64_t* __restrict__ part_off,
-                                    const BGradGroup* __restrict__ grp, const uint32_t* __restrict__ slot_grad,
-                                    double* __restrict__ grad) {
+__global__ void k_grad_reduce_batch(const double* __restrict__ partial, const BGradGroup* __restrict__ grp,
+                                    const uint32_t* __restrict__ slot_grad, double* __restrict__ grad) {
     const BGradGroup g = grp[blockIdx.x];
     __shared__ double ws[32];
     for (uint32_t s = 0; s < g.nslots; ++s) {
         double v = 0.0;
-        for (uint32_t it = g.item_begin + threadIdx.x; it < g.item_end; it += blockDim.x) v += partial[part_off[it] + s];
+        for (uint32_t c = threadIdx.x; c < g.nctas; c += blockDim.x) v += partial[g.part0 + (uint64_t)c * g.nslots + s];
         v = warp_sum(v);
         if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
         __syncthreads();

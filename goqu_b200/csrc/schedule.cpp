@@ -1000,9 +1000,13 @@ int grad_gate(std::vector<Z> m, std::vector<int> qubits, uint64_t ctrl, int para
                 diag = false;
                 break;
             }
+    const bool xtype = t == 1 && m[0].re == 0.0 && m[0].im == 0.0 && m[3].re == 0.0 && m[3].im == 0.0;
     if (t == 0) {
         g.grad_kind = K_PHASE;
         g.data = {m[0]};
+    } else if (xtype) {  // Pauli-X generators (RX, and X-type parts): G a_0 = p0 a_1, G a_1 = p1 a_0
+        g.grad_kind = K_X;
+        g.data = {m[1], m[2]};
     } else if (diag) {
         g.grad_kind = K_DIAG;
         g.data.resize(dim);
@@ -1069,6 +1073,13 @@ int adjoint_gates(int nq, const gq_op* ops, size_t n_ops, size_t n_params, std::
         }
         for (size_t kk = before; kk < reverse.size(); ++kk) rev_op.push_back((int)ii);
     }
+    // Ops ahead of the first parameterised op (an initial H layer, say) need no
+    // un-applying: no gradient is taken below them.
+    size_t keep = 0;
+    for (size_t k = 0; k < reverse.size(); ++k)
+        if (reverse[k].type == K_GRAD) keep = k + 1;
+    reverse.resize(keep);
+    rev_op.resize(keep);
     return GQ_OK;
 }
 

@@ -614,6 +614,19 @@ GQ_HD double grad_diag_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], con
     return acc;
 }
 
+// G = [[0, p0], [p1, 0]] on register bit S (a Pauli-X generator such as
+// RX's -i/2 X): sum over the pairs of Re(conj(b_0) p0 a_1 + conj(b_1) p1 a_0).
+template <class T, int S>
+GQ_HD double grad_x_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], cplx<T> p0, cplx<T> p1, uint32_t creg) {
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if ((j & (1 << S)) || (j & creg) != creg) continue;
+        acc += cdot_re(b[j], cmul(p0, a[j | (1 << S)])) + cdot_re(b[j | (1 << S)], cmul(p1, a[j]));
+    }
+    return acc;
+}
+
 template <class T>
 GQ_HD double grad_pairsum_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const cplx<T>* d, uint32_t K,
                             uint64_t g0) {
@@ -642,6 +655,15 @@ GQ_HD double grad_partial(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], co
             return grad_diag_c<T>(a, b, m, (uint32_t)(pext64(g0, op.dmask) << op.nreg), creg, op.ridx);
         case K_PAIRSUM:  // G = sum of the pairs' generators: T[c] per slot
             return grad_pairsum_c<T>(a, b, m, op.nreg, g0);
+        case K_X: {
+            const cplx<T> p0 = ldc(m, 0), p1 = ldc(m, 1);
+            switch (op.t0) {
+                case 0: return grad_x_c<T, 0>(a, b, p0, p1, creg);
+                case 1: return grad_x_c<T, 1>(a, b, p0, p1, creg);
+                case 2: return grad_x_c<T, 2>(a, b, p0, p1, creg);
+                default: return grad_x_c<T, 3>(a, b, p0, p1, creg);
+            }
+        }
         default: {
             // dense G on the target register bits: apply it to a copy of psi
             // (the amplitudes whose controls are unset keep psi's values and
@@ -696,7 +718,7 @@ GQ_HD void run_phase_dual(cplx<T>* sm_a, cplx<T>* sm_b, const PhaseDesc& ph, con
     for (int o = ob; o < oe; ++o) {
         const KOp& op = ops[o];
         if (op.type == K_GRAD) {
-            const double v = (op.flags == K_PHASE || op.flags == K_DIAG || op.flags == K_PAIRSUM)
+            const double v = (op.flags == K_PHASE || op.flags == K_DIAG || op.flags == K_PAIRSUM || op.flags == K_X)
                                  ? grad_partial<T>(a, b, op, pool, g0)
                                  : grad_partial_dense<T>(a, b, op, pool, g0, sm_a, sbase, ph.rslot);
             grad(op.slot, v);

@@ -165,7 +165,8 @@ int gq_sv_expect_z_mask(gq_sv* sv, uint64_t mask, double* out);
  * circuit `ops` applied to |0...0> (new: goqu only has ParameterShift and
  * FiniteDifference, algorithm/gradient/gradient.go:49-86). grad_out has
  * n_params entries; op parameters use gq_op.param_index / dmatrix.
- * The handle's state holds psi(theta) afterwards.                            */
+ * The reverse sweep runs on the handle's state in place and stops at the
+ * first parameterised op: evolve again before reading the state.            */
 int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops,
                            const gq_pauli_term* terms, size_t n_terms,
                            size_t n_params, double* grad_out, double* energy_out);
@@ -252,7 +253,10 @@ int gq_dm_set_option(gq_dm* dm, int key, int64_t value);
  * algorithm/vqe: every item is a circuit applied to |0...0> with a Pauli sum;
  * gq_batch_run returns Re <psi|H|psi> per item and, with want_gradients, the
  * adjoint gradient of each item (n_params entries per item, concatenated in
- * item order). All items run in one sequence of batched launches.          */
+ * item order). All items run in one sequence of batched launches; the items
+ * are analysed and scheduled on the host's threads first. Stats: last_ms
+ * covers the whole call (host planning, upload, launches, results), pass_ms
+ * the batched launches alone.                                               */
 typedef struct gq_batch gq_batch;
 typedef struct gq_batch_item {
     int32_t num_qubits;
