@@ -96,6 +96,7 @@ class gq_stats(ctypes.Structure):
         ("d2h_bytes", ctypes.c_int64),
         ("jit_passes", ctypes.c_int64),
         ("jit_compile_ms", ctypes.c_double),
+        ("host_ms", ctypes.c_double),
     ]
 
 

@@ -426,11 +426,13 @@ GQ_HD void k_pairsum(cplx<T> (&a)[NREG], const cplx<T>* d, uint32_t K, uint64_t 
     for (int j = 0; j < NREG; ++j) a[j] = cmul(ldc(table, slot_count(lo, hi, j)), a[j]);
 }
 
-// Applies one op to the thread's 16 amplitudes. g0 is the global index of the
-// thread's register slot 0 (its thread bits and the CTA's base).
-template <class T>
-GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint64_t g0, cplx<T>* sm,
-                    uint32_t sbase, const uint32_t* rslot) {
+// Decodes one op and hands its body to `each`: each(body) calls body(a, sm)
+// with a thread's 16 amplitudes and its shared-memory tile (U4's scratch).
+// g0 is the global index of the thread's register slot 0 (its thread bits
+// and the CTA's base).
+template <class T, class Each>
+GQ_HD void dispatch_op(const KOp& op, const cplx<T>* pool, uint64_t g0, uint32_t sbase, const uint32_t* rslot,
+                       Each each) {
     if ((g0 & op.cmask) != op.cmask) return;
     const cplx<T>* m = pool + op.mat;
     const uint32_t creg = op.creg;
@@ -438,101 +440,108 @@ GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint
         case K_U1:
             if (creg == 0) {
                 switch (op.t0) {
-                    case 0: k_u1<T, 0, false>(a, m, 0); break;
-                    case 1: k_u1<T, 1, false>(a, m, 0); break;
-                    case 2: k_u1<T, 2, false>(a, m, 0); break;
-                    default: k_u1<T, 3, false>(a, m, 0); break;
+                    case 0: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u1<T, 0, false>(x, m, 0); }); break;
+                    case 1: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u1<T, 1, false>(x, m, 0); }); break;
+                    case 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u1<T, 2, false>(x, m, 0); }); break;
+                    default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u1<T, 3, false>(x, m, 0); }); break;
                 }
             } else {
                 switch (op.t0) {
-                    case 0: k_u1<T, 0, true>(a, m, creg); break;
-                    case 1: k_u1<T, 1, true>(a, m, creg); break;
-                    case 2: k_u1<T, 2, true>(a, m, creg); break;
-                    default: k_u1<T, 3, true>(a, m, creg); break;
+                    case 0: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u1<T, 0, true>(x, m, creg); }); break;
+                    case 1: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u1<T, 1, true>(x, m, creg); }); break;
+                    case 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u1<T, 2, true>(x, m, creg); }); break;
+                    default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u1<T, 3, true>(x, m, creg); }); break;
                 }
             }
             break;
         case K_U2:
             if (creg == 0) {
                 switch (op.t0 * 4 + op.t1) {
-                    case 1: k_u2<T, 0, 1, false>(a, m, 0); break;
-                    case 2: k_u2<T, 0, 2, false>(a, m, 0); break;
-                    case 3: k_u2<T, 0, 3, false>(a, m, 0); break;
-                    case 6: k_u2<T, 1, 2, false>(a, m, 0); break;
-                    case 7: k_u2<T, 1, 3, false>(a, m, 0); break;
-                    default: k_u2<T, 2, 3, false>(a, m, 0); break;
+                    case 1: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 0, 1, false>(x, m, 0); }); break;
+                    case 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 0, 2, false>(x, m, 0); }); break;
+                    case 3: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 0, 3, false>(x, m, 0); }); break;
+                    case 6: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 1, 2, false>(x, m, 0); }); break;
+                    case 7: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 1, 3, false>(x, m, 0); }); break;
+                    default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 2, 3, false>(x, m, 0); }); break;
                 }
             } else {
                 switch (op.t0 * 4 + op.t1) {
-                    case 1: k_u2<T, 0, 1, true>(a, m, creg); break;
-                    case 2: k_u2<T, 0, 2, true>(a, m, creg); break;
-                    case 3: k_u2<T, 0, 3, true>(a, m, creg); break;
-                    case 6: k_u2<T, 1, 2, true>(a, m, creg); break;
-                    case 7: k_u2<T, 1, 3, true>(a, m, creg); break;
-                    default: k_u2<T, 2, 3, true>(a, m, creg); break;
+                    case 1: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 0, 1, true>(x, m, creg); }); break;
+                    case 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 0, 2, true>(x, m, creg); }); break;
+                    case 3: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 0, 3, true>(x, m, creg); }); break;
+                    case 6: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 1, 2, true>(x, m, creg); }); break;
+                    case 7: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 1, 3, true>(x, m, creg); }); break;
+                    default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u2<T, 2, 3, true>(x, m, creg); }); break;
                 }
             }
             break;
         case K_U3:
             switch (op.t0 * 16 + op.t1 * 4 + op.t2) {
-                case 0 * 16 + 1 * 4 + 2: k_u3<T, 0, 1, 2>(a, m, creg); break;
-                case 0 * 16 + 1 * 4 + 3: k_u3<T, 0, 1, 3>(a, m, creg); break;
-                case 0 * 16 + 2 * 4 + 3: k_u3<T, 0, 2, 3>(a, m, creg); break;
-                default: k_u3<T, 1, 2, 3>(a, m, creg); break;
+                case 0 * 16 + 1 * 4 + 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u3<T, 0, 1, 2>(x, m, creg); }); break;
+                case 0 * 16 + 1 * 4 + 3: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u3<T, 0, 1, 3>(x, m, creg); }); break;
+                case 0 * 16 + 2 * 4 + 3: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u3<T, 0, 2, 3>(x, m, creg); }); break;
+                default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_u3<T, 1, 2, 3>(x, m, creg); }); break;
             }
             break;
         case K_U4:
-            k_u4<T>(a, m, sm, sbase, rslot);
+            each([&](cplx<T>(&x)[NREG], cplx<T>* xs) { k_u4<T>(x, m, xs, sbase, rslot); });
             break;
         case K_X: {
             const bool pure = op.flags & 1;
             if (creg == 0) {
                 switch (op.t0) {
-                    case 0: k_x<T, 0, false>(a, m, 0, pure); break;
-                    case 1: k_x<T, 1, false>(a, m, 0, pure); break;
-                    case 2: k_x<T, 2, false>(a, m, 0, pure); break;
-                    default: k_x<T, 3, false>(a, m, 0, pure); break;
+                    case 0: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_x<T, 0, false>(x, m, 0, pure); }); break;
+                    case 1: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_x<T, 1, false>(x, m, 0, pure); }); break;
+                    case 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_x<T, 2, false>(x, m, 0, pure); }); break;
+                    default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_x<T, 3, false>(x, m, 0, pure); }); break;
                 }
             } else {
                 switch (op.t0) {
-                    case 0: k_x<T, 0, true>(a, m, creg, pure); break;
-                    case 1: k_x<T, 1, true>(a, m, creg, pure); break;
-                    case 2: k_x<T, 2, true>(a, m, creg, pure); break;
-                    default: k_x<T, 3, true>(a, m, creg, pure); break;
+                    case 0: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_x<T, 0, true>(x, m, creg, pure); }); break;
+                    case 1: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_x<T, 1, true>(x, m, creg, pure); }); break;
+                    case 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_x<T, 2, true>(x, m, creg, pure); }); break;
+                    default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_x<T, 3, true>(x, m, creg, pure); }); break;
                 }
             }
             break;
         }
         case K_SWAP:
             switch (op.t0 * 4 + op.t1) {
-                case 1: k_swap<T, 0, 1>(a, creg); break;
-                case 2: k_swap<T, 0, 2>(a, creg); break;
-                case 3: k_swap<T, 0, 3>(a, creg); break;
-                case 6: k_swap<T, 1, 2>(a, creg); break;
-                case 7: k_swap<T, 1, 3>(a, creg); break;
-                default: k_swap<T, 2, 3>(a, creg); break;
+                case 1: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_swap<T, 0, 1>(x, creg); }); break;
+                case 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_swap<T, 0, 2>(x, creg); }); break;
+                case 3: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_swap<T, 0, 3>(x, creg); }); break;
+                case 6: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_swap<T, 1, 2>(x, creg); }); break;
+                case 7: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_swap<T, 1, 3>(x, creg); }); break;
+                default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_swap<T, 2, 3>(x, creg); }); break;
             }
             break;
         case K_DIAG:
-            k_diag<T>(a, op, m, g0);
+            each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_diag<T>(x, op, m, g0); });
             break;
         case K_PHASE:
-            k_phase<T>(a, ldc(m, 0), creg);
+            each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_phase<T>(x, ldc(m, 0), creg); });
             break;
         case K_PAIRSUM:
-            k_pairsum<T>(a, m, op.nreg, g0);
+            each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_pairsum<T>(x, m, op.nreg, g0); });
             break;
         case K_RESET:
             switch (op.t0) {
-                case 0: k_reset<T, 0>(a); break;
-                case 1: k_reset<T, 1>(a); break;
-                case 2: k_reset<T, 2>(a); break;
-                default: k_reset<T, 3>(a); break;
+                case 0: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_reset<T, 0>(x); }); break;
+                case 1: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_reset<T, 1>(x); }); break;
+                case 2: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_reset<T, 2>(x); }); break;
+                default: each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_reset<T, 3>(x); }); break;
             }
             break;
         default:
             break;
     }
+}
+
+// Applies one op to the thread's 16 amplitudes.
+template <class T>
+GQ_HD void apply_op(cplx<T> (&a)[NREG], const KOp& op, const cplx<T>* pool, uint64_t g0, cplx<T>* sm,
+                    uint32_t sbase, const uint32_t* rslot) {
+    dispatch_op<T>(op, pool, g0, sbase, rslot, [&](auto body) { body(a, sm); });
 }
 
 // Global index base of a CTA: bit k of the CTA index goes to outer_q[k].
@@ -724,8 +733,9 @@ GQ_HD void run_phase_dual(cplx<T>* sm_a, cplx<T>* sm_b, const PhaseDesc& ph, con
             grad(op.slot, v);
             continue;
         }
-        // U4 spills through the thread's own slots: keep the two states'
-        // slots apart by applying to psi and lambda with their own tiles.
+        // Each state decodes the op on its own: one decode for both holds
+        // both states' operands live at once and measured slower (register
+        // pressure). U4 spills through the thread's own slots of each tile.
         apply_op<T>(a, op, pool, g0, sm_a, sbase, ph.rslot);
         apply_op<T>(b, op, pool, g0, sm_b, sbase, ph.rslot);
     }

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define GQ_ABI_VERSION 2
+#define GQ_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------ */
 #define GQ_OK 0
@@ -117,6 +117,8 @@ typedef struct gq_stats {
     int64_t d2h_bytes;       /* device->host bytes the last call copied (results)   */
     int64_t jit_passes;      /* passes of the last call run by a specialised kernel */
     double jit_compile_ms;   /* process total: milliseconds spent compiling them    */
+    double host_ms;          /* batches: host time of the last call before its first
+                                launch (analysis, scheduling, table packing, upload) */
 } gq_stats;
 
 /* ---- library ------------------------------------------------------------- */
