@@ -883,16 +883,32 @@ __global__ void k_apply_terms_batch(const cplx<T>* __restrict__ psi_all, cplx<T>
     const cplx<T>* psi = psi_all + c.state;
     cplx<T>* lam = lam_all + c.state;
     const uint64_t end = (uint64_t)ch.begin + chunk_len < c.n_amps ? (uint64_t)ch.begin + chunk_len : c.n_amps;
+    // The circuit's groups and terms, read by every amplitude, are staged in
+    // shared memory once per block when they fit (global loads of them
+    // otherwise throttle the load pipe).
+    constexpr int kSharedGroups = 64, kSharedTerms = 384;
+    __shared__ DGroup sgr[kSharedGroups];
+    __shared__ DTerm stm[kSharedTerms];
+    const int t_lo = c.ngroups ? groups[c.group0].t0 : 0;
+    const int t_hi = c.ngroups ? groups[c.group0 + c.ngroups - 1].t1 : 0;
+    const bool staged = c.ngroups <= kSharedGroups && t_hi - t_lo <= kSharedTerms;
+    if (staged) {
+        for (int k = threadIdx.x; k < c.ngroups; k += blockDim.x) sgr[k] = groups[c.group0 + k];
+        for (int k = threadIdx.x; k < t_hi - t_lo; k += blockDim.x) stm[k] = terms[t_lo + k];
+    }
+    __syncthreads();
+    const DGroup* gp = staged ? sgr : groups + c.group0;
+    const DTerm* tp = staged ? stm : terms + t_lo;
     double e = 0.0;
     for (uint64_t i = ch.begin + threadIdx.x; i < end; i += blockDim.x) {
         double lr = 0.0, li = 0.0;
-        for (int g = c.group0; g < c.group0 + c.ngroups; ++g) {
-            const DGroup gr = groups[g];
+        for (int g = 0; g < c.ngroups; ++g) {
+            const DGroup gr = gp[g];
             const uint64_t j = i ^ gr.x;
             const cplx<T> v = psi[j];
             double fr = 0.0, fi = 0.0;
-            for (int k = gr.t0; k < gr.t1; ++k) {
-                const DTerm tm = terms[k];
+            for (int k = gr.t0 - t_lo; k < gr.t1 - t_lo; ++k) {
+                const DTerm tm = tp[k];
                 const double sg = (__popcll(j & tm.z) & 1) ? -1.0 : 1.0;
                 fr += sg * tm.wre;
                 fi += sg * tm.wim;

@@ -528,6 +528,12 @@ std::vector<NGate> fuse_pairsums(const std::vector<NGate>& in, uint64_t R, const
             }
             (h.type == K_GRAD ? grads : units).push_back(f);
         }
+        // A unitary pair sum right after the gradient pair sum of the same
+        // pairs reuses the pair counts (flag `pure` here, KOp.flags bit 1).
+        if (!grads.empty() && !units.empty() && grads.back().type == K_GRAD &&
+            grads.back().grad_kind == K_PAIRSUM && units.front().type == K_PAIRSUM &&
+            units.front().targets == grads.back().targets)
+            units.front().pure = true;
         out.insert(out.end(), grads.begin(), grads.end());
         out.insert(out.end(), units.begin(), units.end());
         i = j;
@@ -768,6 +774,7 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                     prog.pool.insert(prog.pool.end(), g.data.begin(), g.data.end());
                 } else if (kind == K_PAIRSUM) {
                     op.nreg = (uint8_t)((g.data.size() - 1) / 2);
+                    op.flags = g.pure ? 2 : 0;  // counts of the preceding gradient pair sum
                     prog.pool.insert(prog.pool.end(), g.data.begin(), g.data.end());
                 } else if (kind == K_SWAP) {
                     int a = kbit(g.targets[0]), b = kbit(g.targets[1]);

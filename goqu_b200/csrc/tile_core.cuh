@@ -13,6 +13,7 @@
 // FMAs and is compiled both for sm_100a and for the host emulator.
 #pragma once
 #if !defined(__CUDACC_RTC__)
+#include <math.h>
 #include <stdint.h>
 #endif
 
@@ -417,13 +418,18 @@ GQ_HD uint32_t slot_count(uint64_t lo, uint64_t hi, int j) {
     return (uint32_t)(((j < 8 ? lo : hi) >> (8 * (j & 7))) & 0xffull);
 }
 
+// The pair sum's factor T[c] per slot, given its counts.
+template <class T>
+GQ_HD void k_pairsum_lh(cplx<T> (&a)[NREG], const cplx<T>* table, uint64_t lo, uint64_t hi) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) a[j] = cmul(ldc(table, slot_count(lo, hi, j)), a[j]);
+}
+
 template <class T>
 GQ_HD void k_pairsum(cplx<T> (&a)[NREG], const cplx<T>* d, uint32_t K, uint64_t g0) {
     uint64_t lo, hi;
     pair_counts<T>(d, K, g0, lo, hi);
-    const cplx<T>* table = d + K;
-#pragma unroll
-    for (int j = 0; j < NREG; ++j) a[j] = cmul(ldc(table, slot_count(lo, hi, j)), a[j]);
+    k_pairsum_lh<T>(a, d + K, lo, hi);
 }
 
 // Decodes one op and hands its body to `each`: each(body) calls body(a, sm)
@@ -589,6 +595,10 @@ template <class T>
 GQ_HD double cdot_re(cplx<T> b, cplx<T> v) {  // Re(conj(b) * v) in FP64
     return (double)b.x * (double)v.x + (double)b.y * (double)v.y;
 }
+// complex64: the product of two FP32 amplitudes is formed in FP32 (one fused
+// multiply-add, the precision of the amplitudes) and the sums over
+// amplitudes accumulate in FP64.
+GQ_HD double cdot_re(cplx<float> b, cplx<float> v) { return (double)fmaf(b.x, v.x, b.y * v.y); }
 
 // Gradient partials with the op's fields as arguments (the specialised dual
 // kernels pass literals; grad_partial below passes the op record's).
@@ -637,15 +647,20 @@ GQ_HD double grad_x_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], cplx<T
 }
 
 template <class T>
-GQ_HD double grad_pairsum_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const cplx<T>* d, uint32_t K,
-                            uint64_t g0) {
-    uint64_t lo, hi;
-    pair_counts<T>(d, K, g0, lo, hi);
-    const cplx<T>* table = d + K;
+GQ_HD double grad_pairsum_lh(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const cplx<T>* table, uint64_t lo,
+                             uint64_t hi) {
     double acc = 0.0;
 #pragma unroll
     for (int j = 0; j < NREG; ++j) acc += cdot_re(b[j], cmul(ldc(table, slot_count(lo, hi, j)), a[j]));
     return acc;
+}
+
+template <class T>
+GQ_HD double grad_pairsum_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const cplx<T>* d, uint32_t K,
+                            uint64_t g0) {
+    uint64_t lo, hi;
+    pair_counts<T>(d, K, g0, lo, hi);
+    return grad_pairsum_lh<T>(a, b, d + K, lo, hi);
 }
 
 // Re sum_j conj(lambda_j) (G psi)_j over the thread's amplitudes, G being the
@@ -724,15 +739,35 @@ GQ_HD void run_phase_dual(cplx<T>* sm_a, cplx<T>* sm_b, const PhaseDesc& ph, con
     load_regs(a, sm_a, sbase, ph.rslot);
     load_regs(b, sm_b, sbase, ph.rslot);
     const int ob = ph.op_begin, oe = ph.op_end;
+    // Pair sums: counts computed once for both states, and once for a
+    // gradient pair sum and the unitary one after it (KOp.flags bit 1).
+    uint64_t plo = 0, phi = 0;
+    bool pcount = false;
     for (int o = ob; o < oe; ++o) {
         const KOp& op = ops[o];
         if (op.type == K_GRAD) {
-            const double v = (op.flags == K_PHASE || op.flags == K_DIAG || op.flags == K_PAIRSUM || op.flags == K_X)
-                                 ? grad_partial<T>(a, b, op, pool, g0)
-                                 : grad_partial_dense<T>(a, b, op, pool, g0, sm_a, sbase, ph.rslot);
+            double v;
+            if (op.flags == K_PAIRSUM) {
+                pair_counts<T>(pool + op.mat, op.nreg, g0, plo, phi);
+                pcount = true;
+                v = grad_pairsum_lh<T>(a, b, pool + op.mat + op.nreg, plo, phi);
+            } else {
+                pcount = false;
+                v = (op.flags == K_PHASE || op.flags == K_DIAG || op.flags == K_X)
+                        ? grad_partial<T>(a, b, op, pool, g0)
+                        : grad_partial_dense<T>(a, b, op, pool, g0, sm_a, sbase, ph.rslot);
+            }
             grad(op.slot, v);
             continue;
         }
+        if (op.type == K_PAIRSUM) {
+            if (!((op.flags & 2) && pcount)) pair_counts<T>(pool + op.mat, op.nreg, g0, plo, phi);
+            pcount = true;
+            k_pairsum_lh<T>(a, pool + op.mat + op.nreg, plo, phi);
+            k_pairsum_lh<T>(b, pool + op.mat + op.nreg, plo, phi);
+            continue;
+        }
+        pcount = false;
         // Each state decodes the op on its own: one decode for both holds
         // both states' operands live at once and measured slower (register
         // pressure). U4 spills through the thread's own slots of each tile.
