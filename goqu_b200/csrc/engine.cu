@@ -1360,12 +1360,21 @@ uint64_t fnv_par(uint64_t h, const void* p, size_t n) {
 
 struct gq_batch {
     Engine e;
-    BatchPlan plan;
-    cudaGraphExec_t graph = nullptr;
-    uint64_t graph_sig = 0;
-    int64_t graph_launches = 0;
+    BatchPlan plan;  // of the segment being planned
+    // per segment: captured launch sequence, its structure signature and the
+    // buffer generation its pointers belong to
+    std::vector<cudaGraphExec_t> graphs;
+    std::vector<uint64_t> graph_sig, graph_gen;
+    std::vector<int64_t> graph_launches;
+    uint64_t buf_gen = 0;  // bumped when a device buffer is reallocated
     bool use_graph = true;
     DevBuf states, lams, partials, energies, grads, tables;
+    // two host staging buffers: segment k packs into one while the upload of
+    // segment k - 1 may still read the other
+    PinnedBuf stage[2];
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    bool staged_pending[2] = {false, false};
+    PinnedBuf results;  // energies and gradients of all segments (pinned: copies do not block)
     std::chrono::steady_clock::time_point call_t0;  // start of the current gq_batch_run
 };
 
@@ -1635,9 +1644,16 @@ int build_batch_plan(int prec, const gq_batch_item* items, size_t n, bool grads,
 }
 
 template <class T>
-int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* grad_out) {
+// One segment of a batch (b->plan, n circuits): packs its tables into staging
+// buffer `slot`, uploads them and enqueues its launches (a captured graph,
+// replayed while the segment's structure and buffers are unchanged), then
+// the copies of its energies and gradients into res_e / res_g (pinned).
+// Nothing here waits for the device, so the host can plan the next segment
+// while this one runs.
+int batch_segment_t(gq_batch* b, bool grads, size_t n, size_t seg, bool first, double* res_e, double* res_g) {
     Engine& e = b->e;
     BatchPlan& P = b->plan;
+    const int slot = (int)(seg & 1);
     // ---- one upload: program, descriptors, runs, reduction tables
     struct Off {
         size_t pass, phase, ops, pool, descs, runs, ggroups, slotg, bcirc, chunks, seg, groups, terms, soff, total;
@@ -1663,9 +1679,12 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
     o.terms = put(P.terms.size() * sizeof(DTerm));
     o.soff = put(P.state_off.size() * sizeof(uint64_t));
     o.total = at;
-    void* hp = nullptr;
-    GQ_TRY(e.stage(o.total, &hp));
-    char* h = (char*)hp;
+    if (b->staged_pending[slot]) {
+        GQ_CUDA(cudaEventSynchronize(b->staged[slot]));
+        b->staged_pending[slot] = false;
+    }
+    GQ_TRY(b->stage[slot].ensure(o.total));
+    char* h = (char*)b->stage[slot].p;
     auto cp = [&](size_t off, const void* src, size_t bytes) {
         const size_t chunk = 4u << 20;
         parallel_for((bytes + chunk - 1) / chunk, 4, [&](size_t i) {
@@ -1698,22 +1717,34 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
                          std::max<uint64_t>(P.total_partials, P.chunks.size()) * sizeof(double) > b->partials.cap ||
                          (n + 1) * sizeof(double) > b->energies.cap ||
                          std::max<size_t>(1, P.total_params) * sizeof(double) > b->grads.cap;
+    if (resized) {
+        // buffers grow: the previous segment's launches may still use them
+        GQ_CUDA(cudaStreamSynchronize(e.stream));
+        ++b->buf_gen;  // captured graphs hold the old pointers
+    }
     GQ_TRY(b->states.ensure(P.total_amps * sizeof(cplx<T>)));
     GQ_TRY(b->lams.ensure(P.total_amps * sizeof(cplx<T>)));
     GQ_TRY(b->partials.ensure(std::max<uint64_t>(1, std::max<uint64_t>(P.total_partials, P.chunks.size())) * sizeof(double)));
     GQ_TRY(b->energies.ensure((n + 1) * sizeof(double)));
     GQ_TRY(b->grads.ensure(std::max<size_t>(1, P.total_params) * sizeof(double)));
     GQ_TRY(b->tables.ensure(o.total));
-    GQ_CUDA(cudaMemcpyAsync(b->tables.p, e.staging.p, o.total, cudaMemcpyHostToDevice, e.stream));
-    GQ_CUDA(cudaEventRecord(e.staged, e.stream));
-    e.staged_pending = true;
+    GQ_CUDA(cudaMemcpyAsync(b->tables.p, b->stage[slot].p, o.total, cudaMemcpyHostToDevice, e.stream));
+    GQ_CUDA(cudaEventRecord(b->staged[slot], e.stream));
+    b->staged_pending[slot] = true;
     e.stats.h2d_bytes += (int64_t)o.total;
     char* d = (char*)b->tables.p;
     cplx<T>* states = (cplx<T>*)b->states.p;
     cplx<T>* lams = (cplx<T>*)b->lams.p;
     double* partial = (double*)b->partials.p;
 
-    const bool replay = b->use_graph && b->graph && b->graph_sig == P.signature && !resized;
+    if (b->graphs.size() <= seg) {
+        b->graphs.resize(seg + 1, nullptr);
+        b->graph_sig.resize(seg + 1, 0);
+        b->graph_gen.resize(seg + 1, 0);
+        b->graph_launches.resize(seg + 1, 0);
+    }
+    const bool replay = b->use_graph && b->graphs[seg] && b->graph_sig[seg] == P.signature &&
+                        b->graph_gen[seg] == b->buf_gen;
     int64_t launches = 0;
     auto record = [&]() -> int {
         GQ_CUDA(cudaMemsetAsync(states, 0, P.total_amps * sizeof(cplx<T>), e.stream));
@@ -1768,6 +1799,7 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
     };
     // the batch's device work alone (pass_ms): from the first launch on
     auto mark0 = [&]() -> int {
+        if (!first) return GQ_OK;
         e.stats.host_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - b->call_t0).count();
         if (e.timing) GQ_CUDA(cudaEventRecord(e.ev_pass0, e.stream));
@@ -1775,12 +1807,12 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
     };
     if (replay) {
         GQ_TRY(mark0());
-        GQ_CUDA(cudaGraphLaunch(b->graph, e.stream));
-        launches = b->graph_launches;  // the recorded sequence
+        GQ_CUDA(cudaGraphLaunch(b->graphs[seg], e.stream));
+        launches = b->graph_launches[seg];  // the recorded sequence
     } else if (b->use_graph) {
-        if (b->graph) {
-            cudaGraphExecDestroy(b->graph);
-            b->graph = nullptr;
+        if (b->graphs[seg]) {
+            cudaGraphExecDestroy(b->graphs[seg]);
+            b->graphs[seg] = nullptr;
         }
         cudaGraph_t g = nullptr;
         GQ_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
@@ -1791,30 +1823,26 @@ int batch_run_t(gq_batch* b, bool grads, size_t n, double* energies, double* gra
             return rc;
         }
         if (ce != cudaSuccess) return fail(GQ_ECUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&b->graph, g, 0);
+        ce = cudaGraphInstantiate(&b->graphs[seg], g, 0);
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) {
-            b->graph = nullptr;
+            b->graphs[seg] = nullptr;
             return fail(GQ_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
         }
-        b->graph_sig = P.signature;
-        b->graph_launches = launches;
+        b->graph_sig[seg] = P.signature;
+        b->graph_gen[seg] = b->buf_gen;
+        b->graph_launches[seg] = launches;
         GQ_TRY(mark0());
-        GQ_CUDA(cudaGraphLaunch(b->graph, e.stream));
+        GQ_CUDA(cudaGraphLaunch(b->graphs[seg], e.stream));
     } else {
         GQ_TRY(mark0());
         GQ_TRY(record());
     }
-    if (e.timing) {
-        GQ_CUDA(cudaEventRecord(e.ev_pass1, e.stream));
-        e.pass_timed = true;
-    }
-    e.stats.kernel_launches = launches;
-    if (energies) GQ_CUDA(cudaMemcpyAsync(energies, b->energies.p, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
-    if (grads && grad_out && P.total_params)
-        GQ_CUDA(cudaMemcpyAsync(grad_out, b->grads.p, P.total_params * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+    e.stats.kernel_launches += launches;
+    GQ_CUDA(cudaMemcpyAsync(res_e, b->energies.p, n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+    if (grads && P.total_params)
+        GQ_CUDA(cudaMemcpyAsync(res_g, b->grads.p, P.total_params * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
     e.stats.d2h_bytes += (int64_t)(n * sizeof(double) + (grads ? P.total_params * sizeof(double) : 0));
-    GQ_CUDA(cudaStreamSynchronize(e.stream));
     return GQ_OK;
 }
 
@@ -1835,6 +1863,18 @@ int gq_batch_create(int precision, gq_batch** out) {
         return rc;
     }
     b->e.opt.tile_qubits = precision == GQ_C64 ? 12 : 11;
+    for (int k = 0; k < 2 && rc == GQ_OK; ++k)
+        if (cudaEventCreateWithFlags(&b->staged[k], cudaEventDisableTiming) != cudaSuccess) {
+            (void)cudaGetLastError();
+            rc = fail(GQ_ECUDA, "cudaEventCreate failed");
+        }
+    if (rc != GQ_OK) {
+        for (cudaEvent_t ev : b->staged)
+            if (ev) cudaEventDestroy(ev);
+        b->e.destroy();
+        delete b;
+        return rc;
+    }
     *out = b;
     return GQ_OK;
 }
@@ -1842,7 +1882,13 @@ int gq_batch_create(int precision, gq_batch** out) {
 int gq_batch_destroy(gq_batch* b) {
     if (!b) return GQ_OK;
     if (b->e.stream) cudaStreamSynchronize(b->e.stream);
-    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (cudaGraphExec_t g : b->graphs)
+        if (g) cudaGraphExecDestroy(g);
+    for (cudaEvent_t ev : b->staged)
+        if (ev) cudaEventDestroy(ev);
+    b->stage[0].release();
+    b->stage[1].release();
+    b->results.release();
     b->states.release();
     b->lams.release();
     b->partials.release();
@@ -1863,13 +1909,58 @@ int gq_batch_run(gq_batch* b, const gq_batch_item* items, size_t n_items, int wa
     e.clear_stats();
     b->call_t0 = std::chrono::steady_clock::now();
     GQ_TRY(e.time_begin());
-    GQ_TRY(build_batch_plan(e.prec, items, n_items, want_gradients != 0, e.opt, b->plan));
-    const int rc = e.prec == GQ_C64 ? batch_run_t<float>(b, want_gradients != 0, n_items, energies_out, grads_out)
-                                    : batch_run_t<double>(b, want_gradients != 0, n_items, energies_out, grads_out);
-    if (rc != GQ_OK) return rc;
-    e.stats.passes = (int64_t)b->plan.prog.passes.size();
-    e.stats.phases = (int64_t)b->plan.prog.phases.size();
-    e.stats.state_bytes = (int64_t)(b->plan.total_amps * e.amp_bytes());
+    const bool grads = want_gradients != 0;
+    // Segments of about equal work (state size x ops), planned one after
+    // another on the host while the device runs the previous one.
+    const size_t nseg = std::max<size_t>(1, std::min<size_t>(8, n_items / 512));
+    std::vector<double> work(n_items);
+    double wsum = 0.0;
+    size_t total_params = 0;
+    for (size_t c = 0; c < n_items; ++c) {
+        const int nq = std::max(1, std::min(30, items[c].num_qubits));
+        work[c] = std::ldexp((double)(items[c].n_ops + 1), std::max(nq, RQ));
+        wsum += work[c];
+        total_params += items[c].n_params;
+    }
+    std::vector<size_t> cut{0};
+    {
+        double acc = 0.0;
+        for (size_t c = 0; c < n_items; ++c) {
+            acc += work[c];
+            if (cut.size() < nseg && acc >= wsum * (double)cut.size() / (double)nseg && c + 1 < n_items)
+                cut.push_back(c + 1);
+        }
+        cut.push_back(n_items);
+    }
+    GQ_TRY(b->results.ensure((n_items + std::max<size_t>(1, total_params)) * sizeof(double)));
+    double* res_e = (double*)b->results.p;
+    double* res_g = res_e + n_items;
+    size_t poff = 0;
+    int64_t passes = 0, phases = 0, state_bytes = 0;
+    for (size_t sg = 0; sg + 1 < cut.size(); ++sg) {
+        const size_t c0 = cut[sg], cnt = cut[sg + 1] - c0;
+        GQ_TRY(build_batch_plan(e.prec, items + c0, cnt, grads, e.opt, b->plan));
+        const int rc = e.prec == GQ_C64 ? batch_segment_t<float>(b, grads, cnt, sg, sg == 0, res_e + c0, res_g + poff)
+                                        : batch_segment_t<double>(b, grads, cnt, sg, sg == 0, res_e + c0, res_g + poff);
+        if (rc != GQ_OK) {
+            cudaStreamSynchronize(e.stream);
+            return rc;
+        }
+        poff += b->plan.total_params;
+        passes += (int64_t)b->plan.prog.passes.size();
+        phases += (int64_t)b->plan.prog.phases.size();
+        state_bytes = std::max<int64_t>(state_bytes, (int64_t)(b->plan.total_amps * e.amp_bytes()));
+    }
+    if (e.timing) {
+        GQ_CUDA(cudaEventRecord(e.ev_pass1, e.stream));
+        e.pass_timed = true;
+    }
+    GQ_CUDA(cudaStreamSynchronize(e.stream));
+    if (energies_out) std::memcpy(energies_out, res_e, n_items * sizeof(double));
+    if (grads && grads_out && total_params) std::memcpy(grads_out, res_g, total_params * sizeof(double));
+    e.stats.passes = passes;
+    e.stats.phases = phases;
+    e.stats.state_bytes = state_bytes;
     return e.time_end();
 }
 

@@ -255,10 +255,12 @@ int gq_dm_set_option(gq_dm* dm, int key, int64_t value);
  * algorithm/vqe: every item is a circuit applied to |0...0> with a Pauli sum;
  * gq_batch_run returns Re <psi|H|psi> per item and, with want_gradients, the
  * adjoint gradient of each item (n_params entries per item, concatenated in
- * item order). All items run in one sequence of batched launches; the items
- * are analysed and scheduled on the host's threads first. Stats: last_ms
- * covers the whole call (host planning, upload, launches, results), pass_ms
- * the batched launches alone.                                               */
+ * item order). Items run as batched launches in up to 8 segments of about
+ * equal work: the host's threads analyse and schedule a segment while the
+ * device runs the one before, and each segment's launches are a captured CUDA
+ * graph, replayed while its structure (not its angles) stays the same.
+ * Stats: last_ms covers the whole call, pass_ms the span of the launches,
+ * host_ms the host time before the first launch.                            */
 typedef struct gq_batch gq_batch;
 typedef struct gq_batch_item {
     int32_t num_qubits;

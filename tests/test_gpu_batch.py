@@ -65,3 +65,18 @@ def test_qaoa_gradients_match_oracle_central_differences():
                 xp[i] += 1e-6
                 xm[i] -= 1e-6
                 assert abs(grads[k][i] - (energy(xp) - energy(xm)) / 2e-6) < tol
+
+
+def test_segmented_batch_matches_single_segment():
+    # 1100 circuits run as two segments (host planning of one overlaps the
+    # other's launches); every energy and gradient equals the same circuits
+    # run in a batch of their own, and a second call replays both segments
+    evals = workloads.qaoa_batch(1100, seed=31, n_values=(4, 6, 8, 10), p_range=(1, 3))
+    b = batch.Batch(_abi.GQ_C128)
+    energies, grads = b.Run(evals)
+    energies2, grads2 = b.Run(evals)
+    for k in list(range(0, 1100, 97)) + [549, 550, 551, 1099]:
+        one = batch.Batch(_abi.GQ_C128)
+        e1, g1 = one.Run([evals[k]])
+        assert abs(energies[k] - e1[0]) < 1e-12 and abs(energies2[k] - e1[0]) < 1e-12
+        assert np.max(np.abs(grads[k] - g1[0])) < 1e-12 and np.max(np.abs(grads2[k] - g1[0])) < 1e-12
