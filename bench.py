@@ -277,23 +277,30 @@ def extra_density():
                                "max_abs_z_error_vs_fp64_oracle": z_err}}
 
 
-def extra_qaoa():
+def extra_qaoa(qubits=0, count=0, calls=3, graph=True):
     """4096 QAOA MaxCut circuits on seeded random 3-regular graphs, n in
     {10..20} even, p in 1..4, complex64: energies + adjoint gradients in one
-    batched call (second call replays the captured CUDA graph)."""
+    batched call (later calls replay the captured CUDA graphs). qubits / count
+    keep only the circuits of that size / the first `count` (profiling cases)."""
     from goqu_b200 import _abi, batch, workloads
     t0 = time.perf_counter()
     evals = workloads.qaoa_batch(4096, seed=4)
+    if qubits:
+        evals = [e for e in evals if e[0].NumQubits() == qubits]
+    if count:
+        evals = evals[:count]
     streams, terms = batch.Batch.encode(evals)
     host_s = time.perf_counter() - t0
     npar = [len(e[1]) for e in evals]
     b = batch.Batch(_abi.GQ_C64)
     b.set_option(_abi.GQ_OPT_TIMING, 1)
-    ms, dev = [], []
-    for _ in range(3):
+    b.set_option(_abi.GQ_OPT_USE_GRAPH, 1 if graph else 0)
+    ms, dev, host = [], [], []
+    for _ in range(calls):
         energies, grads = b.run_encoded(streams, terms, npar)
         ms.append(b.stats()["last_ms"])
         dev.append(b.stats()["pass_ms"])
+        host.append(b.stats()["host_ms"])
     st = b.stats()
     # error against the FP64 oracle on a sample of the batch: energies, and
     # gradients against central differences of the oracle energy (each QAOA
@@ -307,7 +314,7 @@ def extra_qaoa():
         return orc.expect_pauli_sum(orc.sv_evolve(encode.statevector_ops(bound)), pauli.to_terms(h)).real
 
     e_err = g_err = 0.0
-    for k in range(0, 4096, 256):
+    for k in range(0, len(evals), max(1, len(evals) // 16)):
         c, names, h, x = evals[k]
         e_err = max(e_err, abs(energies[k] - energy(c, names, h, x)))
         for i in range(len(names)):
@@ -315,13 +322,15 @@ def extra_qaoa():
             xp[i] += 1e-6
             xm[i] -= 1e-6
             g_err = max(g_err, abs(grads[k][i] - (energy(c, names, h, xp) - energy(c, names, h, xm)) / 2e-6))
-    return {"workload": "4096 QAOA MaxCut circuits (n 10..20, p 1..4), complex64, energies + gradients",
-            "circuits_per_s": 4096 / (ms[-1] / 1000.0), "ms_call_first": ms[0], "ms_call_replay": ms[-1],
-            "ms_device_replay": dev[-1], "timing": "call: host planning on all threads + upload + graph + results "
-                                                  "(CUDA events on the batch stream); device: the batched launches",
+    sub = "" if not (qubits or count) else f" (subset: {'n = %d, ' % qubits if qubits else ''}{len(evals)} circuits)"
+    return {"workload": "4096 QAOA MaxCut circuits (n 10..20, p 1..4), complex64, energies + gradients" + sub,
+            "circuits": len(evals), "circuits_per_s": len(evals) / (ms[-1] / 1000.0), "ms_call_first": ms[0],
+            "ms_call_replay": ms[-1], "ms_device_replay": dev[-1], "ms_host_before_launch": host[-1],
+            "timing": "call: host planning (overlapped with the device by segments) + upload + graphs + results "
+                      "(CUDA events on the batch stream); device: span of the batched launches",
             "passes": st["passes"], "launches": st["kernel_launches"], "host_encode_s": host_s,
             "max_abs_energy_error_vs_fp64_oracle": e_err, "max_abs_grad_error_vs_fp64_central_difference": g_err,
-            "error_sample": "16 circuits (every 256th)"}
+            "error_sample": f"{len(range(0, len(evals), max(1, len(evals) // 16)))} circuits evenly spaced"}
 
 
 def extra_parity():
@@ -473,7 +482,19 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--jit", type=int, choices=[0, 1, 2], default=2,
                     help="specialised pass kernels: 0 off, 1 when compiled, 2 wait for them (default)")
+    ap.add_argument("--only-extra", choices=["parity_20q", "adjoint", "density_matrix", "qaoa_batch"],
+                    help="run one extra workload alone and print its JSON (profiling)")
+    ap.add_argument("--qaoa-qubits", type=int, default=0, help="qaoa_batch: keep the circuits of this size")
+    ap.add_argument("--qaoa-count", type=int, default=0, help="qaoa_batch: keep the first N circuits")
+    ap.add_argument("--qaoa-calls", type=int, default=3)
+    ap.add_argument("--qaoa-graph", type=int, choices=[0, 1], default=1)
     args = ap.parse_args()
+    if args.only_extra:
+        fns = {"parity_20q": extra_parity, "adjoint": extra_adjoint, "density_matrix": extra_density,
+               "qaoa_batch": lambda: extra_qaoa(args.qaoa_qubits, args.qaoa_count, args.qaoa_calls,
+                                                args.qaoa_graph == 1)}
+        print(json.dumps({args.only_extra: fns[args.only_extra]()}))
+        return
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
