@@ -908,7 +908,7 @@ bool jit_plan_dual(const Program& pr, size_t pi, bool c64, int threads, int min_
                     case K_SWAP: return "k_swap<T, " + S0 + ", " + S1 + ">(" + x + ", " + creg + ");";
                     case K_PHASE: return "k_phase<T>(" + x + ", p.m[" + num(gen.copy(rm, 1)) + "], " + creg + ");";
                     case K_PAIRSUM:
-                        return "k_pairsum<T>(" + x + ", pool + " + num(rm) + "u, " + num(op.nreg) + "u, g0);";
+                        return "k_pairsum<T>(" + x + ", pool + " + num(rm) + "u, g0);";
                     case K_DIAG: {
                         std::string h = "{ uint32_t hi = 0; ";
                         int k = 0;
@@ -945,7 +945,7 @@ bool jit_plan_dual(const Program& pr, size_t pi, bool c64, int threads, int min_
                 e = h + "gv = grad_diag_c<T>(a, bb, pool + " + num(rm) + "u, hi << " + num(op.nreg) + ", " + creg +
                     ", " + hex64(op.ridx) + ");";
             } else if (kind == K_PAIRSUM) {
-                e = "gv = grad_pairsum_c<T>(a, bb, pool + " + num(rm) + "u, " + num(op.nreg) + "u, g0);";
+                e = "gv = grad_pairsum_c<T>(a, bb, pool + " + num(rm) + "u, g0);";
             } else if (kind == K_X) {
                 const uint32_t px = gen.copy(rm, 2);
                 e = "gv = grad_x_c<T, " + S0 + ">(a, bb, p.m[" + num(px) + "], p.m[" + num(px + 1) + "], " + creg + ");";

@@ -443,12 +443,47 @@ bool unit_modulus(const NGate& g) {
     return true;
 }
 
-std::vector<NGate> fuse_pairsums(const std::vector<NGate>& in, uint64_t R, const int* rq) {
-    auto code = [&](int q) {
+// The classified pair data of a K_PAIRSUM (layout in tile_core.cuh,
+// pair_counts): counts of the pairs on two register bits per slot, a qubit
+// mask per register bit for its pairs with global qubits, the packed pairs of
+// two global qubits. Every value is an integer below 2^16, exact in FP32.
+void pair_data(const std::vector<int>& targets, uint64_t R, const int* rq, std::vector<Z>& data) {
+    auto regbit = [&](int q) {
         for (int k = 0; k < RQ; ++k)
-            if (rq[k] == q && (R >> q & 1ull)) return (double)k;
-        return (double)(16 + q);
+            if (rq[k] == q && (R >> q & 1ull)) return k;
+        return -1;
     };
+    uint64_t lo = 0, hi = 0, M[RQ] = {0, 0, 0, 0};
+    int nr[RQ] = {0, 0, 0, 0};
+    std::vector<int> gg;
+    for (size_t p = 0; p + 1 < targets.size(); p += 2) {
+        const int a = targets[p], b = targets[p + 1], ka = regbit(a), kb = regbit(b);
+        if (ka >= 0 && kb >= 0) {
+            for (int j = 0; j < NREG; ++j)
+                if (((j >> ka) ^ (j >> kb)) & 1) (j < 8 ? lo : hi) += 1ull << (8 * (j & 7));
+        } else if (ka >= 0 || kb >= 0) {
+            const int r = ka >= 0 ? ka : kb, q = ka >= 0 ? b : a;
+            M[r] |= 1ull << q;
+            ++nr[r];
+        } else {
+            gg.push_back(a | (b << 6));
+        }
+    }
+    auto c16 = [](uint64_t v, int i) { return (double)((v >> (16 * i)) & 0xffffull); };
+    data.push_back(Z{c16(lo, 0), c16(lo, 1)});
+    data.push_back(Z{c16(lo, 2), c16(lo, 3)});
+    data.push_back(Z{c16(hi, 0), c16(hi, 1)});
+    data.push_back(Z{c16(hi, 2), c16(hi, 3)});
+    for (int r = 0; r < RQ; ++r) {
+        data.push_back(Z{c16(M[r], 0), c16(M[r], 1)});
+        data.push_back(Z{c16(M[r], 2), (double)nr[r]});
+    }
+    data.push_back(Z{(double)gg.size(), 0.0});
+    for (size_t k = 0; k < gg.size(); k += 2)
+        data.push_back(Z{(double)gg[k], k + 1 < gg.size() ? (double)gg[k + 1] : 0.0});
+}
+
+std::vector<NGate> fuse_pairsums(const std::vector<NGate>& in, uint64_t R, const int* rq) {
     std::vector<NGate> out;
     size_t i = 0;
     while (i < in.size()) {
@@ -484,6 +519,12 @@ std::vector<NGate> fuse_pairsums(const std::vector<NGate>& in, uint64_t R, const
                 const NGate& h = in[grp[0]];
                 if (h.type == g.type && h.param == g.param && eq(h.data[0], g.data[0]) && eq(h.data[1], g.data[1]) &&
                     grp.size() < 200) {
+                    // a pair at most once per op (its qubit masks hold each pair once)
+                    bool dup = false;
+                    for (size_t q : grp)
+                        dup = dup || (std::min(in[q].targets[0], in[q].targets[1]) == std::min(g.targets[0], g.targets[1]) &&
+                                      std::max(in[q].targets[0], in[q].targets[1]) == std::max(g.targets[0], g.targets[1]));
+                    if (dup) continue;
                     grp.push_back(k);
                     placed = true;
                     break;
@@ -508,8 +549,8 @@ std::vector<NGate> fuse_pairsums(const std::vector<NGate>& in, uint64_t R, const
             for (size_t k : grp) {
                 f.targets.push_back(in[k].targets[0]);
                 f.targets.push_back(in[k].targets[1]);
-                f.data.push_back(Z{code(in[k].targets[0]), code(in[k].targets[1])});
             }
+            pair_data(f.targets, R, rq, f.data);
             const Z e = h.data[0], o = h.data[1];
             if (h.type == K_GRAD) {
                 for (int c = 0; c <= K; ++c)
@@ -773,7 +814,7 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                     op.flags = g.pure ? 1 : 0;
                     prog.pool.insert(prog.pool.end(), g.data.begin(), g.data.end());
                 } else if (kind == K_PAIRSUM) {
-                    op.nreg = (uint8_t)((g.data.size() - 1) / 2);
+                    op.nreg = (uint8_t)(g.targets.size() / 2);  // pairs; the table has nreg + 1 entries
                     op.flags = g.pure ? 2 : 0;  // counts of the preceding gradient pair sum
                     prog.pool.insert(prog.pool.end(), g.data.begin(), g.data.end());
                 } else if (kind == K_SWAP) {

@@ -389,29 +389,66 @@ GQ_HD void k_phase(cplx<T> (&a)[NREG], const cplx<T> s, uint32_t creg) {
 }
 
 // Per-slot counts of a K_PAIRSUM's odd pairs, one byte per register slot
-// (slots 0..7 in lo, 8..15 in hi): each pair adds 1 to the slots where its
-// two bits differ. slot_bits(r, h): byte j = bit r of slot j (h: of j + 8).
+// (slots 0..7 in lo, 8..15 in hi). slot_bits(r, h): byte j = bit r of slot j
+// (h: of j + 8).
 GQ_HD uint64_t slot_bits(int r, bool h) {
     return r == 0 ? 0x0100010001000100ull
                   : (r == 1 ? 0x0101000001010000ull : (r == 2 ? 0x0101010100000000ull : (h ? 0x0101010101010101ull : 0ull)));
 }
 
-// Byte mask of a pair code: a register bit's slot pattern, or a global
-// qubit's bit of g0 broadcast to every slot.
-GQ_HD uint64_t code_bits(int code, uint64_t g0, bool h) {
-    if (code < 16) return slot_bits(code, h);
-    return ((g0 >> (code - 16)) & 1ull) ? 0x0101010101010101ull : 0ull;
+GQ_HD uint32_t popc64(uint64_t v) {
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)__popcll(v);
+#else
+    return (uint32_t)__builtin_popcountll(v);
+#endif
 }
 
-template <class T, class MP>
-GQ_HD void pair_counts(MP codes, uint32_t K, uint64_t g0, uint64_t& lo, uint64_t& hi) {
-    lo = hi = 0;
-    for (uint32_t k = 0; k < K; ++k) {
-        const cplx<T> cd = ldc(codes, k);
-        const int c0 = (int)cd.x, c1 = (int)cd.y;
-        lo += code_bits(c0, g0, false) ^ code_bits(c1, g0, false);
-        hi += code_bits(c0, g0, true) ^ code_bits(c1, g0, true);
+// The op's data, classified on the host (all values small integers, exact in
+// FP32), then its factor table T[0..K]:
+//   d[0..1], d[2..3]: lo and hi counts of the pairs on two register bits, as
+//     16-bit chunks (fixed per slot);
+//   d[4 + 2r], d[5 + 2r]: pairs of register bit r with global qubits: their
+//     qubit mask M_r (three 16-bit chunks) and number n_r. Slots with bit r
+//     set differ from the pairs whose qubit bit of g0 is 0 (n_r - m_r of
+//     them, m_r = popcount(g0 & M_r)), slots with bit r clear from the m_r
+//     others;
+//   d[12].x = G pairs of two global qubits, packed q0 | q1 << 6, two per
+//     entry from d[13]: they add the same count to every slot.
+// Returns the factor table.
+template <class T>
+GQ_HD const cplx<T>* pair_counts(const cplx<T>* d, uint64_t g0, uint64_t& lo, uint64_t& hi) {
+    auto u = [](T v) { return (uint64_t)(uint32_t)v; };
+    lo = u(d[0].x) | (u(d[0].y) << 16) | (u(d[1].x) << 32) | (u(d[1].y) << 48);
+    hi = u(d[2].x) | (u(d[2].y) << 16) | (u(d[3].x) << 32) | (u(d[3].y) << 48);
+    constexpr uint64_t ONES = 0x0101010101010101ull;
+#pragma unroll
+    for (int r = 0; r < RQ; ++r) {
+        const cplx<T> c0 = d[4 + 2 * r], c1 = d[5 + 2 * r];
+        const uint64_t n = u(c1.y);
+        if (n == 0) continue;
+        const uint64_t M = u(c0.x) | (u(c0.y) << 16) | (u(c1.x) << 32);
+        const uint64_t m = popc64(g0 & M);
+        const uint64_t sl = slot_bits(r, false), sh = slot_bits(r, true);
+        lo += (n - m) * sl + m * (ONES - sl);
+        hi += (n - m) * sh + m * (ONES - sh);
     }
+    const uint32_t G = (uint32_t)d[12].x;
+    uint64_t ng = 0;
+    for (uint32_t k = 0; k < G; ++k) {
+        const cplx<T> c = d[13 + (k >> 1)];
+        const uint32_t pq = (uint32_t)((k & 1) ? c.y : c.x);
+        ng += ((g0 >> (pq & 63u)) ^ (g0 >> (pq >> 6))) & 1ull;
+    }
+    lo += ng * ONES;
+    hi += ng * ONES;
+    return d + 13 + ((G + 1) >> 1);
+}
+
+// The factor table of a K_PAIRSUM's data (after its classified pairs).
+template <class T>
+GQ_HD const cplx<T>* pair_counts_table(const cplx<T>* d) {
+    return d + 13 + (((uint32_t)d[12].x + 1) >> 1);
 }
 
 GQ_HD uint32_t slot_count(uint64_t lo, uint64_t hi, int j) {
@@ -426,10 +463,10 @@ GQ_HD void k_pairsum_lh(cplx<T> (&a)[NREG], const cplx<T>* table, uint64_t lo, u
 }
 
 template <class T>
-GQ_HD void k_pairsum(cplx<T> (&a)[NREG], const cplx<T>* d, uint32_t K, uint64_t g0) {
+GQ_HD void k_pairsum(cplx<T> (&a)[NREG], const cplx<T>* d, uint64_t g0) {
     uint64_t lo, hi;
-    pair_counts<T>(d, K, g0, lo, hi);
-    k_pairsum_lh<T>(a, d + K, lo, hi);
+    const cplx<T>* table = pair_counts<T>(d, g0, lo, hi);
+    k_pairsum_lh<T>(a, table, lo, hi);
 }
 
 // Decodes one op and hands its body to `each`: each(body) calls body(a, sm)
@@ -528,7 +565,7 @@ GQ_HD void dispatch_op(const KOp& op, const cplx<T>* pool, uint64_t g0, uint32_t
             each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_phase<T>(x, ldc(m, 0), creg); });
             break;
         case K_PAIRSUM:
-            each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_pairsum<T>(x, m, op.nreg, g0); });
+            each([&](cplx<T>(&x)[NREG], cplx<T>*) { k_pairsum<T>(x, m, g0); });
             break;
         case K_RESET:
             switch (op.t0) {
@@ -656,11 +693,10 @@ GQ_HD double grad_pairsum_lh(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG],
 }
 
 template <class T>
-GQ_HD double grad_pairsum_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const cplx<T>* d, uint32_t K,
-                            uint64_t g0) {
+GQ_HD double grad_pairsum_c(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], const cplx<T>* d, uint64_t g0) {
     uint64_t lo, hi;
-    pair_counts<T>(d, K, g0, lo, hi);
-    return grad_pairsum_lh<T>(a, b, d + K, lo, hi);
+    const cplx<T>* table = pair_counts<T>(d, g0, lo, hi);
+    return grad_pairsum_lh<T>(a, b, table, lo, hi);
 }
 
 // Re sum_j conj(lambda_j) (G psi)_j over the thread's amplitudes, G being the
@@ -678,7 +714,7 @@ GQ_HD double grad_partial(const cplx<T> (&a)[NREG], const cplx<T> (&b)[NREG], co
         case K_DIAG:
             return grad_diag_c<T>(a, b, m, (uint32_t)(pext64(g0, op.dmask) << op.nreg), creg, op.ridx);
         case K_PAIRSUM:  // G = sum of the pairs' generators: T[c] per slot
-            return grad_pairsum_c<T>(a, b, m, op.nreg, g0);
+            return grad_pairsum_c<T>(a, b, m, g0);
         case K_X: {
             const cplx<T> p0 = ldc(m, 0), p1 = ldc(m, 1);
             switch (op.t0) {
@@ -742,15 +778,16 @@ GQ_HD void run_phase_dual(cplx<T>* sm_a, cplx<T>* sm_b, const PhaseDesc& ph, con
     // Pair sums: counts computed once for both states, and once for a
     // gradient pair sum and the unitary one after it (KOp.flags bit 1).
     uint64_t plo = 0, phi = 0;
+    const cplx<T>* ptab = nullptr;
     bool pcount = false;
     for (int o = ob; o < oe; ++o) {
         const KOp& op = ops[o];
         if (op.type == K_GRAD) {
             double v;
             if (op.flags == K_PAIRSUM) {
-                pair_counts<T>(pool + op.mat, op.nreg, g0, plo, phi);
+                ptab = pair_counts<T>(pool + op.mat, g0, plo, phi);
                 pcount = true;
-                v = grad_pairsum_lh<T>(a, b, pool + op.mat + op.nreg, plo, phi);
+                v = grad_pairsum_lh<T>(a, b, ptab, plo, phi);
             } else {
                 pcount = false;
                 v = (op.flags == K_PHASE || op.flags == K_DIAG || op.flags == K_X)
@@ -761,10 +798,12 @@ GQ_HD void run_phase_dual(cplx<T>* sm_a, cplx<T>* sm_b, const PhaseDesc& ph, con
             continue;
         }
         if (op.type == K_PAIRSUM) {
-            if (!((op.flags & 2) && pcount)) pair_counts<T>(pool + op.mat, op.nreg, g0, plo, phi);
+            // the unitary's own table: its data has the same pair layout as the gradient's
+            const cplx<T>* tab = pair_counts_table<T>(pool + op.mat);
+            if (!((op.flags & 2) && pcount)) pair_counts<T>(pool + op.mat, g0, plo, phi);
             pcount = true;
-            k_pairsum_lh<T>(a, pool + op.mat + op.nreg, plo, phi);
-            k_pairsum_lh<T>(b, pool + op.mat + op.nreg, plo, phi);
+            k_pairsum_lh<T>(a, tab, plo, phi);
+            k_pairsum_lh<T>(b, tab, plo, phi);
             continue;
         }
         pcount = false;
