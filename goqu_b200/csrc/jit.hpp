@@ -54,8 +54,7 @@ struct JitEntry {
 
 // A chain of one-qubit ops on one register bit inside a phase: uncontrolled
 // one-qubit unitaries and X-type ops, each X either unconditional (pred -1)
-// or controlled by predicate `pred` (0 or 1, local to the chain) on qubits
-// outside the registers (CTA-index or thread bits).
+// or controlled by CTA-uniform predicate `pred` (0 or 1, local to the chain).
 // No other op of the phase touches the bit between them, so the chain acts as
 // one unitary per combination of its (at most two) predicates. Ops are pass
 // relative, in order of application.
@@ -107,8 +106,8 @@ bool jit_pack(const Program& pr, size_t pass, const JitPlan& plan, bool c64, voi
 // 1e-150 (the generator then keeps the dense 2x2).
 bool u1_decompose(const Z* m, double* t, Z* lam, Z* post0, Z* post1);
 
-// Candidate chains (JitChain) of pass `pass`, per phase, with the control
-// mask of each predicate, and whether every product of the chain
+// Candidate chains (JitChain) of pass `pass`, per phase, with the outer-qubit
+// control mask of each predicate, and whether every product of the chain
 // decomposes into the shear form with the program's current numbers. A chain
 // holds at least two one-qubit unitaries.
 struct ChainCand {

@@ -10,7 +10,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <functional>
 #include <map>
 
 namespace gq {
@@ -242,6 +241,8 @@ std::vector<ChainCand> jit_chains(const Program& pr, size_t pi) {
     const PassDesc& pd = pr.passes[pi];
     uint32_t op_base, pool_base;
     jit_bases(pr, pi, &op_base, &pool_base);
+    uint64_t outer = 0;
+    for (int k = 0; k < pd.n_outer; ++k) outer |= 1ull << pd.outer_q[k];
     std::vector<ChainCand> res;
     for (int p = 0; p < pd.n_phases; ++p) {
         const PhaseDesc& ph = pr.phases[pd.phase0 + p];
@@ -249,7 +250,7 @@ std::vector<ChainCand> jit_chains(const Program& pr, size_t pi) {
             auto element = [&](const KOp& op) {
                 if (op.t0 != r || op.creg) return false;
                 if (op.type == K_U1) return op.cmask == 0;
-                return op.type == K_X;  // unconditional, or controlled from CTA or thread bits
+                return op.type == K_X && (op.cmask & ~outer) == 0;
             };
             std::vector<int> run;
             auto finish = [&]() {
@@ -390,23 +391,17 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
                 }
             if (sv != ph.tlo_slot[v] || g != ph.tlo_glob[v]) return PLAN_UNCOVERED;
         }
-        // Predicates: controls of X-type ops outside the registers. One that
-        // lies in the CTA's outer bits holds for a whole CTA. Such an op costs
-        // no arithmetic: the X swaps registers under a branch on the predicate,
-        // and its phases become predicate-dependent pending factors, read from
-        // a table of the predicates' values when they are applied.
-        // Controls on thread bits vary inside a CTA: their tables are read
-        // with selects between constant-bank values instead of an index.
+        // Uniform predicates: controls of X-type and phase ops that lie in the
+        // CTA's outer bits hold for a whole CTA. Such an op costs no arithmetic:
+        // the X swaps registers under a CTA-uniform branch, and both become
+        // predicate-dependent pending factors, read from a table indexed by
+        // the predicates' values when they are applied.
         std::vector<uint64_t> upred;
-        for (int pass_kind = 0; pass_kind < 2; ++pass_kind)
-            for (int oa = ph.op_begin; oa < ph.op_end && (int)upred.size() < kmax; ++oa) {
-                const KOp& op = pr.ops[oa];
-                if (op.type != K_X || !op.cmask || ((op.cmask & ~outer_mask) != 0) != (pass_kind == 1)) continue;
-                if (std::find(upred.begin(), upred.end(), op.cmask) == upred.end()) upred.push_back(op.cmask);
-            }
-        uint32_t tpred = 0;  // predicates on thread bits
-        for (size_t k = 0; k < upred.size(); ++k)
-            if (upred[k] & ~outer_mask) tpred |= 1u << k;
+        for (int oa = ph.op_begin; oa < ph.op_end && (int)upred.size() < kmax; ++oa) {
+            const KOp& op = pr.ops[oa];
+            if (op.type != K_X || !op.cmask || (op.cmask & ~outer_mask)) continue;
+            if (std::find(upred.begin(), upred.end(), op.cmask) == upred.end()) upred.push_back(op.cmask);
+        }
         const int K = (int)upred.size(), NC = 1 << K;
         auto upred_of = [&](uint64_t cmask) {
             for (int k = 0; k < K; ++k)
@@ -448,32 +443,11 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
         if (K > 0) {
             b += "        const uint32_t pc = 0u";
             for (int k = 0; k < K; ++k)
-                b += " | (((" + std::string((tpred >> k) & 1 ? "g0" : "base") + " & " + hex64(upred[k]) + ") == " +
-                     hex64(upred[k]) + ") ? " + hex32(1u << k) + " : 0u)";
+                b += " | (((base & " + hex64(upred[k]) + ") == " + hex64(upred[k]) + ") ? " + hex32(1u << k) + " : 0u)";
             b += ";\n";
         }
         b += "        cplx<T> a[16];\n";
         for (int j = 0; j < NREG; ++j) b += "        a[" + num(j) + "] = sm[sb ^ " + hex32(ph.rslot[j]) + "];\n";
-
-        // Entry e of the table at `off` over predicate bits `bits` (entry index
-        // bit i = predicate bits[i]): an index for CTA-uniform predicates, a
-        // tree of selects when one varies by thread.
-        auto table_read = [&](uint32_t off, const std::vector<int>& bits, const std::string& field) {
-            bool thr = false;
-            for (int k : bits) thr = thr || ((tpred >> k) & 1);
-            if (!thr) {
-                std::string idx = "0u";
-                for (size_t i = 0; i < bits.size(); ++i)
-                    idx += " | (((pc >> " + num(bits[i]) + ") & 1u) << " + num((long long)i) + ")";
-                return "p.m[" + num(off) + " + (" + idx + ")]" + field;
-            }
-            std::function<std::string(int, uint32_t)> tree = [&](int level, uint32_t e) -> std::string {
-                if (level < 0) return "p.m[" + num(off + e) + "]" + field;
-                return "(((pc >> " + num(bits[level]) + ") & 1u) ? " + tree(level - 1, e | (1u << level)) + " : " +
-                       tree(level - 1, e) + ")";
-            };
-            return tree((int)bits.size() - 1, 0u);
-        };
 
         PendT pend[NREG];
         for (int j = 0; j < NREG; ++j) pend[j].assign(NC, Pend());
@@ -506,7 +480,12 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
                 td.push_back(dn[c]);
             }
             const uint32_t off = gen.ratio_table(tn, td);
-            b += "        a[" + num(j) + "] = cmul(" + table_read(off, bits, "") + ", a[" + num(j) + "]);\n";
+            std::string idx;
+            for (size_t i = 0; i < bits.size(); ++i) {
+                if (i) idx += " | ";
+                idx += "(((pc >> " + num(bits[i]) + ") & 1u) << " + num((long long)i) + ")";
+            }
+            b += "        a[" + num(j) + "] = cmul(p.m[" + num(off) + " + (" + idx + ")], a[" + num(j) + "]);\n";
         };
         // Groups of an op on target bits `tm` under register controls `creg`.
         auto groups = [&](uint32_t tm, uint32_t creg) {
@@ -590,9 +569,11 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
                             for (int c = 0; c < NC; ++c) pend_add(pend[g[1]][c], gen.atom(4, f.fid * 4 + local(c)));
                             normalize(g);
                         }
-                        const std::vector<int> cbits(f.ubit, f.ubit + f.nl);
-                        b += "        k_shear<T, " + S0 + ", false>(a, " +
-                             table_read(gen.chain_t(f.fid, f.nl), cbits, ".x") + ", 0u);\n";
+                        std::string idx = "0u";
+                        for (int k = 0; k < f.nl; ++k)
+                            idx += " | (((pc >> " + num(f.ubit[k]) + ") & 1u) << " + num(k) + ")";
+                        b += "        k_shear<T, " + S0 + ", false>(a, p.m[" + num(gen.chain_t(f.fid, f.nl)) + " + (" +
+                             idx + ")].x, 0u);\n";
                         for (const auto& g : gs) {
                             pend[g[1]] = pend[g[0]];
                             for (int c = 0; c < NC; ++c) {
