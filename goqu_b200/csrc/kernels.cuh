@@ -897,29 +897,35 @@ __global__ void k_apply_terms_batch(const cplx<T>* __restrict__ psi_all, cplx<T>
         for (int k = threadIdx.x; k < t_hi - t_lo; k += blockDim.x) stm[k] = terms[t_lo + k];
     }
     __syncthreads();
-    const DGroup* gp = staged ? sgr : groups + c.group0;
-    const DTerm* tp = staged ? stm : terms + t_lo;
     double e = 0.0;
-    for (uint64_t i = ch.begin + threadIdx.x; i < end; i += blockDim.x) {
-        double lr = 0.0, li = 0.0;
-        for (int g = 0; g < c.ngroups; ++g) {
-            const DGroup gr = gp[g];
-            const uint64_t j = i ^ gr.x;
-            const cplx<T> v = psi[j];
-            double fr = 0.0, fi = 0.0;
-            for (int k = gr.t0 - t_lo; k < gr.t1 - t_lo; ++k) {
-                const DTerm tm = tp[k];
-                const double sg = (__popcll(j & tm.z) & 1) ? -1.0 : 1.0;
-                fr += sg * tm.wre;
-                fi += sg * tm.wim;
+    // The loop is instantiated once for the shared copies and once for the
+    // global arrays, so that each reads its terms with its own load kind.
+    auto run = [&](const DGroup* gp, const DTerm* tp) {
+        for (uint64_t i = ch.begin + threadIdx.x; i < end; i += blockDim.x) {
+            double lr = 0.0, li = 0.0;
+            for (int g = 0; g < c.ngroups; ++g) {
+                const DGroup gr = gp[g];
+                const uint64_t j = i ^ gr.x;
+                const cplx<T> v = psi[j];
+                double fr = 0.0, fi = 0.0;
+                for (int k = gr.t0 - t_lo; k < gr.t1 - t_lo; ++k) {
+                    const DTerm tm = tp[k];
+                    const double sg = (__popcll(j & tm.z) & 1) ? -1.0 : 1.0;
+                    fr += sg * tm.wre;
+                    fi += sg * tm.wim;
+                }
+                lr += fr * (double)v.x - fi * (double)v.y;
+                li += fr * (double)v.y + fi * (double)v.x;
             }
-            lr += fr * (double)v.x - fi * (double)v.y;
-            li += fr * (double)v.y + fi * (double)v.x;
+            lam[i] = {(T)lr, (T)li};
+            const cplx<T> a = psi[i];
+            e += (double)a.x * lr + (double)a.y * li;
         }
-        lam[i] = {(T)lr, (T)li};
-        const cplx<T> a = psi[i];
-        e += (double)a.x * lr + (double)a.y * li;
-    }
+    };
+    if (staged)
+        run(sgr, stm);
+    else
+        run(groups + c.group0, terms + t_lo);
     e = warp_sum(e);
     __shared__ double ws[32];
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
