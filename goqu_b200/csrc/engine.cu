@@ -1380,7 +1380,7 @@ struct gq_batch {
 
 namespace {
 
-// Batched tile pass per precision: the same launch shapes as variant 0.
+// Batched tile pass per precision.
 template <class T>
 struct BatchTile;
 template <>
@@ -1389,7 +1389,9 @@ struct BatchTile<double> {
 };
 template <>
 struct BatchTile<float> {
-    static constexpr auto kernel = k_tile_pass_batch<float, 256, 2>;
+    // 3 CTAs of 256 threads per SM (80 registers, a few spilled): measured
+    // 4.8% faster on 4096 QAOA circuits than 2 CTAs with 128 registers
+    static constexpr auto kernel = k_tile_pass_batch<float, 256, 3>;
 };
 
 template <class T>
