@@ -9,14 +9,19 @@ engine's stream. e2e is the public C-ABI call gq_sv_run (Evolve + 1024
 inverse-CDF shots) with the op stream coming from host memory and the sampled
 indices copied back, timed on the host around the call.
 
-Extras (other configurations of the same path, reported in "extras"):
-adjoint gradients of a 20-qubit 400-parameter ansatz against the engine's own
-parameter shift; a noisy 12-qubit density matrix; a batch of 4096 QAOA MaxCut
-circuits (complex64, energies + gradients).
+Extras (N = 1 only; other configurations of the same path and parity checks,
+reported in "extras"): the full 28-qubit circuit against the FP64 oracle
+(complex128 amplitudes and samples, and the complex64 bulk with its error and
+throughput); adjoint gradients of a 20-qubit 400-parameter ansatz against the
+oracle's parameter shift; a noisy 12-qubit density matrix; a batch of 4096
+QAOA MaxCut circuits (complex64, energies + gradients); the 20-qubit
+configuration.
 
 --impl reference times the CPU restatement of goqu's pure-Go path (the oracle,
-threaded like goqu's auto-parallel kernels) on this host's cores, on a bounded
-sample of the same circuit (the first gates of the 2080). Multi-GPU runs
+threaded like goqu's auto-parallel kernels) on this host's cores: each step is
+a stratified sample of the same circuit (one U3 layer, one CNOT layer of each
+parity, the first QFT row and one SWAP, timed gate by gate), and the rate is
+the full circuit's gate count over the class-weighted time. Multi-GPU runs
 (torchrun) are independent replicas, one state per GPU.
 """
 from __future__ import annotations
@@ -148,29 +153,87 @@ def build_workload(n):
     return c, encode.statevector_ops(c), workloads.count_gates(c)
 
 
-def cpu_baseline(n, stream, gates_total, budget_s=20.0):
-    """Oracle (goqu's CPU algorithm restated, threaded like goqu) on the first
-    gates of the same circuit at full size."""
-    import ctypes
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
-    from oracle import binding as orc
-    threads = os.cpu_count() or 1
-    state = orc.zero_state(n)
-    ops = stream.array()
-    done, t_used = 0, 0.0
-    for i in range(len(stream)):
-        one = (type(ops[0]) * 1)(ops[i])
+
+# Stratified CPU sample of the benchmark circuit: per gate class, the first
+# occurrences covering one U3 layer, one CNOT layer of each parity, the first
+# QFT row (H + its controlled phases) and one SWAP.
+def sample_plan(c, n):
+    names = [op.Gate.Name().split("(")[0] for op in c.Ops()
+             if op.Gate is not None and op.Gate.Name() not in ("barrier", "delay")]
+    want = {"U3": n, "CNOT": n - 1, "H": 1, "CP": n - 1, "SWAP": 1}
+    picked, seen = [], {}
+    for i, nm in enumerate(names):
+        k = seen.get(nm, 0)
+        if k < want.get(nm, 0):
+            picked.append(i)
+            seen[nm] = k + 1
+    counts = {nm: names.count(nm) for nm in set(names)}
+    return names, picked, counts
+
+
+class CpuSample:
+    """goqu's CPU path (the oracle, threaded like goqu's GOMAXPROCS workers)
+    timed gate by gate on the stratified sample of the full-size circuit; the
+    full-circuit rate weighs each class's mean gate time by its count."""
+
+    def __init__(self, n, c, stream, threads=None):
+        from oracle import binding as orc
+        self.n, self.stream = n, stream
+        self.threads = threads or os.cpu_count() or 1
+        self.names, self.picked, self.counts = sample_plan(c, n)
+        self.state = orc.zero_state(n)
+        self.ops = stream.array()
+        self._apply(self.picked[0])  # first touch of the state's pages, untimed
+
+    def _apply(self, i):
+        import ctypes
+
+        from oracle import binding as orc
+        one = (type(self.ops[0]) * 1)(self.ops[i])
         t0 = time.perf_counter()
-        rc = orc.lib().or_sv_apply(n, state.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                                   ctypes.cast(one, ctypes.POINTER(type(ops[0]))), 1, threads)
-        t_used += time.perf_counter() - t0
+        rc = orc.lib().or_sv_apply(self.n, self.state.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                   ctypes.cast(one, ctypes.POINTER(type(self.ops[0]))), 1, self.threads)
+        dt = time.perf_counter() - t0
         assert rc == 0
-        done += 1
-        if t_used > budget_s:
-            break
-    return {"value": done / t_used, "unit": "gates/s", "cores": threads, "kind": "port",
-            "sample": f"first {done} of {gates_total} gates at {n} qubits (complex128, {t_used:.1f} s), "
-                      f"oracle threaded like goqu's GOMAXPROCS workers"}
+        return dt
+
+    def step(self):
+        per = {}
+        for i in self.picked:
+            per.setdefault(self.names[i], []).append(self._apply(i))
+        timed = sum(sum(v) for v in per.values())
+        est = sum(self.counts[k] * float(np.mean(v)) for k, v in per.items())
+        return sum(self.counts.values()) / est, timed, {k: len(v) for k, v in per.items()}
+
+    def describe(self, value, timed_s, steps, per):
+        total = sum(self.counts.values())
+        mix = ", ".join(f"{per[k]} {k} of {self.counts[k]}" for k in sorted(per))
+        return {"value": value, "unit": "gates/s", "cores": self.threads, "kind": "port", "cpu_model": cpu_model(),
+                "sample": f"stratified sample of the {total}-gate circuit at {self.n} qubits (complex128), per step "
+                          f"{len(self.picked)} gates ({mix}) timed one by one; rate = {total} gates / sum over "
+                          f"classes of (class gate count x class mean time); {timed_s:.1f} s timed over {steps} "
+                          f"step(s); oracle threaded like goqu's GOMAXPROCS workers",
+                "gates_timed_per_step": len(self.picked), "seconds_timed": timed_s}
+
+
+def cpu_baseline(n, c, stream, steps=3):
+    cs = CpuSample(n, c, stream)
+    vals, timed, per = [], 0.0, None
+    for _ in range(steps):
+        v, t, per = cs.step()
+        vals.append(v)
+        timed += t
+    return cs.describe(float(np.mean(vals)), timed, steps, per)
 
 
 def run_reference(args, world, rank):
@@ -178,20 +241,23 @@ def run_reference(args, world, rank):
         return
     n = args.qubits
     c, stream, gates = build_workload(n)
-    budget = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    cs = CpuSample(n, c, stream)
     for _ in range(args.warmup):
-        cpu_baseline(n, stream, gates, budget_s=min(budget, 3.0))
-    vals, last = [], None
+        cs.step()
+    vals, times, per = [], [], None
     for _ in range(args.steps):
-        last = cpu_baseline(n, stream, gates, budget_s=budget)
-        vals.append(last["value"])
+        v, t, per = cs.step()
+        vals.append(v)
+        times.append(t)
     value = float(np.mean(vals))
     line = {"impl": "reference", "metric": f"{n}q gates/s", "value": value, "unit": "gates/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * gates / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * float(np.mean(times)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload_name(n, "c128"), "qubits": n, "gates": gates, "seed": SEED,
-                       "l2": "state 4 GiB > 126 MB L2 (no flush needed)"},
-            "cpu_baseline": dict(last, value=value),
+                       "l2": "state 4 GiB > 126 MB L2 (no flush needed)",
+                       "step": "one stratified sample of the circuit's gate classes (ms_per_step is its measured "
+                               "time); value is the full-circuit rate those class times give"},
+            "cpu_baseline": cs.describe(value, float(np.sum(times)), args.steps, per),
             "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -231,17 +297,24 @@ def extra_adjoint():
         g_ps[i] = (ep - em) / 2
     ps_wall = time.perf_counter() - t1
     adj_ms = float(np.median(dev))
+    from oracle import gradient as og
+    sel = og.stratified_hea_params(20, 10)
+    g_or = og.parameter_shift(c, names, x, h, sel, threads=os.cpu_count() or 1)
     return {"workload": "adjoint gradient, 20q HEA 10 layers, 400 params, Ising H (39 terms), complex128",
+            "max_abs_diff_vs_oracle_param_shift": float(np.max(np.abs(g_adj[sel] - g_or))),
+            "oracle_sample": f"{len(sel)} parameters: RY and RZ of 2 qubits in each of the 10 layers",
             "adjoint_grads_per_s": 1000.0 / adj_ms, "adjoint_ms_device": adj_ms, "adjoint_ms_wall": wall * 1e3,
             "param_shift_grads_per_s": 1000.0 / ps_dev, "param_shift_ms_device": ps_dev,
             "param_shift_ms_wall": ps_wall * 1e3, "speedup_device": ps_dev / adj_ms,
-            "speedup_wall": ps_wall / wall, "max_abs_diff_vs_param_shift": float(np.max(np.abs(g_adj - g_ps)))}
+            "speedup_wall": ps_wall / wall,
+            "max_abs_diff_vs_engine_param_shift": float(np.max(np.abs(g_adj - g_ps)))}
 
 
 def extra_density():
     """Noisy 12-qubit density matrix: 30 U3 + CNOT brickwork layers,
     depolarizing 1e-3 after every gate, amplitude damping 1e-3 on idle qubits."""
     from goqu_b200 import _abi, densitymatrix, encode, pauli, workloads
+    from oracle import binding as orc
     c, nm = workloads.noisy_brickwork(12, layers=30, seed=12)
     dm = densitymatrix.New(12).WithNoise(nm)
     dm.set_option(_abi.GQ_OPT_TIMING, 1)
@@ -250,31 +323,43 @@ def extra_density():
     lib = _abi.lib()
     for _ in range(2):
         _abi.check(lib.gq_dm_evolve(dm._h, s.ptr(), len(s)))
-    ms = []
+    ms, pms = [], []
     for _ in range(5):
         _abi.check(lib.gq_dm_evolve(dm._h, s.ptr(), len(s)))
         ms.append(dm.stats()["last_ms"])
+        pms.append(dm.stats()["pass_ms"])
     st = dm.stats()
     z = [dm.ExpectPauliString(pauli.ZOn([q], 12)) for q in range(12)]
     tr = dm.Trace()
-    # error against the FP64 oracle (row/column passes and Kraus sums as goqu)
-    # on the same construction at 8 qubits, where the CPU pass takes seconds
-    from oracle import binding as orc
-    c8, nm8 = workloads.noisy_brickwork(8, layers=30, seed=12)
-    s8 = encode.density_ops(c8, nm8)
-    want = orc.dm_evolve(s8)
-    d8 = densitymatrix.New(8).WithNoise(nm8)
-    d8.set_option(_abi.GQ_OPT_JIT, 2)
-    d8.set_option(_abi.GQ_OPT_JIT_MIN_QUBITS, 0)
-    _abi.check(lib.gq_dm_evolve(d8._h, s8.ptr(), len(s8)))
-    terms = [pauli.to_terms(pauli.ZOn([q], 8)) for q in range(8)]
-    z_err = max(abs(d8.ExpectPauliString(pauli.ZOn([q], 8)) - orc.dm_expect_pauli_sum(want, 8, terms[q]).real)
-                for q in range(8))
+    dm.Close()
+    peak, peak_kind = peaks()
+    pass_bytes = 2 * 16 * (1 << 24)  # rho (2^24 complex128 entries) read and written once per pass
+    pass_ms = float(np.median(pms)) / max(1, st["passes"])
+    achieved = pass_bytes / (pass_ms / 1000.0) / 1e9
+
+    def check(n, layers):
+        cc, nn = workloads.noisy_brickwork(n, layers=layers, seed=12)
+        ss = encode.density_ops(cc, nn)
+        want = orc.dm_evolve(ss, threads=os.cpu_count() or 1)
+        d = densitymatrix.New(n).WithNoise(nn)
+        d.set_option(_abi.GQ_OPT_JIT, 2)
+        d.set_option(_abi.GQ_OPT_JIT_MIN_QUBITS, 0)
+        _abi.check(lib.gq_dm_evolve(d._h, ss.ptr(), len(ss)))
+        terms = [pauli.to_terms(pauli.ZOn([q], n)) for q in range(n)]
+        z_err = max(abs(d.ExpectPauliString(pauli.ZOn([q], n)) - orc.dm_expect_pauli_sum(want, n, terms[q]).real)
+                    for q in range(n))
+        out = {"layers": layers, "max_abs_rho_error_vs_fp64_oracle": float(np.max(np.abs(d.DensityMatrix() - want))),
+               "max_abs_z_error_vs_fp64_oracle": z_err,
+               "trace_error_vs_fp64_oracle": abs(d.Trace() - np.trace(want.reshape(1 << n, 1 << n)))}
+        d.Close()
+        return out
+
     return {"workload": "density matrix 12q, 30 noisy U3+CNOT layers (depolarizing + amplitude damping)",
             "ms_device": float(np.median(ms)), "gates": workloads.count_gates(c), "ops_with_channels": len(s),
             "passes": st["passes"], "trace_minus_one": abs(tr - 1.0), "z_expectations": z[:3],
-            "error_check_8q": {"max_abs_rho_error_vs_fp64_oracle": float(np.max(np.abs(d8.DensityMatrix() - want))),
-                               "max_abs_z_error_vs_fp64_oracle": z_err}}
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": pass_bytes, "launch_ms": pass_ms},
+            "error_check_12q": check(12, 2), "error_check_8q": check(8, 30)}
 
 
 def extra_qaoa(qubits=0, count=0, calls=3, graph=True):
@@ -306,22 +391,15 @@ def extra_qaoa(qubits=0, count=0, calls=3, graph=True):
     # gradients against central differences of the oracle energy (each QAOA
     # angle drives every RZZ / RX of its layer, so the +-pi/2 shift rule of a
     # single gate does not apply)
-    from goqu_b200 import circuit as ir, encode, pauli
-    from oracle import binding as orc
-
-    def energy(c, names, h, x):
-        bound = ir.Bind(c, {nm: float(x[i]) for i, nm in enumerate(names)})
-        return orc.expect_pauli_sum(orc.sv_evolve(encode.statevector_ops(bound)), pauli.to_terms(h)).real
-
+    from oracle import gradient as og
+    th = os.cpu_count() or 1
     e_err = g_err = 0.0
     for k in range(0, len(evals), max(1, len(evals) // 16)):
         c, names, h, x = evals[k]
-        e_err = max(e_err, abs(energies[k] - energy(c, names, h, x)))
-        for i in range(len(names)):
-            xp, xm = np.array(x, float), np.array(x, float)
-            xp[i] += 1e-6
-            xm[i] -= 1e-6
-            g_err = max(g_err, abs(grads[k][i] - (energy(c, names, h, xp) - energy(c, names, h, xm)) / 2e-6))
+        x = np.asarray(x, float)
+        e_err = max(e_err, abs(energies[k] - og.energy(c, names, x, h, threads=th)))
+        fd = og.parameter_shift(c, names, x, h, threads=th, shift=1e-6, denom=2e-6)
+        g_err = max(g_err, float(np.max(np.abs(grads[k] - fd))))
     sub = "" if not (qubits or count) else f" (subset: {'n = %d, ' % qubits if qubits else ''}{len(evals)} circuits)"
     return {"workload": "4096 QAOA MaxCut circuits (n 10..20, p 1..4), complex64, energies + gradients" + sub,
             "circuits": len(evals), "circuits_per_s": len(evals) / (ms[-1] / 1000.0), "ms_call_first": ms[0],
@@ -331,6 +409,64 @@ def extra_qaoa(qubits=0, count=0, calls=3, graph=True):
             "passes": st["passes"], "launches": st["kernel_launches"], "host_encode_s": host_s,
             "max_abs_energy_error_vs_fp64_oracle": e_err, "max_abs_grad_error_vs_fp64_central_difference": g_err,
             "error_sample": f"{len(range(0, len(evals), max(1, len(evals) // 16)))} circuits evenly spaced"}
+
+
+def max_abs_diff(a, b, chunk=1 << 24):
+    m = 0.0
+    for k in range(0, a.size, chunk):
+        m = max(m, float(np.max(np.abs(a[k:k + chunk] - b[k:k + chunk]))))
+    return m
+
+
+def extra_parity_28q(n=28, steps=3):
+    """The benchmark circuit itself (40 layers + QFT28, 2080 gates) against the
+    FP64 oracle: complex128 amplitudes and 1024 sampled indices, and the
+    complex64 bulk's throughput, roofline and error against the same state."""
+    import ctypes
+
+    from goqu_b200 import _abi, statevector
+    from oracle import binding as orc
+    c, stream, gates = build_workload(n)
+    u = statevector.uniforms(SHOTS, np.random.default_rng(SEED))
+    peak, peak_kind = peaks()
+    out = {"workload": workload_name(n, "c128") + " (complex128 and complex64)"}
+    got = {}
+    for prec, tag, amp in ((_abi.GQ_C128, "c128", 16), (_abi.GQ_C64, "c64", 8)):
+        sim = statevector.New(n, prec)
+        sim.set_option(_abi.GQ_OPT_TIMING, 1)
+        sim.set_option(_abi.GQ_OPT_JIT, 2)
+        for _ in range(2):
+            sim.evolve_ops(stream)
+        ms, pms, passes = [], [], 0
+        for _ in range(steps):
+            sim.evolve_ops(stream)
+            st = sim.stats()
+            ms.append(st["last_ms"])
+            pms.append(st["pass_ms"])
+            passes += st["passes"]
+        launch_ms = float(np.sum(pms)) / max(1, passes)
+        achieved = 2 * amp * (1 << n) / (launch_ms / 1000.0) / 1e9
+        out[tag] = {"gates_per_s": gates / (float(np.median(ms)) / 1000.0), "ms_device": float(np.median(ms)),
+                    "passes": passes // steps,
+                    "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                 "frac": achieved / peak, "peak_kind": peak_kind, "launch_ms": launch_ms}}
+        if prec == _abi.GQ_C128:
+            got[tag] = sim.StateVector()
+            idx = sim.Sample(u)
+        else:  # kept as complex64 on the host (2 GiB) until the comparison
+            got[tag] = np.empty(1 << n, dtype=np.complex64)
+            _abi.check(_abi.lib().gq_sv_get_state(sim.handle, got[tag].ctypes.data_as(ctypes.c_void_p),
+                                                  got[tag].nbytes))
+        sim.Close()
+    t0 = time.perf_counter()
+    want = orc.sv_evolve(stream, threads=os.cpu_count() or 1)
+    out["oracle_s"] = time.perf_counter() - t0
+    out["c128"]["max_abs_amplitude_error_vs_fp64_oracle"] = max_abs_diff(got["c128"], want)
+    out["c128"]["samples_bit_exact_vs_oracle"] = bool(
+        np.array_equal(idx, orc.sample_fast(orc.probabilities(got["c128"]), u)))
+    del got["c128"]
+    out["c64"]["max_abs_amplitude_error_vs_fp64_oracle"] = max_abs_diff(got["c64"], want)
+    return out
 
 
 def extra_parity():
@@ -453,12 +589,12 @@ def run_gpu(args, world, rank, local):
         "clocks": clk.summary(),
     }
     sim.Close()
-    if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(n, stream, gates, budget_s=args.cpu_seconds)
-    if rank == 0 and not args.no_extras:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(n, c, stream, steps=args.cpu_steps)
+    if rank == 0 and world == 1 and not args.no_extras:
         extras = {}
         for name, fn in (("parity_20q", extra_parity), ("adjoint", extra_adjoint), ("density_matrix", extra_density),
-                         ("qaoa_batch", extra_qaoa)):
+                         ("qaoa_batch", extra_qaoa), ("parity_28q", extra_parity_28q)):
             try:
                 extras[name] = fn()
             except Exception as exc:  # an extra must not hide the headline line
@@ -477,12 +613,12 @@ def main():
     ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
     ap.add_argument("--qubits", type=int, default=28)
     ap.add_argument("--budget", type=int, default=0)
-    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="stratified CPU samples for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--jit", type=int, choices=[0, 1, 2], default=2,
                     help="specialised pass kernels: 0 off, 1 when compiled, 2 wait for them (default)")
-    ap.add_argument("--only-extra", choices=["parity_20q", "adjoint", "density_matrix", "qaoa_batch"],
+    ap.add_argument("--only-extra", choices=["parity_20q", "adjoint", "density_matrix", "qaoa_batch", "parity_28q"],
                     help="run one extra workload alone and print its JSON (profiling)")
     ap.add_argument("--qaoa-qubits", type=int, default=0, help="qaoa_batch: keep the circuits of this size")
     ap.add_argument("--qaoa-count", type=int, default=0, help="qaoa_batch: keep the first N circuits")
@@ -491,6 +627,7 @@ def main():
     args = ap.parse_args()
     if args.only_extra:
         fns = {"parity_20q": extra_parity, "adjoint": extra_adjoint, "density_matrix": extra_density,
+               "parity_28q": extra_parity_28q,
                "qaoa_batch": lambda: extra_qaoa(args.qaoa_qubits, args.qaoa_count, args.qaoa_calls,
                                                 args.qaoa_graph == 1)}
         print(json.dumps({args.only_extra: fns[args.only_extra]()}))

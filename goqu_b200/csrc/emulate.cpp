@@ -584,4 +584,11 @@ int gqx_jit_check_dual(int nq, int precision, const gq_op* ops, size_t n_ops, si
     return GQ_OK;
 }
 
+// The adjoint's checkpoint policy (gq::adjoint_segments) with the device's
+// free memory given by the caller: the same host function the engine calls
+// after cudaMemGetInfo.
+int gqx_adjoint_segments(int requested, int c64, uint64_t n_ops, uint64_t state_bytes, uint64_t avail_bytes) {
+    return gq::adjoint_segments(requested, c64 != 0, (size_t)n_ops, (size_t)state_bytes, (size_t)avail_bytes);
+}
+
 }  // extern "C"

@@ -975,9 +975,11 @@ int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_p
     GQ_TRY(e.adj_grad.ensure(std::max<size_t>(1, n_params) * sizeof(double)));
     e.adj_nparams = (int)n_params;
     // Forward segments (checkpoints bound the drift of un-applying gates).
-    int segs = e.adj_segments;
-    if (segs <= 0) segs = (e.prec == GQ_C64 && n_ops > 256) ? (int)std::min<size_t>(8, n_ops / 128) : 1;
-    segs = std::max(1, std::min<int>(segs, (int)std::max<size_t>(1, n_ops)));
+    // The automatic count only takes the device memory that is free: the
+    // checkpoint buffer's current allocation is released before it grows.
+    size_t mem_free = 0, mem_total = 0;
+    GQ_CUDA(cudaMemGetInfo(&mem_free, &mem_total));
+    const int segs = adjoint_segments(e.adj_segments, e.prec == GQ_C64, n_ops, sbytes, mem_free + e.ckpt.cap);
     std::vector<size_t> bound(segs + 1);
     for (int j = 0; j <= segs; ++j) bound[j] = n_ops * (size_t)j / (size_t)segs;
     if (segs > 1) GQ_TRY(e.ckpt.ensure(sbytes * (segs - 1)));

@@ -13,9 +13,16 @@
 // the Pauli sum to GQ_NOALLOC_MAX_TERMS terms. Host code cannot use the
 // symbol `g_scratch` as a device address, so the address is looked up with
 // cudaGetSymbolAddress once per device, on the first call made with that
-// device current (make that first call before any stream capture). All calls
-// share the array and it keeps the last call's contents: two calls that
-// overlap on the GPU (different streams or threads) race on it.
+// device current, and again only when the device's context has changed (after
+// a cudaDeviceReset, or under another driver-API context). All calls share the
+// array and it keeps the last call's contents: two calls that overlap on the
+// GPU (different streams or threads) race on it.
+//
+// The call is synchronous: it copies the term tables from host memory and
+// waits for its result on `stream`, so it cannot be recorded into a CUDA graph
+// (a stream that is capturing is refused with GQ_EINVAL). The state must be
+// device (or managed) memory of the current device.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -132,7 +139,11 @@ static_assert(kGroupsBytes + kTermsBytes + kPartialBytes <= kScratchBytes, "scra
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void* g_scratch_ptr[kMaxDevices] = {nullptr};
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;  // driver context the address belongs to (0: none yet)
+    void* ptr = nullptr;
+};
+ScratchAddr g_scratch_addr[kMaxDevices];
 std::mutex g_setup_mutex;
 
 int fail(int code, const std::string& msg) {
@@ -140,20 +151,53 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
-// Device address of g_scratch on the current device (looked up once).
-int scratch_address(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail(GQ_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+// Unique id (for the life of the process) of the calling thread's current
+// driver context, 0 when none is current. The two driver functions come
+// through the runtime's entry-point query, so the library needs no link
+// against libcuda.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        cudaDriverEntryPointQueryResult q1, q2;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = (GetCurrent)f1;
+            get_id = (GetId)f2;
+        }
+        cudaGetLastError();
+        looked_up = true;
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of g_scratch in the current device's context: looked up
+// with cudaGetSymbolAddress on the first call on a device and again when that
+// device's current context is not the one the cached address came from.
+int scratch_address(int dev, void** out) {
     if (dev < 0 || dev >= kMaxDevices) return fail(GQ_EINVAL, "device ordinal beyond the supported range");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
+    ScratchAddr& a = g_scratch_addr[dev];
+    const unsigned long long ctx = current_context_id();
+    if (!a.ptr || ctx == 0 || a.ctx_id != ctx) {
         void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess) return fail(GQ_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_ptr[dev] = p;
+        a.ptr = p;
+        a.ctx_id = current_context_id();  // the lookup made the device's context current
     }
-    *out = g_scratch_ptr[dev];
+    *out = a.ptr;
     return GQ_OK;
 }
 
@@ -191,15 +235,40 @@ int gq_expect_pauli_sum_noalloc(const void* device_state, int num_qubits, int pr
         if (ny == 3) pr = 0, pi = -1;
         dt.push_back({t.coeff_re * pr - t.coeff_im * pi, t.coeff_re * pi + t.coeff_im * pr, t.z_mask});
     }
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(GQ_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    // The call copies from host memory and waits for its result: it cannot
+    // be recorded into a graph.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(GQ_EINVAL, std::string("stream capture query failed: ") + cudaGetErrorString(e));
+    }
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(GQ_EINVAL, "gq_expect_pauli_sum_noalloc is synchronous and cannot be called on a capturing stream");
+    // The state must be device memory the current device can address; a host
+    // pointer or another device's allocation would fault the kernel.
+    cudaPointerAttributes attr;
+    e = cudaPointerGetAttributes(&attr, device_state);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(GQ_EINVAL, std::string("device_state is not a CUDA pointer: ") + cudaGetErrorString(e));
+    }
+    if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)
+        return fail(GQ_EINVAL, "device_state is not device memory");
+    if (attr.type == cudaMemoryTypeDevice && attr.device != dev)
+        return fail(GQ_EINVAL, "device_state belongs to device " + std::to_string(attr.device) +
+                                   ", but device " + std::to_string(dev) + " is current");
     void* base = nullptr;
-    int rc = scratch_address(&base);
+    int rc = scratch_address(dev, &base);
     if (rc != GQ_OK) return rc;
     char* sc = (char*)base;
     NGroup* d_groups = (NGroup*)sc;
     NTerm* d_terms = (NTerm*)(sc + kGroupsBytes);
     double2* d_partial = (double2*)(sc + kGroupsBytes + kTermsBytes);
-    cudaStream_t s = (cudaStream_t)stream;
-    cudaError_t e = cudaSuccess;
     if (!groups.empty()) e = cudaMemcpyAsync(d_groups, groups.data(), sizeof(NGroup) * groups.size(), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && !dt.empty())
         e = cudaMemcpyAsync(d_terms, dt.data(), sizeof(NTerm) * dt.size(), cudaMemcpyHostToDevice, s);

@@ -1131,4 +1131,23 @@ int adjoint_gates(int nq, const gq_op* ops, size_t n_ops, size_t n_params, std::
     return GQ_OK;
 }
 
+int adjoint_segments(int requested, bool c64, size_t n_ops, size_t state_bytes, size_t avail_bytes) {
+    const int most = (int)std::max<size_t>(1, n_ops);
+    if (requested > 0) return std::min(requested, most);
+    // Un-applying gates in FP32 drifts: complex64 circuits of more than 256
+    // ops restart the reverse sweep from a stored forward state every 128 ops,
+    // up to 8 segments. complex128 circuits need none.
+    int segs = (c64 && n_ops > 256) ? (int)std::min<size_t>(8, n_ops / 128) : 1;
+    segs = std::max(1, std::min(segs, most));
+    // The (segs - 1) checkpoint copies must fit in the memory left for them,
+    // keeping kAdjointHeadroom for the program and reduction buffers; with too
+    // little room take fewer segments, down to none.
+    if (segs > 1 && state_bytes > 0) {
+        const size_t usable = avail_bytes > kAdjointHeadroom ? avail_bytes - kAdjointHeadroom : 0;
+        const size_t fit = usable / state_bytes;
+        segs = (int)std::min<size_t>((size_t)segs, fit + 1);
+    }
+    return std::max(1, segs);
+}
+
 }  // namespace gq

@@ -82,5 +82,12 @@ int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, 
 // receives, per forward gate, the op index it came from (for checkpoints).
 int adjoint_gates(int nq, const gq_op* ops, size_t n_ops, size_t n_params, std::vector<NGate>& forward,
                   std::vector<NGate>& reverse, std::vector<int>& fwd_op, std::vector<int>& rev_op, std::string& err);
+// Forward checkpoints of an adjoint gradient. requested > 0 (the caller's
+// GQ_OPT_ADJOINT_SEGMENTS) is kept, capped at the op count. Automatic (0):
+// complex64 circuits of more than 256 ops take one segment per 128 ops (at most
+// 8), others none; the count is then cut so that the (segments - 1) stored
+// states of state_bytes fit in avail_bytes less kAdjointHeadroom, down to 1.
+constexpr size_t kAdjointHeadroom = size_t(256) << 20;
+int adjoint_segments(int requested, bool c64, size_t n_ops, size_t state_bytes, size_t avail_bytes);
 
 }  // namespace gq

@@ -289,9 +289,13 @@ int gq_batch_stats(const gq_batch* b, gq_stats* out);
  * device_state) on `stream` (a cudaStream_t, NULL for the default stream).
  * Its scratch is a 256 KiB array compiled into the library, so at most
  * GQ_NOALLOC_MAX_TERMS terms are accepted (larger sums return GQ_EINVAL).
- * The first call on a device looks up the array's device address; make it
- * before any stream capture. Calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller.                             */
+ * The first call on a device looks up the array's device address (again after
+ * the device's context changes). The call is synchronous: it copies the term
+ * tables from host memory and waits for the result, so it cannot be captured
+ * into a CUDA graph, and a capturing `stream` is refused with GQ_EINVAL, as is
+ * a device_state that is not device (or managed) memory of the current
+ * device. Calls share the array: calls that overlap on the GPU race and must
+ * be serialised by the caller.                                               */
 #define GQ_NOALLOC_MAX_TERMS 2048
 int gq_expect_pauli_sum_noalloc(const void* device_state, int num_qubits, int precision,
                                 const gq_pauli_term* terms, size_t n_terms, void* stream,

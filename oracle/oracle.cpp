@@ -588,13 +588,27 @@ void dm_channel(DM& s, const gq_op& op) {
         return;
     }
     long long n = s.dim * s.dim;
-    std::vector<cd> temp(n, cd{0.0, 0.0}), saved(s.rho, s.rho + n);
+    // goqu runs the restore, accumulate and final copy loops serially; in the
+    // threaded mode they are split across workers. Each element's additions
+    // are the same in the same order, so the result is bit-identical.
+    const int w = s.par() ? s.workers() : 1;
+    std::vector<cd> temp(n), saved(n);
+    parallel_chunks(n, w, [&](long long a, long long b) {
+        std::memcpy(saved.data() + a, s.rho + a, (b - a) * sizeof(cd));
+        for (long long i = a; i < b; ++i) temp[i] = cd{0.0, 0.0};
+    });
     for (int e = 0; e < op.num_kraus; ++e) {
-        std::memcpy(s.rho, saved.data(), n * sizeof(cd));
+        parallel_chunks(n, w, [&](long long a, long long b) {
+            std::memcpy(s.rho + a, saved.data() + a, (b - a) * sizeof(cd));
+        });
         dm_gate(s, op.qubits, k, kraus + e * kd * kd);
-        for (long long i = 0; i < n; ++i) temp[i] = add(temp[i], s.rho[i]);
+        parallel_chunks(n, w, [&](long long a, long long b) {
+            for (long long i = a; i < b; ++i) temp[i] = add(temp[i], s.rho[i]);
+        });
     }
-    std::memcpy(s.rho, temp.data(), n * sizeof(cd));
+    parallel_chunks(n, w, [&](long long a, long long b) {
+        std::memcpy(s.rho + a, temp.data() + a, (b - a) * sizeof(cd));
+    });
 }
 
 }  // namespace

@@ -238,3 +238,28 @@ def test_qaoa_layers_fuse_into_pair_sums(emu):
             xm[i] -= 1e-5
             fd = (_oracle_energy(c, names, xp, h) - _oracle_energy(c, names, xm, h)) / 2e-5
             assert abs(g[i] - fd) < 1e-6
+
+
+def test_adjoint_checkpoints_fit_free_memory(emu):
+    """The automatic checkpoint count of the adjoint (engine: after
+    cudaMemGetInfo) never asks for more stored states than the free memory
+    holds: a 33-qubit complex64 circuit of 2000 ops wants 8 segments, i.e. 7
+    stored 64 GiB states, and gets what fits, down to none."""
+    f = emu.gqx_adjoint_segments
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]
+    gib = 1 << 30
+    head = 256 << 20  # kept free for program and reduction buffers
+    s33 = 64 * gib  # one 33-qubit complex64 state
+    assert f(0, 1, 2000, s33, 1000 * gib) == 8
+    assert f(0, 1, 2000, s33, 3 * s33 + head) == 4  # three stored states fit
+    assert f(0, 1, 2000, s33, 3 * s33 + head - 1) == 3
+    assert f(0, 1, 2000, s33, s33) == 1  # no room: no checkpoints, no failure
+    assert f(0, 1, 2000, s33, 0) == 1
+    # complex128 and short circuits take none; small states are unaffected
+    assert f(0, 0, 2000, s33, 1000 * gib) == 1
+    assert f(0, 1, 256, 1 << 20, 1000 * gib) == 1
+    assert f(0, 1, 600, 1 << 20, 8 * gib) == 4
+    # an explicit request is kept (capped at the op count only)
+    assert f(5, 1, 2000, s33, 0) == 5
+    assert f(5, 0, 3, s33, 0) == 3
