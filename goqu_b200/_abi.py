@@ -54,6 +54,7 @@ GQ_OPT_JIT = 9
 GQ_OPT_JIT_MIN_QUBITS = 10
 GQ_OPT_JIT_MIN_BLOCKS = 11
 GQ_OPT_JIT_PERSISTENT = 12
+GQ_OPT_DM_DENSE_CHANNELS = 13
 
 GQ_NOALLOC_MAX_TERMS = 2048
 

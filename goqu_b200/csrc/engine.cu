@@ -686,6 +686,7 @@ struct gq_sv {
 struct gq_dm {
     Engine e;
     int nq = 0;
+    bool dense_channels = false;  // GQ_OPT_DM_DENSE_CHANNELS
 };
 
 extern "C" {
@@ -1077,7 +1078,7 @@ static int dm_apply_impl(gq_dm* dm, const gq_op* ops, size_t n_ops) {
     std::vector<NGate> gates;
     {
         std::string err;
-        int rc = dm_gates(dm->nq, ops, n_ops, gates, err);
+        int rc = dm_gates(dm->nq, ops, n_ops, gates, err, !dm->dense_channels);
         if (rc != GQ_OK) return fail(rc, err);
     }
     return dm->e.run_gates(gates);
@@ -1121,6 +1122,10 @@ int gq_dm_set_option(gq_dm* dm, int key, int64_t value) {
     if (key == GQ_OPT_JIT || key == GQ_OPT_JIT_MIN_QUBITS || key == GQ_OPT_JIT_MIN_BLOCKS ||
         key == GQ_OPT_JIT_PERSISTENT)
         return dm->e.set_jit_option(key, value);
+    if (key == GQ_OPT_DM_DENSE_CHANNELS) {
+        dm->dense_channels = value != 0;
+        return GQ_OK;
+    }
     return fail(GQ_EINVAL, "unknown option");
 }
 

@@ -905,6 +905,71 @@ std::vector<Z> unitary_superop(const std::vector<Z>& u, int k) {
     return superop(u.data(), 1, k);
 }
 
+// A channel superoperator S (4^k x 4^k, index (a << k) | b for the row
+// pattern a and column pattern b) is in population / coherence form when it
+// maps the populations rho[a,a] only among themselves, by
+// T[a][a'] = S[(a,a),(a',a')], and scales each coherence rho[a,b], a != b, by
+// D[(a,b)] = S[(a,b),(a,b)]. Depolarizing (1q: T = (1-2p/3) I + (2p/3) X on the
+// populations, coherences x (1-4p/3); 2q: T = (1-16p/15) I + (4p/15) J,
+// coherences x (1-16p/15)), amplitude damping and phase damping have it, with
+// the other entries exactly zero in the FP64 sum over Kraus operators.
+bool population_coherence(const std::vector<Z>& S, int k, std::vector<Z>& T, std::vector<Z>& D) {
+    const int d = 1 << k, dd = d * d;
+    for (int R = 0; R < dd; ++R)
+        for (int C = 0; C < dd; ++C) {
+            if (R == C || (S[R * dd + C].re == 0.0 && S[R * dd + C].im == 0.0)) continue;
+            const int a = R >> k, b = R & (d - 1), a2 = C >> k, b2 = C & (d - 1);
+            if (!(a == b && a2 == b2)) return false;
+        }
+    T.assign(d * d, Z{0, 0});
+    D.assign(dd, Z{1, 0});
+    for (int a = 0; a < d; ++a)
+        for (int a2 = 0; a2 < d; ++a2) T[a * d + a2] = S[((a << k) | a) * dd + ((a2 << k) | a2)];
+    for (int R = 0; R < dd; ++R)
+        if ((R >> k) != (R & (d - 1))) D[R] = S[R * dd + R];
+    return true;
+}
+
+// Emits a population / coherence channel on row qubits rq and column qubits
+// cq as cheap ops instead of a dense superoperator. With
+// V = prod_i X(c_i) CNOT(r_i -> c_i), which maps |a, b> to |a, b ^ a ^ 1..1>
+// and is its own inverse, S = V S'' V where S'' scales (a, b'') by
+// D[(a, b'' ^ a ^ 1..1)] for b'' != 1..1 (a diagonal) and applies T to the
+// row qubits where every column qubit is 1 (T controlled by the c_i). The
+// CNOTs and X are permutations, the diagonal a pending factor; only T does
+// arithmetic, on a 2^-k share of the entries.
+int emit_population_coherence(const std::vector<Z>& T, const std::vector<Z>& D, const std::vector<int>& rq,
+                              const std::vector<int>& cq, int src, std::vector<NGate>& out, std::string& err) {
+    const int k = (int)rq.size(), d = 1 << k, dd = d * d;
+    const std::vector<Z> cnot = {Z{1, 0}, Z{0, 0}, Z{0, 0}, Z{0, 0}, Z{0, 0}, Z{1, 0}, Z{0, 0}, Z{0, 0},
+                                 Z{0, 0}, Z{0, 0}, Z{0, 0}, Z{1, 0}, Z{0, 0}, Z{0, 0}, Z{1, 0}, Z{0, 0}};
+    const std::vector<Z> x = {Z{0, 0}, Z{1, 0}, Z{1, 0}, Z{0, 0}};
+    auto emit_v = [&]() {
+        for (int i = 0; i < k; ++i) {
+            int rc = analyze_matrix(cnot, {rq[i], cq[i]}, 0, src, out, err);
+            if (rc == GQ_OK) rc = analyze_matrix(x, {cq[i]}, 0, src, out, err);
+            if (rc != GQ_OK) return rc;
+        }
+        return (int)GQ_OK;
+    };
+    int rc = emit_v();
+    if (rc != GQ_OK) return rc;
+    std::vector<Z> diag(dd * dd, Z{0, 0});
+    for (int a = 0; a < d; ++a)
+        for (int b2 = 0; b2 < d; ++b2) {
+            const int R = (a << k) | b2;
+            diag[R * dd + R] = b2 == d - 1 ? Z{1, 0} : D[(a << k) | (b2 ^ a ^ (d - 1))];
+        }
+    std::vector<int> all(rq);
+    all.insert(all.end(), cq.begin(), cq.end());
+    rc = analyze_matrix(diag, all, 0, src, out, err);
+    uint64_t cmask = 0;
+    for (int c : cq) cmask |= 1ull << c;
+    if (rc == GQ_OK) rc = analyze_matrix(T, rq, cmask, src, out, err);
+    if (rc == GQ_OK) rc = emit_v();
+    return rc;
+}
+
 std::vector<Z> full_controlled(const gq_op& op) {
     const int tot = op.num_qubits, nt = op.num_qubits - op.num_controls;
     const int dim = 1 << tot, inner = 1 << nt, start = dim - inner;
@@ -918,7 +983,7 @@ std::vector<Z> full_controlled(const gq_op& op) {
 
 }  // namespace
 
-int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, std::string& err) {
+int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, std::string& err, bool structured) {
     auto vec_qubits = [&](const gq_op& op) {
         std::vector<int> q;
         for (int i = 0; i < op.num_qubits; ++i) q.push_back(op.qubits[i] + nq);  // row qubits
@@ -944,10 +1009,20 @@ int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, 
             continue;
         }
         if (!op.matrix) { err = "op " + std::to_string(i) + ": no matrix"; return GQ_EINVAL; }
-        std::vector<Z> sop;
+        std::vector<int> rq, cq;  // row and column vector qubits of the op
+        for (int j = 0; j < k; ++j) {
+            rq.push_back(op.qubits[j] + nq);
+            cq.push_back(op.qubits[j]);
+        }
+        std::vector<Z> sop, pop_t, coh_d;
         if (op.kind == GQ_OP_CHANNEL) {
             if (op.num_kraus < 1) { err = "channel without Kraus operators"; return GQ_EINVAL; }
             sop = superop((const Z*)op.matrix, op.num_kraus, k);
+            if (structured && k <= 2 && population_coherence(sop, k, pop_t, coh_d)) {
+                int rc = emit_population_coherence(pop_t, coh_d, rq, cq, (int)i, gates, err);
+                if (rc != GQ_OK) { err = "op " + std::to_string(i) + ": " + err; return rc; }
+                continue;
+            }
         } else {
             std::vector<Z> u;
             if (op.kind == GQ_OP_CONTROLLED)
@@ -957,22 +1032,24 @@ int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, 
             const bool fold = k <= 2 && i + 1 < n_ops && ops[i + 1].kind == GQ_OP_CHANNEL &&
                               ops[i + 1].num_qubits == k && std::equal(ops[i + 1].qubits, ops[i + 1].qubits + k, op.qubits) &&
                               ops[i + 1].matrix && ops[i + 1].num_kraus >= 1;
-            if (fold) {
+            std::vector<Z> chan;
+            if (fold) chan = superop((const Z*)ops[i + 1].matrix, ops[i + 1].num_kraus, k);
+            if (fold && !(structured && population_coherence(chan, k, pop_t, coh_d))) {
                 // The channel that follows on the same qubits folds into one
                 // superoperator S * (U (x) conj(U)).
-                sop = matmul(superop((const Z*)ops[i + 1].matrix, ops[i + 1].num_kraus, k), unitary_superop(u, k), d * d);
+                sop = matmul(chan, unitary_superop(u, k), d * d);
                 ++i;
             } else {
-                // U on the row qubits, conj(U) on the column qubits.
-                std::vector<int> rq, cq;
-                for (int j = 0; j < k; ++j) {
-                    rq.push_back(op.qubits[j] + nq);
-                    cq.push_back(op.qubits[j]);
-                }
+                // U on the row qubits, conj(U) on the column qubits, then the
+                // following channel's cheap population / coherence form.
                 std::vector<Z> uc(u);
                 for (auto& z : uc) z.im = -z.im;
                 int rc = analyze_matrix(u, rq, 0, (int)i, gates, err);
                 if (rc == GQ_OK) rc = analyze_matrix(uc, cq, 0, (int)i, gates, err);
+                if (rc == GQ_OK && fold) {
+                    rc = emit_population_coherence(pop_t, coh_d, rq, cq, (int)(i + 1), gates, err);
+                    ++i;
+                }
                 if (rc != GQ_OK) { err = "op " + std::to_string(i) + ": " + err; return rc; }
                 continue;
             }

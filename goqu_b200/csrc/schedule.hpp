@@ -73,8 +73,13 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
 // Density matrix ops -> NGates on the 2n-qubit vectorised rho (row qubit q is
 // vector bit q+n, column qubit q is bit q): U on rows and conj(U) on columns,
 // channels as sum_k E_k (x) conj(E_k), a gate and the channel that follows it
-// on the same qubits folded into one superoperator.
-int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, std::string& err);
+// on the same qubits folded into one superoperator. With `structured`, a
+// channel whose superoperator only mixes populations among themselves and
+// scales coherences (depolarizing, amplitude and phase damping) is applied
+// after its gate as permutations, a diagonal and the population map on a
+// 2^-k share of the entries instead.
+int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, std::string& err,
+             bool structured = true);
 // Adjoint differentiation: `forward` are the gates of `ops`; `reverse` is the
 // reverse sweep: for each op from last to first, one K_GRAD gate per
 // parameter it depends on (G = dU/dtheta * U^dagger, zero where its controls

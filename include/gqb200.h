@@ -206,6 +206,11 @@ int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 #define GQ_OPT_JIT_MIN_QUBITS 10 /* smallest state (physical qubits) that uses them (default 20) */
 #define GQ_OPT_JIT_MIN_BLOCKS 11 /* their CTAs per SM (register bound); 0 = the launch shape's */
 #define GQ_OPT_JIT_PERSISTENT 12 /* 1: persistent CTAs prefetching the next tile; 0: one CTA per tile (default) */
+/* Density matrices: channels that only mix populations and scale coherences
+ * (depolarizing, amplitude and phase damping) run as permutations, a
+ * diagonal and the population map (default 0); 1 folds every channel into a
+ * dense superoperator with the gate before it. */
+#define GQ_OPT_DM_DENSE_CHANNELS 13
 int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
 
 /* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */

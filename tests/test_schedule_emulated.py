@@ -116,6 +116,26 @@ def test_emulated_density_matrix_matches_oracle(emu, n, seed, tile):
     np.testing.assert_allclose(got, want, atol=1e-12, rtol=0)
 
 
+@pytest.mark.parametrize("kind", ["depol", "amp", "phase", "gad", "thermal", "bitflip", "phaseflip"])
+def test_emulated_density_matrix_channel_kinds(emu, kind):
+    # population / coherence channels (depolarizing, amplitude, phase and
+    # generalized amplitude damping, thermal relaxation, phase flip) take the
+    # structured form after their gate; bit flip mixes coherences and keeps
+    # the dense superoperator. Both against goqu's Kraus sums.
+    from goqu_b200 import noise as N
+    ch1 = {"depol": N.Depolarizing1Q(0.07), "amp": N.AmplitudeDamping(0.2), "phase": N.PhaseDamping(0.15),
+           "gad": N.GeneralizedAmplitudeDamping(0.3, 0.2), "thermal": N.ThermalRelaxation(50.0, 40.0, 7.0),
+           "bitflip": N.BitFlip(0.1), "phaseflip": N.PhaseFlip(0.1)}[kind]
+    c = random_circuit(5, 40, 17, allow_3q=False, allow_ctrl=False, allow_reset=True)
+    nm = N.New()
+    nm.AddDefaultError(1, ch1)
+    nm.AddDefaultError(2, N.Depolarizing2Q(0.05) if kind != "bitflip" else N.Custom(
+        "bf2", 2, [np.kron(np.reshape(k1, (2, 2)), np.reshape(k2, (2, 2))) for k1 in N.BitFlip(0.1).Kraus()
+                   for k2 in N.BitFlip(0.2).Kraus()]))
+    ops = encode.density_ops(c, nm)
+    np.testing.assert_allclose(_emu_dm(emu, ops), orc.dm_evolve(ops), atol=1e-12, rtol=0)
+
+
 def test_emulated_noisy_brickwork(emu):
     from goqu_b200 import workloads
     c, nm = workloads.noisy_brickwork(5, layers=4, seed=1)
