@@ -149,6 +149,8 @@ SIGNATURES = {
     "gq_sv_probabilities": (_I, [_VP, _DBL_P, _SZ]),
     "gq_sv_sample": (_I, [_VP, _DBL_P, _SZ, _U64P]),
     "gq_sv_run": (_I, [_VP, _OPP, _SZ, _DBL_P, _SZ, _U64P]),
+    "gq_sv_sample_counts": (_I, [_VP, _DBL_P, _SZ, _U64P, _U64P, ctypes.POINTER(_SZ)]),
+    "gq_sv_run_counts": (_I, [_VP, _OPP, _SZ, _DBL_P, _SZ, _U64P, _U64P, ctypes.POINTER(_SZ)]),
     "gq_sv_expect_pauli_sum": (_I, [_VP, _TP, _SZ, _DBL_P, _DBL_P]),
     "gq_sv_expect_z_mask": (_I, [_VP, ctypes.c_uint64, _DBL_P]),
     "gq_sv_adjoint_gradient": (_I, [_VP, _OPP, _SZ, _TP, _SZ, _SZ, _DBL_P, _DBL_P]),
@@ -171,6 +173,7 @@ SIGNATURES = {
     "gq_dm_purity": (_I, [_VP, _DBL_P]),
     "gq_dm_fidelity": (_I, [_VP, _DBL_P, _SZ, _DBL_P]),
     "gq_dm_sample": (_I, [_VP, _DBL_P, _DBL_P, _DBL_P, _SZ, _U64P]),
+    "gq_dm_sample_counts": (_I, [_VP, _DBL_P, _DBL_P, _DBL_P, _SZ, _U64P, _U64P, ctypes.POINTER(_SZ)]),
     "gq_dm_prob0": (_I, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "gq_dm_collapse": (_I, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
     "gq_dm_measure": (_I, [_VP, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),

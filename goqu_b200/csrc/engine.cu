@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/gqb200.h"
+#include "counts.cuh"
 #include "kernels.cuh"
 #include "jit.hpp"
 #include "schedule.hpp"
@@ -193,6 +194,7 @@ struct Engine {
     cudaStream_t stream = nullptr;
     DevBuf state, prog, scratch, scratch2, aux;
     DevBuf lam, ckpt, adj_partial, adj_grad;  // adjoint differentiation
+    DevBuf hist;                              // shot histograms (counts.cuh)
     int adj_nparams = 0;                      // parameters of the current gradient
     int adj_segments = 0;                     // forward checkpoints (0: automatic)
     PinnedBuf staging, hostio;
@@ -253,6 +255,7 @@ struct Engine {
         ckpt.release();
         adj_partial.release();
         adj_grad.release();
+        hist.release();
         staging.release();
         hostio.release();
         if (staged) cudaEventDestroy(staged);
@@ -626,12 +629,69 @@ struct Engine {
         return GQ_OK;
     }
 
+    // ---- shot histograms ---------------------------------------------------
+    struct CountsOut {
+        uint64_t* outcomes;
+        uint64_t* counts;
+        size_t* n_distinct;
+        int key_bits;  // significant bits of an outcome index
+    };
+
+    // The distinct values of the `shots` indices at d_idx (device) with their
+    // counts, in increasing order, copied to the caller's host arrays.
+    int counts_impl(uint64_t* d_idx, size_t shots, const CountsOut& co) {
+        const uint64_t n = shots;
+        const uint32_t ntiles = (uint32_t)((n + kHistTile - 1) / kHistTile);
+        const uint64_t ncounts = 256ull * ntiles;
+        const size_t o_alt = 0, o_cnt = align16(n * 8), o_flag = o_cnt + align16(ncounts * 4);
+        const size_t o_start = o_flag + align16(n * 4), o_out = o_start + align16(n * 8);
+        const size_t o_num = o_out + align16(n * 8), o_total = o_num + align16(n * 8);
+        GQ_TRY(hist.ensure(o_total + 16));
+        char* h = (char*)hist.p;
+        uint64_t* src = d_idx;
+        uint64_t* dst = (uint64_t*)(h + o_alt);
+        uint32_t* cnt = (uint32_t*)(h + o_cnt);
+        for (int shift = 0; shift < co.key_bits; shift += 8) {
+            k_radix_counts<<<ntiles, kHistThreads, 0, stream>>>(src, n, shift, ntiles, cnt);
+            k_scan_u32<<<1, 1024, 0, stream>>>(cnt, ncounts, nullptr);
+            k_radix_scatter<<<ntiles, kHistThreads, 0, stream>>>(src, n, shift, ntiles, cnt, dst);
+            std::swap(src, dst);
+            stats.kernel_launches += 3;
+        }
+        uint32_t* flag = (uint32_t*)(h + o_flag);
+        uint32_t* total = (uint32_t*)(h + o_total);
+        const unsigned g = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)reduce_grid());
+        k_run_flags<<<g, 256, 0, stream>>>(src, n, flag);
+        k_scan_u32<<<1, 1024, 0, stream>>>(flag, n, total);
+        k_run_starts<<<g, 256, 0, stream>>>(src, n, flag, (uint64_t*)(h + o_out), (uint64_t*)(h + o_start));
+        k_run_counts<<<g, 256, 0, stream>>>((const uint64_t*)(h + o_start), n, total, (uint64_t*)(h + o_num));
+        GQ_CUDA(cudaGetLastError());
+        stats.kernel_launches += 4;
+        GQ_TRY(hostio.ensure(64));
+        GQ_CUDA(cudaMemcpyAsync(hostio.p, total, 4, cudaMemcpyDeviceToHost, stream));
+        GQ_CUDA(cudaStreamSynchronize(stream));
+        const size_t nd = *(const uint32_t*)hostio.p;
+        if (nd) {
+            GQ_CUDA(cudaMemcpyAsync(co.outcomes, h + o_out, nd * 8, cudaMemcpyDeviceToHost, stream));
+            GQ_CUDA(cudaMemcpyAsync(co.counts, h + o_num, nd * 8, cudaMemcpyDeviceToHost, stream));
+            GQ_CUDA(cudaStreamSynchronize(stream));
+        }
+        *co.n_distinct = nd;
+        stats.d2h_bytes += (int64_t)(4 + 16 * nd);
+        return GQ_OK;
+    }
+
     // ---- sampling --------------------------------------------------------
     // Exact inverse-CDF sampling (see k_chunk_steps in kernels.cuh). The
-    // exact chunk-end sums are cached until the state changes.
+    // exact chunk-end sums are cached until the state changes. With `co`,
+    // the indices stay on the device and become (outcome, count) pairs.
     template <class P>
-    int sample_impl(P prob, uint64_t n, const double* uniforms, size_t shots, uint64_t* idx_out) {
-        if (shots == 0) return GQ_OK;
+    int sample_impl(P prob, uint64_t n, const double* uniforms, size_t shots, uint64_t* idx_out,
+                    const CountsOut* co = nullptr) {
+        if (shots == 0) {
+            if (co) *co->n_distinct = 0;
+            return GQ_OK;
+        }
         const int chunk_log = n >= 2048 ? 11 : (int)std::max<uint64_t>(0, (uint64_t)std::log2((double)n));
         const uint64_t nchunks = (n + (1ull << chunk_log) - 1) >> chunk_log;
         // scratch: sums | incl | ends | steps | cexp | clean | n_seq
@@ -661,6 +721,7 @@ struct Engine {
             prob, n, chunk_log, ends, nchunks, (const double*)(d + o_u), shots, (uint64_t*)(d + o_out));
         GQ_CUDA(cudaGetLastError());
         stats.kernel_launches += 5;
+        if (co) return counts_impl((uint64_t*)(d + o_out), shots, *co);
         stats.d2h_bytes += (int64_t)(shots * 8);
         GQ_CUDA(cudaMemcpyAsync(idx_out, d + o_out, shots * 8, cudaMemcpyDeviceToHost, stream));
         GQ_CUDA(cudaStreamSynchronize(stream));
@@ -825,6 +886,27 @@ int gq_sv_sample(gq_sv* sv, const double* uniforms, size_t shots, uint64_t* idx_
 int gq_sv_run(gq_sv* sv, const gq_op* ops, size_t n_ops, const double* uniforms, size_t shots, uint64_t* idx_out) {
     GQ_TRY(gq_sv_evolve(sv, ops, n_ops));  // resets the counters of this call
     return gq_sv_sample(sv, uniforms, shots, idx_out);
+}
+
+int gq_sv_sample_counts(gq_sv* sv, const double* uniforms, size_t shots, uint64_t* outcomes_out, uint64_t* counts_out,
+                        size_t* n_distinct) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    if (!n_distinct || (shots && (!uniforms || !outcomes_out || !counts_out))) return fail(GQ_EINVAL, "null argument");
+    if (shots > 0xffffffffull) return fail(GQ_EINVAL, "more than 2^32 - 1 shots");
+    for (size_t i = 0; i < shots; ++i)
+        if (!(uniforms[i] >= 0.0 && uniforms[i] < 1.0)) return fail(GQ_EINVAL, "uniform outside [0, 1)");
+    const uint64_t na = 1ull << sv->nq;
+    Engine& e = sv->e;
+    const Engine::CountsOut co{outcomes_out, counts_out, n_distinct, sv->nq};
+    if (e.prec == GQ_C64)
+        return e.sample_impl(ProbState<float>{(const cplx<float>*)e.state.p}, na, uniforms, shots, nullptr, &co);
+    return e.sample_impl(ProbState<double>{(const cplx<double>*)e.state.p}, na, uniforms, shots, nullptr, &co);
+}
+
+int gq_sv_run_counts(gq_sv* sv, const gq_op* ops, size_t n_ops, const double* uniforms, size_t shots,
+                     uint64_t* outcomes_out, uint64_t* counts_out, size_t* n_distinct) {
+    GQ_TRY(gq_sv_evolve(sv, ops, n_ops));  // resets the counters of this call
+    return gq_sv_sample_counts(sv, uniforms, shots, outcomes_out, counts_out, n_distinct);
 }
 
 int gq_sv_expect_pauli_sum(gq_sv* sv, const gq_pauli_term* terms, size_t n_terms, double* out_re, double* out_im) {
@@ -1215,10 +1297,8 @@ int gq_dm_fidelity(gq_dm* dm, const double* psi, size_t n, double* out) {
     return GQ_OK;
 }
 
-int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* uniforms, size_t shots,
-                 uint64_t* idx_out) {
-    if (!dm) return fail(GQ_EINVAL, "null handle");
-    if (shots && (!uniforms || !idx_out)) return fail(GQ_EINVAL, "null argument");
+static int dm_sample_impl(gq_dm* dm, const double* p01, const double* p10, const double* uniforms, size_t shots,
+                          uint64_t* idx_out, const Engine::CountsOut* co) {
     for (size_t i = 0; i < shots; ++i)
         if (!(uniforms[i] >= 0.0 && uniforms[i] < 1.0)) return fail(GQ_EINVAL, "uniform outside [0, 1)");
     Engine& e = dm->e;
@@ -1235,7 +1315,23 @@ int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* 
             std::swap(a, b);
         }
     GQ_CUDA(cudaGetLastError());
-    return e.sample_impl(ProbArray{a}, dim, uniforms, shots, idx_out);
+    return e.sample_impl(ProbArray{a}, dim, uniforms, shots, idx_out, co);
+}
+
+int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* uniforms, size_t shots,
+                 uint64_t* idx_out) {
+    if (!dm) return fail(GQ_EINVAL, "null handle");
+    if (shots && (!uniforms || !idx_out)) return fail(GQ_EINVAL, "null argument");
+    return dm_sample_impl(dm, p01, p10, uniforms, shots, idx_out, nullptr);
+}
+
+int gq_dm_sample_counts(gq_dm* dm, const double* p01, const double* p10, const double* uniforms, size_t shots,
+                        uint64_t* outcomes_out, uint64_t* counts_out, size_t* n_distinct) {
+    if (!dm) return fail(GQ_EINVAL, "null handle");
+    if (!n_distinct || (shots && (!uniforms || !outcomes_out || !counts_out))) return fail(GQ_EINVAL, "null argument");
+    if (shots > 0xffffffffull) return fail(GQ_EINVAL, "more than 2^32 - 1 shots");
+    const Engine::CountsOut co{outcomes_out, counts_out, n_distinct, dm->nq};
+    return dm_sample_impl(dm, p01, p10, uniforms, shots, nullptr, &co);
 }
 
 int gq_dm_prob0(gq_dm* dm, int qubit, double* p0) {

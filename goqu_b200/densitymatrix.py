@@ -16,7 +16,7 @@ import numpy as np
 from . import _abi
 from . import encode as _encode
 from . import pauli as _pauli
-from .statevector import _round14, counts_from_indices, uniforms
+from .statevector import _round14, counts_from_pairs, sample_counts_call, uniforms
 
 _D = ctypes.POINTER(ctypes.c_double)
 _U64 = ctypes.POINTER(ctypes.c_uint64)
@@ -75,7 +75,7 @@ class Sim:
             from . import dynamic
             return dynamic.run_dynamic_dm(self, c, shots, rng)
         self.Evolve(c)
-        return counts_from_indices(self.Sample(uniforms(shots, rng)), self._n)
+        return counts_from_pairs(*self.SampleCounts(uniforms(shots, rng)), self._n)
 
     def _readout_arrays(self):
         p01 = np.full(self._n, -1.0)
@@ -86,6 +86,14 @@ class Sim:
                 if re is not None:
                     p01[q], p10[q] = re.P01, re.P10
         return p01, p10
+
+    def SampleCounts(self, u):
+        """Distinct outcomes of the readout-mixed sampling and their counts,
+        histogrammed on the device."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        p01, p10 = self._readout_arrays()
+        return sample_counts_call(_abi.lib().gq_dm_sample_counts, u.size, self._h, p01.ctypes.data_as(_D),
+                                  p10.ctypes.data_as(_D), u.ctypes.data_as(_D), u.size)
 
     def Sample(self, u):
         """Inverse-CDF sampling of the readout-mixed diagonal (sim.go:45-60)."""

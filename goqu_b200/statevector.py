@@ -31,7 +31,22 @@ def format_bitstring(idx, n):
 
 def counts_from_indices(idx, n):
     vals, cnt = np.unique(np.asarray(idx, dtype=np.uint64), return_counts=True)
-    return {format_bitstring(v, n): int(c) for v, c in zip(vals, cnt)}
+    return counts_from_pairs(vals, cnt, n)
+
+
+def counts_from_pairs(outcomes, counts, n):
+    """goqu's map[bitstring]int from (outcome, count) pairs."""
+    return {format_bitstring(v, n): int(c) for v, c in zip(outcomes, counts)}
+
+
+def sample_counts_call(fn, shots, *head):
+    """Calls a *_sample_counts entry point: (distinct outcomes, counts)."""
+    m = max(1, shots)
+    outc = np.empty(m, dtype=np.uint64)
+    cnt = np.empty(m, dtype=np.uint64)
+    nd = ctypes.c_size_t()
+    _abi.check(fn(*head, outc.ctypes.data_as(_U64), cnt.ctypes.data_as(_U64), ctypes.byref(nd)))
+    return outc[:nd.value].copy(), cnt[:nd.value].copy()
 
 
 class Sim:
@@ -94,7 +109,7 @@ class Sim:
             from . import dynamic
             return dynamic.run_dynamic(self, c, shots, rng)
         self.Evolve(c)
-        return counts_from_indices(self.Sample(uniforms(shots, rng)), self._n)
+        return counts_from_pairs(*self.SampleCounts(uniforms(shots, rng)), self._n)
 
     # -- readout -----------------------------------------------------------
     def StateVector(self):
@@ -115,6 +130,11 @@ class Sim:
         out = np.empty(1 << self._n, dtype=np.float64)
         _abi.check(_abi.lib().gq_sv_probabilities(self._h, out.ctypes.data_as(_D), out.size))
         return out
+
+    def SampleCounts(self, u):
+        """Distinct sampled outcomes and their counts, histogrammed on the device."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        return sample_counts_call(_abi.lib().gq_sv_sample_counts, u.size, self._h, u.ctypes.data_as(_D), u.size)
 
     def Sample(self, u):
         u = np.ascontiguousarray(u, dtype=np.float64)

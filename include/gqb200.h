@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define GQ_ABI_VERSION 3
+#define GQ_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------ */
 #define GQ_OK 0
@@ -156,6 +156,18 @@ int gq_sv_sample(gq_sv* sv, const double* uniforms, size_t shots, uint64_t* idx_
 /* Run for static circuits: Evolve then sample (sim/statevector/sim.go:40-58). */
 int gq_sv_run(gq_sv* sv, const gq_op* ops, size_t n_ops, const double* uniforms,
               size_t shots, uint64_t* idx_out);
+/* Sampling with the histogram built on the device: the distinct sampled
+ * outcomes in increasing index order with their counts, i.e. the entries of
+ * the map[bitstring]int that Run returns (sim/statevector/sim.go:40-58; the
+ * bitstring is formatBitstring of the outcome, :306-316). outcomes_out and
+ * counts_out need room for min(shots, 2^n) entries; *n_distinct receives how
+ * many were written. Same uniforms, same outcomes as gq_sv_sample. At most
+ * 2^32 - 1 shots per call. */
+int gq_sv_sample_counts(gq_sv* sv, const double* uniforms, size_t shots, uint64_t* outcomes_out,
+                        uint64_t* counts_out, size_t* n_distinct);
+/* Run with counts: Evolve, then gq_sv_sample_counts. */
+int gq_sv_run_counts(gq_sv* sv, const gq_op* ops, size_t n_ops, const double* uniforms, size_t shots,
+                     uint64_t* outcomes_out, uint64_t* counts_out, size_t* n_distinct);
 /* sum_t coeff_t <psi|P_t|psi> as a complex number (pauli.ExpectSum,
  * sim/pauli/expect_sv.go:21-97); ExpectPauliSum is its real part.            */
 int gq_sv_expect_pauli_sum(gq_sv* sv, const gq_pauli_term* terms, size_t n_terms,
@@ -243,6 +255,11 @@ int gq_dm_fidelity(gq_dm* dm, const double* psi, size_t n, double* out);
  * pairs (ApplyReadoutError, measure.go:29-71); p01[q] < 0 skips qubit q.     */
 int gq_dm_sample(gq_dm* dm, const double* p01, const double* p10, const double* uniforms,
                  size_t shots, uint64_t* idx_out);
+/* The same sampling with the histogram built on the device (densitymatrix
+ * Run's counts, sim/densitymatrix/sim.go:48-66): distinct outcomes in
+ * increasing order and their counts, as gq_sv_sample_counts. */
+int gq_dm_sample_counts(gq_dm* dm, const double* p01, const double* p10, const double* uniforms,
+                        size_t shots, uint64_t* outcomes_out, uint64_t* counts_out, size_t* n_distinct);
 /* Dynamic circuits: measureQubitDM (sim/densitymatrix/dynamic.go:198-255).
  * P(0) = sum of rho[i,i] over i with the qubit's bit clear; the collapse keeps
  * rho[r,c] with both bits equal to the outcome, divided by its probability

@@ -35,7 +35,7 @@ def test_struct_layouts_match_header():
 
 
 def test_abi_version():
-    assert _abi.lib().gq_abi_version() == 3
+    assert _abi.lib().gq_abi_version() == 4
 
 
 @pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES") is None and os.path.exists("/dev/nvidia0"),
