@@ -113,6 +113,14 @@ class gq_batch_item(ctypes.Structure):
     ]
 
 
+class gq_sweep_point(ctypes.Structure):
+    _fields_ = [
+        ("ops", ctypes.POINTER(gq_op)),
+        ("n_ops", ctypes.c_size_t),
+        ("uniforms", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
 class GQError(RuntimeError):
     """An engine call returned a non-zero status."""
 
@@ -185,6 +193,10 @@ SIGNATURES = {
     "gq_batch_run": (_I, [_VP, ctypes.POINTER(gq_batch_item), _SZ, _I, _DBL_P, _DBL_P]),
     "gq_batch_set_option": (_I, [_VP, _I, ctypes.c_int64]),
     "gq_batch_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
+    "gq_sweep_run": (_I, [_I, _I, ctypes.POINTER(gq_sweep_point), _SZ, _SZ, _U64P, _U64P, ctypes.POINTER(_SZ),
+                          ctypes.POINTER(ctypes.c_int32)]),
+    "gq_sweep_run_density": (_I, [_I, _DBL_P, _DBL_P, ctypes.POINTER(gq_sweep_point), _SZ, _SZ, _U64P, _U64P,
+                                  ctypes.POINTER(_SZ), ctypes.POINTER(ctypes.c_int32)]),
     "gq_expect_pauli_sum_noalloc": (_I, [_VP, _I, _I, _TP, _SZ, _VP, _DBL_P, _DBL_P]),
 }
 

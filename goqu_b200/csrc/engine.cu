@@ -2086,3 +2086,98 @@ int gq_batch_stats(const gq_batch* b, gq_stats* out) {
 }
 
 }  // extern "C"
+
+// ---- sweeps ------------------------------------------------------------------
+namespace {
+
+// sweep.RunSim / RunDensitySim (sweep/run.go:27-171): a pool of workers
+// takes the points in order; each worker owns one handle (its own device
+// state and stream), so points overlap on the device while every point is a
+// fresh Evolve followed by sampling with the histogram built on the device.
+// Workers: at most the host's threads, 8, the point count, and as many
+// states as the free device memory holds next to 1 GiB of headroom.
+int sweep_impl(bool density, int nq, int prec, const double* p01, const double* p10, const gq_sweep_point* pts,
+               size_t n_pts, size_t shots, uint64_t* outcomes_out, uint64_t* counts_out, size_t* n_distinct_out,
+               int32_t* status_out) {
+    if (n_pts && (!pts || !n_distinct_out || !status_out)) return fail(GQ_EINVAL, "null argument");
+    if (shots && n_pts && (!outcomes_out || !counts_out)) return fail(GQ_EINVAL, "null argument");
+    if (density ? (nq < 1 || nq > 15) : (nq < 1 || nq > 34)) return fail(GQ_EINVAL, "num_qubits out of range");
+    if (!density && prec != GQ_C128 && prec != GQ_C64) return fail(GQ_EINVAL, "unknown precision");
+    for (size_t i = 0; i < n_pts; ++i)
+        if ((pts[i].n_ops && !pts[i].ops) || (shots && !pts[i].uniforms)) return fail(GQ_EINVAL, "null point data");
+    if (n_pts == 0) return GQ_OK;
+    int dev = 0;
+    GQ_TRY(check_device(&dev));
+    const uint64_t outcomes = 1ull << nq;
+    const size_t stride = (size_t)std::max<uint64_t>(1, std::min<uint64_t>(shots, outcomes));
+    const uint64_t state_bytes =
+        density ? (1ull << (2 * nq)) * 16 : std::max<uint64_t>(16, outcomes) * (prec == GQ_C64 ? 8 : 16);
+    size_t mem_free = 0, mem_total = 0;
+    GQ_CUDA(cudaMemGetInfo(&mem_free, &mem_total));
+    const uint64_t headroom = 1ull << 30;
+    const uint64_t by_mem = mem_free > headroom ? (mem_free - headroom) / (2 * state_bytes) : 0;
+    unsigned hw = std::thread::hardware_concurrency();
+    const size_t nworkers = std::max<size_t>(
+        1, std::min<size_t>({n_pts, (size_t)8, (size_t)std::max(1u, hw), (size_t)std::max<uint64_t>(1, by_mem)}));
+    std::atomic<size_t> next{0};
+    std::mutex err_mu;
+    std::string first_err;
+    size_t first_bad = n_pts;
+    auto worker = [&]() {
+        cudaSetDevice(dev);
+        gq_sv* sv = nullptr;
+        gq_dm* dm = nullptr;
+        int rc_create = density ? gq_dm_create(nq, &dm) : gq_sv_create(nq, prec, &sv);
+        for (size_t i; (i = next.fetch_add(1)) < n_pts;) {
+            int rc = rc_create;
+            if (rc == GQ_OK) {
+                uint64_t* oc = shots ? outcomes_out + i * stride : nullptr;
+                uint64_t* ct = shots ? counts_out + i * stride : nullptr;
+                if (density) {
+                    rc = gq_dm_evolve(dm, pts[i].ops, pts[i].n_ops);
+                    if (rc == GQ_OK)
+                        rc = gq_dm_sample_counts(dm, p01, p10, pts[i].uniforms, shots, oc, ct, &n_distinct_out[i]);
+                } else {
+                    rc = gq_sv_run_counts(sv, pts[i].ops, pts[i].n_ops, pts[i].uniforms, shots, oc, ct,
+                                          &n_distinct_out[i]);
+                }
+            }
+            status_out[i] = rc;
+            if (rc != GQ_OK) {
+                n_distinct_out[i] = 0;
+                std::lock_guard<std::mutex> lk(err_mu);
+                if (i < first_bad) {
+                    first_bad = i;
+                    first_err = "point " + std::to_string(i) + ": " + g_err;
+                }
+            }
+        }
+        if (sv) gq_sv_destroy(sv);
+        if (dm) gq_dm_destroy(dm);
+    };
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < nworkers; ++k) pool.emplace_back(worker);
+    worker();
+    for (std::thread& t : pool) t.join();
+    if (first_bad < n_pts) g_err = first_err;  // the points' own statuses are in status_out
+    return GQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gq_sweep_run(int num_qubits, int precision, const gq_sweep_point* points, size_t n_points, size_t shots,
+                 uint64_t* outcomes_out, uint64_t* counts_out, size_t* n_distinct_out, int32_t* status_out) {
+    return sweep_impl(false, num_qubits, precision, nullptr, nullptr, points, n_points, shots, outcomes_out,
+                      counts_out, n_distinct_out, status_out);
+}
+
+int gq_sweep_run_density(int num_qubits, const double* p01, const double* p10, const gq_sweep_point* points,
+                         size_t n_points, size_t shots, uint64_t* outcomes_out, uint64_t* counts_out,
+                         size_t* n_distinct_out, int32_t* status_out) {
+    return sweep_impl(true, num_qubits, GQ_C128, p01, p10, points, n_points, shots, outcomes_out, counts_out,
+                      n_distinct_out, status_out);
+}
+
+}  // extern "C"

@@ -301,6 +301,33 @@ int gq_batch_run(gq_batch* b, const gq_batch_item* items, size_t n_items, int wa
 int gq_batch_set_option(gq_batch* b, int key, int64_t value);
 int gq_batch_stats(const gq_batch* b, gq_stats* out);
 
+/* ---- sweeps: replaces sweep.RunSim / RunDensitySim (sweep/run.go:27-171) ----
+ * Every point is the same circuit bound to different values: `num_qubits`
+ * qubits from |0...0> (rho = |0><0| for density matrices), the point's op
+ * stream applied (density matrices: gates and their channels, GQ_OP_CHANNEL,
+ * as for gq_dm_apply), then `shots` samples drawn with the point's uniforms
+ * (Run, sim/statevector/sim.go:40-58 and sim/densitymatrix/sim.go:48-66) and
+ * returned as (outcome, count) pairs in increasing outcome order. Point i's
+ * pairs are written at offset i * S of outcomes_out / counts_out, with
+ * S = max(1, min(shots, 2^num_qubits)); n_distinct_out[i] receives their
+ * number and status_out[i] the point's status (goqu's PointResult.Err), so a
+ * failing point does not stop the others; gq_last_error() then describes the
+ * first failing point. Points run on a pool of workers, each with its own
+ * device state and stream (at most 8, and as many as device memory holds).
+ * The density variant applies readout error with p01 / p10 (num_qubits
+ * entries each, a negative p01[q] skips qubit q; both may be NULL). */
+typedef struct gq_sweep_point {
+    const gq_op* ops;
+    size_t n_ops;
+    const double* uniforms; /* `shots` values in [0, 1) */
+} gq_sweep_point;
+
+int gq_sweep_run(int num_qubits, int precision, const gq_sweep_point* points, size_t n_points, size_t shots,
+                 uint64_t* outcomes_out, uint64_t* counts_out, size_t* n_distinct_out, int32_t* status_out);
+int gq_sweep_run_density(int num_qubits, const double* p01, const double* p10, const gq_sweep_point* points,
+                         size_t n_points, size_t shots, uint64_t* outcomes_out, uint64_t* counts_out,
+                         size_t* n_distinct_out, int32_t* status_out);
+
 /* ---- expectation without allocation ---------------------------------------
  * No counterpart in the reference: an extra entry point for callers that own
  * their device memory and must not have the library call cudaMalloc or
