@@ -193,6 +193,9 @@ SIGNATURES = {
     "gq_batch_run": (_I, [_VP, ctypes.POINTER(gq_batch_item), _SZ, _I, _DBL_P, _DBL_P]),
     "gq_batch_set_option": (_I, [_VP, _I, ctypes.c_int64]),
     "gq_batch_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
+    "gq_unitary": (_I, [_I, _OPP, _SZ, _DBL_P, _SZ]),
+    "gq_equivalent": (_I, [_I, _OPP, _SZ, _OPP, _SZ, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
+    "gq_equivalent_on_zero": (_I, [_I, _OPP, _SZ, _OPP, _SZ, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
     "gq_sweep_run": (_I, [_I, _I, ctypes.POINTER(gq_sweep_point), _SZ, _SZ, _U64P, _U64P, ctypes.POINTER(_SZ),
                           ctypes.POINTER(ctypes.c_int32)]),
     "gq_sweep_run_density": (_I, [_I, _DBL_P, _DBL_P, ctypes.POINTER(gq_sweep_point), _SZ, _SZ, _U64P, _U64P,

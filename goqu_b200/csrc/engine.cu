@@ -20,6 +20,7 @@
 #include "../../include/gqb200.h"
 #include "counts.cuh"
 #include "kernels.cuh"
+#include "verify.cuh"
 #include "jit.hpp"
 #include "schedule.hpp"
 
@@ -2178,6 +2179,193 @@ int gq_sweep_run_density(int num_qubits, const double* p01, const double* p10, c
                          size_t* n_distinct_out, int32_t* status_out) {
     return sweep_impl(true, num_qubits, GQ_C128, p01, p10, points, n_points, shots, outcomes_out, counts_out,
                       n_distinct_out, status_out);
+}
+
+}  // extern "C"
+
+// ---- circuit equivalence (transpile/verify/verify.go) ------------------------
+namespace {
+
+// Applies `ops` (qubits < n) to the handle's state without resetting it.
+int apply_on_low(gq_sv* sv, int n, const gq_op* ops, size_t n_ops) {
+    if (n_ops && !ops) return fail(GQ_EINVAL, "null ops");
+    std::vector<NGate> gates;
+    std::string err;
+    for (size_t i = 0; i < n_ops; ++i) {
+        if (ops[i].kind == GQ_OP_CHANNEL) return fail(GQ_EINVAL, "op " + std::to_string(i) + ": channel in a circuit");
+        int rc = normalize_op(ops[i], n, gates, err);
+        if (rc != GQ_OK) return fail(rc, "op " + std::to_string(i) + ": " + err);
+    }
+    return sv->e.run_gates(gates);
+}
+
+// sv (2n qubits) <- every column of the unitary of `ops`: entry (col << n) | row.
+int unitary_into(gq_sv* sv, int n, const gq_op* ops, size_t n_ops) {
+    Engine& e = sv->e;
+    GQ_CUDA(cudaMemsetAsync(e.state.p, 0, e.n_amps * e.amp_bytes(), e.stream));
+    k_unit_columns<<<(unsigned)(((1ull << n) + 255) / 256), 256, 0, e.stream>>>((cplx<double>*)e.state.p, n);
+    GQ_CUDA(cudaGetLastError());
+    return apply_on_low(sv, n, ops, n_ops);
+}
+
+// First index i < len with |state[i]| > tol, or len when there is none.
+int first_above(Engine& e, uint64_t len, double tol, uint64_t* out) {
+    GQ_TRY(e.scratch.ensure(64));
+    GQ_TRY(e.hostio.ensure(64));
+    unsigned long long* d = (unsigned long long*)e.scratch.p;
+    GQ_CUDA(cudaMemsetAsync(d, 0xff, 8, e.stream));
+    const unsigned g = (unsigned)std::min<uint64_t>((len + 255) / 256, (uint64_t)e.reduce_grid());
+    k_first_above<<<g, 256, 0, e.stream>>>((const cplx<double>*)e.state.p, len, tol, d);
+    GQ_CUDA(cudaGetLastError());
+    GQ_CUDA(cudaMemcpyAsync(e.hostio.p, d, 8, cudaMemcpyDeviceToHost, e.stream));
+    GQ_CUDA(cudaStreamSynchronize(e.stream));
+    const unsigned long long v = *(const unsigned long long*)e.hostio.p;
+    *out = v == ~0ull ? len : (uint64_t)v;
+    return GQ_OK;
+}
+
+int amplitude_at(Engine& e, uint64_t i, Z* out) {
+    GQ_TRY(e.hostio.ensure(64));
+    GQ_CUDA(cudaMemcpyAsync(e.hostio.p, (const char*)e.state.p + 16 * i, 16, cudaMemcpyDeviceToHost, e.stream));
+    GQ_CUDA(cudaStreamSynchronize(e.stream));
+    *out = *(const Z*)e.hostio.p;
+    return GQ_OK;
+}
+
+// n / m by Smith's algorithm (R. L. Smith, Algorithm 116: Complex division,
+// CACM 5(8), 1962), the division Go's complex128 arithmetic uses.
+Z smith_div(Z n, Z m) {
+    if (std::fabs(m.re) >= std::fabs(m.im)) {
+        const double r = m.im / m.re, den = m.re + r * m.im;
+        return Z{(n.re + n.im * r) / den, (n.im - n.re * r) / den};
+    }
+    const double r = m.re / m.im, den = m.im + r * m.re;
+    return Z{(n.re * r + n.im) / den, (n.im * r - n.re) / den};
+}
+
+// Whether some |a[i] - phase * b[i]| > tol for i < len (a, b: the handles' states).
+int phase_mismatch(Engine& ea, Engine& eb, uint64_t len, Z phase, double tol, bool* bad) {
+    GQ_CUDA(cudaStreamSynchronize(eb.stream));
+    GQ_TRY(ea.scratch.ensure(64));
+    GQ_TRY(ea.hostio.ensure(64));
+    int* d = (int*)ea.scratch.p;
+    GQ_CUDA(cudaMemsetAsync(d, 0, 4, ea.stream));
+    const unsigned g = (unsigned)std::min<uint64_t>((len + 255) / 256, (uint64_t)ea.reduce_grid());
+    k_phase_mismatch<<<g, 256, 0, ea.stream>>>((const cplx<double>*)ea.state.p, (const cplx<double>*)eb.state.p,
+                                                len, phase.re, phase.im, tol, d);
+    GQ_CUDA(cudaGetLastError());
+    GQ_CUDA(cudaMemcpyAsync(ea.hostio.p, d, 4, cudaMemcpyDeviceToHost, ea.stream));
+    GQ_CUDA(cudaStreamSynchronize(ea.stream));
+    *bad = *(const int*)ea.hostio.p != 0;
+    return GQ_OK;
+}
+
+struct SvPair {
+    gq_sv* a = nullptr;
+    gq_sv* b = nullptr;
+    ~SvPair() {
+        gq_sv_destroy(a);
+        gq_sv_destroy(b);
+    }
+};
+
+int check_pair_args(int n, int max_n, const gq_op* a, size_t na, const gq_op* b, size_t nb, double tol, int* out) {
+    if (!out) return fail(GQ_EINVAL, "null output");
+    if ((na && !a) || (nb && !b)) return fail(GQ_EINVAL, "null ops");
+    if (n < 1 || n > max_n)
+        return fail(GQ_EINVAL, "verify: circuit too large for equivalence check: " + std::to_string(n) + " qubits");
+    if (!(tol >= 0.0)) return fail(GQ_EINVAL, "verify: negative tolerance");
+    return GQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gq_unitary(int num_qubits, const gq_op* ops, size_t n_ops, double* host_out, size_t bytes) {
+    if (!host_out) return fail(GQ_EINVAL, "null output");
+    if (num_qubits < 1 || num_qubits > 16) return fail(GQ_EINVAL, "num_qubits out of range [1, 16]");
+    const uint64_t len = 1ull << (2 * num_qubits);
+    if (bytes < len * 16) return fail(GQ_EINVAL, "output buffer too small");
+    gq_sv* sv = nullptr;
+    GQ_TRY(gq_sv_create(2 * num_qubits, GQ_C128, &sv));
+    int rc = unitary_into(sv, num_qubits, ops, n_ops);
+    if (rc == GQ_OK) {
+        cudaError_t e = cudaMemcpyAsync(host_out, sv->e.state.p, len * 16, cudaMemcpyDeviceToHost, sv->e.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(sv->e.stream);
+        if (e != cudaSuccess) rc = fail(GQ_ECUDA, std::string("unitary copy: ") + cudaGetErrorString(e));
+    }
+    gq_sv_destroy(sv);
+    return rc;
+}
+
+int gq_equivalent(int num_qubits, const gq_op* a, size_t na, const gq_op* b, size_t nb, double tol, int* equal_out) {
+    GQ_TRY(check_pair_args(num_qubits, 15, a, na, b, nb, tol, equal_out));
+    const int n = num_qubits;
+    SvPair p;
+    GQ_TRY(gq_sv_create(2 * n, GQ_C128, &p.a));
+    GQ_TRY(gq_sv_create(2 * n, GQ_C128, &p.b));
+    GQ_TRY(unitary_into(p.a, n, a, na));
+    GQ_TRY(unitary_into(p.b, n, b, nb));
+    // global phase from the first entry of B's column 0 above tol (unitariesClose)
+    const uint64_t dim = 1ull << n;
+    uint64_t ib = 0;
+    GQ_TRY(first_above(p.b->e, dim, tol, &ib));
+    if (ib == dim) {
+        *equal_out = 1;
+        return GQ_OK;
+    }
+    Z va, vb;
+    GQ_CUDA(cudaStreamSynchronize(p.a->e.stream));
+    GQ_TRY(amplitude_at(p.a->e, ib, &va));
+    GQ_TRY(amplitude_at(p.b->e, ib, &vb));
+    if (std::hypot(va.re, va.im) < tol) {
+        *equal_out = 0;
+        return GQ_OK;
+    }
+    bool bad = false;
+    GQ_TRY(phase_mismatch(p.a->e, p.b->e, dim * dim, smith_div(va, vb), tol, &bad));
+    *equal_out = bad ? 0 : 1;
+    return GQ_OK;
+}
+
+int gq_equivalent_on_zero(int num_qubits, const gq_op* a, size_t na, const gq_op* b, size_t nb, double tol,
+                          int* equal_out) {
+    GQ_TRY(check_pair_args(num_qubits, 30, a, na, b, nb, tol, equal_out));
+    const int n = num_qubits;
+    SvPair p;
+    GQ_TRY(gq_sv_create(n, GQ_C128, &p.a));
+    GQ_TRY(gq_sv_create(n, GQ_C128, &p.b));
+    GQ_TRY(gq_sv_reset(p.a));
+    GQ_TRY(apply_on_low(p.a, n, a, na));
+    GQ_TRY(gq_sv_reset(p.b));
+    GQ_TRY(apply_on_low(p.b, n, b, nb));
+    // stateVectorsClose: the first index where either state exceeds tol
+    // decides; B's entry there gives the global phase, of modulus 1 +- tol
+    const uint64_t len = 1ull << n;
+    uint64_t ia = 0, ib = 0;
+    GQ_TRY(first_above(p.a->e, len, tol, &ia));
+    GQ_TRY(first_above(p.b->e, len, tol, &ib));
+    if (ib == len || ia < ib) {
+        *equal_out = (ib == len && ia == len) ? 1 : 0;
+        return GQ_OK;
+    }
+    Z va, vb;
+    GQ_TRY(amplitude_at(p.a->e, ib, &va));
+    GQ_TRY(amplitude_at(p.b->e, ib, &vb));
+    if (std::hypot(va.re, va.im) < tol) {
+        *equal_out = 0;
+        return GQ_OK;
+    }
+    const Z phase = smith_div(va, vb);
+    if (std::fabs(std::hypot(phase.re, phase.im) - 1.0) > tol) {
+        *equal_out = 0;
+        return GQ_OK;
+    }
+    bool bad = false;
+    GQ_TRY(phase_mismatch(p.a->e, p.b->e, len, phase, tol, &bad));
+    *equal_out = bad ? 0 : 1;
+    return GQ_OK;
 }
 
 }  // extern "C"

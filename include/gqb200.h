@@ -328,6 +328,22 @@ int gq_sweep_run_density(int num_qubits, const double* p01, const double* p10, c
                          size_t n_points, size_t shots, uint64_t* outcomes_out, uint64_t* counts_out,
                          size_t* n_distinct_out, int32_t* status_out);
 
+/* ---- circuit equivalence: replaces transpile/verify (verify.go:16-155) ------
+ * gq_unitary: the unitary of a circuit on num_qubits (<= 16) qubits, every
+ * column evolved at once (goqu builds it from 2^n runs that prepend X gates,
+ * verify.go:45-90). host_out receives 4^n complex128 values, column by
+ * column: entry col * 2^n + row = U[row][col] (goqu's unitary[col][row]).
+ * gq_equivalent: verify.Equivalent, the unitaries equal up to a global phase
+ * taken from the first entry of B's column 0 whose modulus exceeds tol, every
+ * entry then within tol (unitariesClose); num_qubits <= 15 (goqu: 10).
+ * gq_equivalent_on_zero: verify.EquivalentOnZero, the states from |0...0>
+ * compared the same way, the phase's modulus within tol of 1
+ * (stateVectorsClose); num_qubits <= 30 (goqu: 14). *equal_out is 1 or 0. */
+int gq_unitary(int num_qubits, const gq_op* ops, size_t n_ops, double* host_out, size_t bytes);
+int gq_equivalent(int num_qubits, const gq_op* a, size_t n_a, const gq_op* b, size_t n_b, double tol, int* equal_out);
+int gq_equivalent_on_zero(int num_qubits, const gq_op* a, size_t n_a, const gq_op* b, size_t n_b, double tol,
+                          int* equal_out);
+
 /* ---- expectation without allocation ---------------------------------------
  * No counterpart in the reference: an extra entry point for callers that own
  * their device memory and must not have the library call cudaMalloc or
