@@ -121,6 +121,36 @@ class gq_sweep_point(ctypes.Structure):
     ]
 
 
+class gq_param_gate(ctypes.Structure):
+    _fields_ = [
+        ("op_index", ctypes.c_int32),
+        ("gate", ctypes.c_int32),
+        ("num_angles", ctypes.c_int32),
+        ("param", ctypes.c_int32 * 3),
+        ("scale", ctypes.c_double * 3),
+        ("shift", ctypes.c_double * 3),
+    ]
+
+
+class gq_adam_options(ctypes.Structure):
+    _fields_ = [
+        ("lr", ctypes.c_double), ("beta1", ctypes.c_double), ("beta2", ctypes.c_double),
+        ("epsilon", ctypes.c_double), ("max_iter", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("fun_tol", ctypes.c_double), ("grad_tol", ctypes.c_double),
+    ]
+
+
+class gq_optim_result(ctypes.Structure):
+    _fields_ = [
+        ("fun", ctypes.c_double), ("iterations", ctypes.c_int32), ("func_evals", ctypes.c_int32),
+        ("grad_evals", ctypes.c_int32), ("converged", ctypes.c_int32),
+    ]
+
+
+GQ_PG = {"RX": 1, "RY": 2, "RZ": 3, "P": 4, "U1": 5, "U2": 6, "U3": 7, "Rot": 8, "CP": 9, "RXX": 10, "RYY": 11,
+         "RZZ": 12, "FSim": 13, "PSwap": 14, "GlobalPhase": 15}
+
+
 class GQError(RuntimeError):
     """An engine call returned a non-zero status."""
 
@@ -193,6 +223,10 @@ SIGNATURES = {
     "gq_batch_run": (_I, [_VP, ctypes.POINTER(gq_batch_item), _SZ, _I, _DBL_P, _DBL_P]),
     "gq_batch_set_option": (_I, [_VP, _I, ctypes.c_int64]),
     "gq_batch_stats": (_I, [_VP, ctypes.POINTER(gq_stats)]),
+    "gq_sv_adjoint_template": (_I, [_VP, _OPP, _SZ, ctypes.POINTER(gq_param_gate), _SZ, _DBL_P, _SZ, _TP, _SZ,
+                                    _DBL_P, _DBL_P]),
+    "gq_sv_minimize_adam": (_I, [_VP, _OPP, _SZ, ctypes.POINTER(gq_param_gate), _SZ, _TP, _SZ, _SZ, _DBL_P,
+                                 ctypes.POINTER(gq_adam_options), ctypes.POINTER(gq_optim_result), _DBL_P, _SZ]),
     "gq_unitary": (_I, [_I, _OPP, _SZ, _DBL_P, _SZ]),
     "gq_equivalent": (_I, [_I, _OPP, _SZ, _OPP, _SZ, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
     "gq_equivalent_on_zero": (_I, [_I, _OPP, _SZ, _OPP, _SZ, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),

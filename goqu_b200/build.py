@@ -17,9 +17,9 @@ NVCC_FLAGS = [
     "-shared",
 ]
 
-ENGINE_SOURCES = ["engine.cu", "noalloc.cu", "schedule.cpp", "jit.cpp", "jit_gen.cpp"]
-EMULATOR_SOURCES = ["emulate.cpp", "schedule.cpp", "jit_gen.cpp"]
-HEADERS = ["tile_core.cuh", "kernels.cuh", "schedule.hpp", "jit.hpp", os.path.join("..", "..", "include", "gqb200.h")]
+ENGINE_SOURCES = ["engine.cu", "noalloc.cu", "schedule.cpp", "jit.cpp", "jit_gen.cpp", "params.cpp"]
+EMULATOR_SOURCES = ["emulate.cpp", "schedule.cpp", "jit_gen.cpp", "params.cpp"]
+HEADERS = ["tile_core.cuh", "kernels.cuh", "counts.cuh", "verify.cuh", "schedule.hpp", "jit.hpp", "params.hpp", os.path.join("..", "..", "include", "gqb200.h")]
 # tile_core.cuh as a C++ string literal, compiled into the engine for the
 # run-time specialised pass kernels (generated; not committed).
 TILE_CORE_INC = os.path.join(CSRC, "tile_core_src.inc")

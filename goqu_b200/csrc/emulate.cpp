@@ -17,6 +17,7 @@
 
 #include "jit.hpp"
 #include "schedule.hpp"
+#include "params.hpp"
 #include "tile_core.cuh"
 
 namespace {
@@ -589,6 +590,17 @@ int gqx_jit_check_dual(int nq, int precision, const gq_op* ops, size_t n_ops, si
 // after cudaMemGetInfo.
 int gqx_adjoint_segments(int requested, int c64, uint64_t n_ops, uint64_t state_bytes, uint64_t avail_bytes) {
     return gq::adjoint_segments(requested, c64 != 0, (size_t)n_ops, (size_t)state_bytes, (size_t)avail_bytes);
+}
+
+// A parameterized gate family's matrix (k < 0) or its derivative with
+// respect to angle k, as the engine binds it; out holds 2 * dim^2 doubles.
+int gqx_param_gate(int family, const double* angles, int n_angles, int k, double* out) {
+    std::vector<gq::Z> m;
+    const bool ok = k < 0 ? gq::param_gate_matrix(family, angles, n_angles, m)
+                          : gq::param_gate_dmatrix(family, angles, n_angles, k, m);
+    if (!ok) return GQ_EINVAL;
+    std::memcpy(out, m.data(), m.size() * sizeof(gq::Z));
+    return (int)m.size();
 }
 
 }  // extern "C"

@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 #include "verify.cuh"
 #include "jit.hpp"
+#include "params.hpp"
 #include "schedule.hpp"
 
 using namespace gq;
@@ -2365,6 +2366,85 @@ int gq_equivalent_on_zero(int num_qubits, const gq_op* a, size_t na, const gq_op
     bool bad = false;
     GQ_TRY(phase_mismatch(p.a->e, p.b->e, len, phase, tol, &bad));
     *equal_out = bad ? 0 : 1;
+    return GQ_OK;
+}
+
+}  // extern "C"
+
+// ---- parameterized templates and the Adam loop ---------------------------------
+extern "C" {
+
+int gq_sv_adjoint_template(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_param_gate* pgates, size_t n_pgates,
+                           const double* theta, size_t n_params, const gq_pauli_term* terms, size_t n_terms,
+                           double* grad_out, double* energy_out) {
+    if (!sv) return fail(GQ_EINVAL, "null handle");
+    if ((n_ops && !ops) || (n_pgates && !pgates) || (n_params && !theta)) return fail(GQ_EINVAL, "null argument");
+    BoundTemplate bt;
+    std::string err;
+    const int rc = bind_template(ops, n_ops, pgates, n_pgates, theta, n_params, bt, err);
+    if (rc != GQ_OK) return fail(rc, err);
+    return gq_sv_adjoint_gradient(sv, bt.ops.data(), bt.ops.size(), terms, n_terms, n_params, grad_out, energy_out);
+}
+
+int gq_sv_minimize_adam(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_param_gate* pgates, size_t n_pgates,
+                        const gq_pauli_term* terms, size_t n_terms, size_t n_params, double* x,
+                        const gq_adam_options* opts, gq_optim_result* result, double* history_out,
+                        size_t history_cap) {
+    if (!sv || !result) return fail(GQ_EINVAL, "null argument");
+    if (n_params == 0) return fail(GQ_EINVAL, "adam: x0 must be non-empty");
+    if (!x) return fail(GQ_EINVAL, "null x");
+    const gq_adam_options o = opts ? *opts : gq_adam_options{};
+    const double lr = o.lr > 0 ? o.lr : 0.001, b1 = o.beta1 > 0 ? o.beta1 : 0.9;
+    const double b2 = o.beta2 > 0 ? o.beta2 : 0.999, eps = o.epsilon > 0 ? o.epsilon : 1e-8;
+    const int max_iter = o.max_iter > 0 ? o.max_iter : 1000;
+    const double fun_tol = o.fun_tol > 0 ? o.fun_tol : 1e-8, grad_tol = o.grad_tol > 0 ? o.grad_tol : 0.0;
+    const size_t n = n_params;
+    std::vector<double> m(n, 0.0), v(n, 0.0), g(n);
+    size_t nh = 0;
+    auto record = [&](double f) {
+        if (history_out && nh < history_cap) history_out[nh] = f;
+        ++nh;
+    };
+    // (energy, gradient) at x: goqu's f(x) and, for the next iteration, grad(x)
+    double fx = 0.0;
+    GQ_TRY(gq_sv_adjoint_template(sv, ops, n_ops, pgates, n_pgates, x, n, terms, n_terms, g.data(), &fx));
+    record(fx);
+    int f_evals = 1, g_evals = 0, iter = 0;
+    bool converged = false;
+    double prev = fx;
+    for (iter = 0; iter < max_iter; ++iter) {
+        ++g_evals;  // g holds grad(x) at the current x
+        if (grad_tol > 0) {
+            double s = 0.0;
+            for (double gj : g) s += gj * gj;
+            if (std::sqrt(s) < grad_tol) {
+                converged = true;
+                break;
+            }
+        }
+        const double t = (double)(iter + 1);
+        for (size_t j = 0; j < n; ++j) {
+            m[j] = b1 * m[j] + (1 - b1) * g[j];
+            v[j] = b2 * v[j] + (1 - b2) * g[j] * g[j];
+            const double mh = m[j] / (1 - std::pow(b1, t));
+            const double vh = v[j] / (1 - std::pow(b2, t));
+            x[j] -= lr * mh / (std::sqrt(vh) + eps);
+        }
+        GQ_TRY(gq_sv_adjoint_template(sv, ops, n_ops, pgates, n_pgates, x, n, terms, n_terms, g.data(), &fx));
+        ++f_evals;
+        record(fx);
+        if (std::fabs(fx - prev) < fun_tol) {
+            converged = true;
+            ++iter;
+            break;
+        }
+        prev = fx;
+    }
+    result->fun = fx;
+    result->iterations = iter;
+    result->func_evals = f_evals;
+    result->grad_evals = g_evals;
+    result->converged = converged ? 1 : 0;
     return GQ_OK;
 }
 

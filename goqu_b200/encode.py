@@ -198,3 +198,92 @@ def density_ops(circuit, noise_model=None):
         if not getattr(g, "noiseless", False):
             channel(g.Name(), op.Qubits)
     return stream
+
+
+# ---- parameterized templates (gq_sv_adjoint_template / gq_sv_minimize_adam) --
+
+def _affine(expr, index):
+    """(parameter index or -1, scale, shift) of an expression that is affine
+    in at most one parameter, else None."""
+    from . import param as _param
+    if isinstance(expr, _param._Literal):
+        return (-1, 0.0, expr.v)
+    if isinstance(expr, _param.Parameter):
+        i = index.get(expr.Name())
+        return None if i is None else (i, 1.0, 0.0)
+    if isinstance(expr, _param._Neg):
+        a = _affine(expr.inner, index)
+        return None if a is None else (a[0], -a[1], -a[2])
+    if isinstance(expr, _param._BinOp):
+        a, b = _affine(expr.left, index), _affine(expr.right, index)
+        if a is None or b is None:
+            return None
+        if expr.op in "+-":
+            sg = 1.0 if expr.op == "+" else -1.0
+            if a[0] >= 0 and b[0] >= 0 and a[0] != b[0]:
+                return None
+            p = a[0] if a[0] >= 0 else b[0]
+            return (p, a[1] + sg * b[1], a[2] + sg * b[2])
+        if expr.op == "*":
+            if a[0] < 0:
+                return (b[0], a[2] * b[1], a[2] * b[2])
+            if b[0] < 0:
+                return (a[0], b[2] * a[1], b[2] * a[2])
+            return None
+        if expr.op == "/" and b[0] < 0 and b[2] != 0.0:
+            return (a[0], a[1] / b[2], a[2] / b[2])
+    return None
+
+
+class Template:
+    """A circuit's op stream with its symbolic gates as gq_param_gate entries
+    the library rebinds from parameter values (angles affine in one
+    parameter each). `ops` holds the stream; `pgates` the entries."""
+
+    def __init__(self, ops, pgates, n_params):
+        self.ops = ops
+        self.pgates = pgates
+        self.n_params = n_params
+
+    def pgate_ptr(self):
+        return ctypes.cast(self.pgates, ctypes.POINTER(_abi.gq_param_gate)) if len(self.pgates) else None
+
+
+def param_template(circuit, param_names, x0=None):
+    """The Template of `circuit` for parameters `param_names` (raises
+    ValueError when a symbolic gate's family or expression cannot be bound
+    by the library). Symbolic ops carry their matrix at x0 as a placeholder."""
+    names = list(param_names)
+    index = {nm: i for i, nm in enumerate(names)}
+    x0 = np.zeros(len(names)) if x0 is None else np.asarray(x0, dtype=np.float64)
+    bindings = {nm: float(x0[i]) for i, nm in enumerate(names)}
+    stream = OpStream(circuit.NumQubits())
+    stream.n_params = len(names)
+    entries = []
+    for op in circuit.Ops():
+        g = op.Gate
+        if g is None:
+            continue
+        d = getattr(g, "directive", None)
+        if d == "barrier" or d == "delay":
+            continue
+        if d == "reset":
+            raise ValueError("template: reset is not unitary")
+        if hasattr(g, "Bind"):
+            fam = _abi.GQ_PG.get(g.base_name)
+            if fam is None:
+                raise ValueError(f"template: symbolic gate {g.base_name} has no library binding")
+            coeffs = [_affine(e, index) for e in g.exprs]
+            if any(a is None for a in coeffs):
+                raise ValueError(f"template: {g.Name()} is not affine in one parameter per angle")
+            e = _abi.gq_param_gate()
+            e.op_index = len(stream)
+            e.gate = fam
+            e.num_angles = len(coeffs)
+            for k, (p, sc, sh) in enumerate(coeffs):
+                e.param[k], e.scale[k], e.shift[k] = p, sc, sh
+            entries.append(e)
+            _gate_record(stream, g.Bind(bindings), op.Qubits)
+            continue
+        _gate_record(stream, g, op.Qubits)
+    return Template(stream, (_abi.gq_param_gate * len(entries))(*entries) if entries else [], len(names))

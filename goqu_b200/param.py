@@ -239,7 +239,7 @@ class SymbolicGate(_gate.Gate):
 
     # exp(-i theta/2 G) with G^2 = I: dU/dtheta = U(theta + pi) / 2
     _SHIFT = {"RX", "RY", "RZ", "RXX", "RYY", "RZZ"}
-    # diag(1, ..., 1, e^(i phi)): dU/dphi = i (U - I)
+    # diag(1, ..., 1, e^(i phi)): dU/dphi is i e^(i phi) on the last diagonal entry
     _PHASE = {"P", "CP", "U1"}
 
     def _dmatrix(self, k, vals):
@@ -247,9 +247,10 @@ class SymbolicGate(_gate.Gate):
         if len(vals) == 1 and base in self._SHIFT:
             return self.constructor([vals[0] + math.pi]).Matrix() / 2
         if len(vals) == 1 and base in self._PHASE:
-            u = self.constructor(vals).Matrix()
-            dim = int(round(math.sqrt(u.size)))
-            return 1j * (u - np.eye(dim, dtype=np.complex128).reshape(-1))
+            u = np.asarray(self.constructor(vals).Matrix(), dtype=np.complex128)
+            d = np.zeros_like(u)
+            d[-1] = 1j * u[-1]
+            return d
         if len(vals) == 1 and base == "GlobalPhase":
             return 1j * self.constructor(vals).Matrix()
 

@@ -184,6 +184,79 @@ int gq_sv_expect_z_mask(gq_sv* sv, uint64_t mask, double* out);
 int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops,
                            const gq_pauli_term* terms, size_t n_terms,
                            size_t n_params, double* grad_out, double* energy_out);
+/* ---- parameterized templates: the optimisation loop ------------------------
+ * A template is the op stream of a circuit whose symbolic gates
+ * (circuit/param/gate.go:13-142) are rebound from parameter values by the
+ * library: each gq_param_gate names an op of the stream (its matrix pointer
+ * is ignored), the gate family (goqu's parameterized gates,
+ * circuit/gate/parameterized.go:91-564) and, per angle k,
+ *   angle_k = scale[k] * theta[param[k]] + shift[k]   (param[k] = -1: shift only).
+ * The library computes the matrix and d(matrix)/d(parameter) (closed forms;
+ * chain rule over the angles that share a parameter) for every call. */
+#define GQ_PG_RX 1
+#define GQ_PG_RY 2
+#define GQ_PG_RZ 3
+#define GQ_PG_PHASE 4        /* P(phi) */
+#define GQ_PG_U1 5
+#define GQ_PG_U2 6           /* (phi, lambda) */
+#define GQ_PG_U3 7           /* (theta, phi, lambda) */
+#define GQ_PG_ROT 8          /* (phi, theta, omega) */
+#define GQ_PG_CP 9
+#define GQ_PG_RXX 10
+#define GQ_PG_RYY 11
+#define GQ_PG_RZZ 12
+#define GQ_PG_FSIM 13        /* (theta, phi) */
+#define GQ_PG_PSWAP 14
+#define GQ_PG_GLOBAL_PHASE 15
+
+typedef struct gq_param_gate {
+    int32_t op_index;   /* op of the template this entry binds               */
+    int32_t gate;       /* GQ_PG_* family                                     */
+    int32_t num_angles; /* the family's angle count (1, 2 or 3)               */
+    int32_t param[3];
+    double scale[3];
+    double shift[3];
+} gq_param_gate;
+
+/* Adjoint gradient (as gq_sv_adjoint_gradient) of the template bound at theta. */
+int gq_sv_adjoint_template(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_param_gate* pgates, size_t n_pgates,
+                           const double* theta, size_t n_params, const gq_pauli_term* terms, size_t n_terms,
+                           double* grad_out, double* energy_out);
+
+/* Adam options (algorithm/optim/adam.go:9-49, optim.go:21-58); zero or
+ * negative fields take goqu's defaults: lr 0.001, beta1 0.9, beta2 0.999,
+ * epsilon 1e-8, max_iter 1000, fun_tol 1e-8; grad_tol 0 disables that test. */
+typedef struct gq_adam_options {
+    double lr, beta1, beta2, epsilon;
+    int32_t max_iter;
+    int32_t reserved;
+    double fun_tol;
+    double grad_tol;
+} gq_adam_options;
+
+/* optim.Result (algorithm/optim/optim.go:60-69). */
+typedef struct gq_optim_result {
+    double fun;
+    int32_t iterations;
+    int32_t func_evals;
+    int32_t grad_evals;
+    int32_t converged;
+} gq_optim_result;
+
+/* optim.Adam.Minimize (adam.go:51-140) of E(theta) = Re <psi(theta)|H|psi(theta)>
+ * with adjoint gradients (vqe.Run with the Adam optimizer and an adjoint
+ * GradientFunc, algorithm/vqe/vqe.go:50-89). The loop runs inside the library:
+ * each iteration binds the template, and one forward + reverse sweep yields
+ * both the energy goqu evaluates after an update and the gradient of the
+ * next iteration, so there is one device evaluation per iteration and the
+ * state stays on the device. x holds x0 and receives the result's X;
+ * history_out (optional, history_cap entries) receives every energy
+ * evaluated, in order (vqe.Result.History). Counts follow goqu's. */
+int gq_sv_minimize_adam(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_param_gate* pgates, size_t n_pgates,
+                        const gq_pauli_term* terms, size_t n_terms, size_t n_params, double* x,
+                        const gq_adam_options* opts, gq_optim_result* result, double* history_out,
+                        size_t history_cap);
+
 /* ---- dynamic circuits: replaces measureQubit (sim/statevector/dynamic.go:179-230) ----
  * The per-shot control flow of RunDynamic (dynamic.go:14-177) stays on the
  * host; shots sharing a measurement history share one device state. */

@@ -86,6 +86,26 @@ def test_adjoint_20q_400_params():
     assert abs(e - oracle_energy(c, names, x, h, threads=8)) < 1e-10
 
 
+def test_adjoint_phase_gates_on_populated_qubits():
+    # P, U1 and CP whose phase lands on amplitudes that are populated: their
+    # derivative is i e^(i phi) on the last diagonal entry only
+    a, b = prm.New("a"), prm.New("b")
+    c = (ir.Builder("ph", 3).H(0).H(1).H(2).SymPhase(a, 0).SymCP(a, 0, 1).Apply(prm.SymU1(prm.Mul(2.0, b)), 2)
+         .CNOT(1, 2).SymCP(b, 2, 0).H(0).H(2).Build())
+    h = P.NewPauliSum([P.NewPauliString(1.0, {0: P.X}, 3), P.NewPauliString(0.5, {0: P.Z, 1: P.Y}, 3),
+                       P.NewPauliString(-0.3, {2: P.X, 1: P.X}, 3)])
+    names = ir.FreeParameters(c)
+    x = np.array([0.7, -1.1])
+    e, g = gradient.AdjointEvaluator(c, h, names)(x)
+    fd = []
+    for i in range(len(names)):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += 1e-5
+        xm[i] -= 1e-5
+        fd.append((oracle_energy(c, names, xp, h) - oracle_energy(c, names, xm, h)) / 2e-5)
+    np.testing.assert_allclose(g, fd, atol=1e-8, rtol=0)
+
+
 def test_adjoint_checkpoints_agree():
     c, names = workloads.hardware_efficient_ansatz(10, 4)
     h = workloads.ising_hamiltonian(10)
