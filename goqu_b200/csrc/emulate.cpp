@@ -603,4 +603,31 @@ int gqx_param_gate(int family, const double* angles, int n_angles, int k, double
     return (int)m.size();
 }
 
+// FNV-1a digest of the plan-cache keys of every reverse (adjoint) pass the
+// engine would run for `ops`: equal digests mean the specialised kernels
+// compiled for one binding serve the other.
+int gqx_adjoint_plan_digest(int nq, int precision, const gq_op* ops, size_t n_ops, size_t n_params, uint64_t* digest,
+                            int64_t* passes) {
+    const int nphys = nq < gq::RQ ? gq::RQ : nq;
+    std::vector<gq::NGate> fwd, rev;
+    std::vector<int> fo, ro;
+    int rc = gq::adjoint_gates(nq, ops, n_ops, n_params, fwd, rev, fo, ro, g_err);
+    if (rc != GQ_OK) return rc;
+    gq::SchedOptions opt;
+    opt.tile_qubits = 11;
+    opt.budget = 320;
+    opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
+    opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    gq::Program pr;
+    gq::schedule(rev, nphys, opt, pr);
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < pr.passes.size(); ++i) {
+        const std::string k = gq::jit_plan_key(pr, i, precision == GQ_C64, 1 << (pr.passes[i].m - gq::RQ), 2, false, true);
+        for (unsigned char ch : k) h = (h ^ ch) * 1099511628211ull;
+    }
+    *digest = h;
+    *passes = (int64_t)pr.passes.size();
+    return GQ_OK;
+}
+
 }  // extern "C"

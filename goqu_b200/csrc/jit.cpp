@@ -157,56 +157,12 @@ PlanCache& plan_cache() {
     return *c;
 }
 
-template <class V>
-void put(std::string& k, const V& v) {
-    k.append(reinterpret_cast<const char*>(&v), sizeof(V));
-}
 
 }  // namespace
 
 const CachedPlan* jit_cached_plan(const Program& pr, size_t pi, bool c64, int threads, int min_blocks,
                                   bool persistent, bool dual) {
-    const PassDesc& pd = pr.passes[pi];
-    uint32_t op_base, pool_base;
-    jit_bases(pr, pi, &op_base, &pool_base);
-    std::string key;
-    key.reserve(4096);
-    put(key, (int)c64);
-    put(key, threads);
-    put(key, min_blocks);
-    put(key, (int)persistent);
-    put(key, (int)dual);
-    put(key, pd.m);
-    put(key, pd.n_outer);
-    put(key, pd.n_phases);
-    key.append((const char*)pd.tile_q, sizeof(int32_t) * pd.m);
-    key.append((const char*)pd.acol, sizeof(uint32_t) * pd.m);
-    key.append((const char*)pd.outer_q, sizeof(int32_t) * pd.n_outer);
-    for (int p = 0; p < pd.n_phases; ++p) {
-        const PhaseDesc& ph = pr.phases[pd.phase0 + p];
-        key.append((const char*)ph.rslot, sizeof(ph.rslot));
-        key.append((const char*)ph.tlo_slot, sizeof(ph.tlo_slot));
-        key.append((const char*)ph.thi_slot, sizeof(ph.thi_slot));
-        key.append((const char*)ph.tlo_glob, sizeof(ph.tlo_glob));
-        key.append((const char*)ph.thi_glob, sizeof(ph.thi_glob));
-        put(key, ph.op_end - ph.op_begin);
-        for (int o = ph.op_begin; o < ph.op_end; ++o) {
-            const KOp& op = pr.ops[o];
-            const uint8_t b[8] = {op.type, op.t0, op.t1, op.t2, op.creg, op.nreg, op.flags, (uint8_t)op.slot};
-            key.append((const char*)b, 8);
-            put(key, op.mat - pool_base);
-            put(key, op.cmask);
-            put(key, op.dmask);
-            put(key, op.ridx);
-            if (op.type == K_U1 && !op.cmask) {
-                double t;
-                Z l, a, c;
-                put(key, (int)u1_decompose(&pr.pool[op.mat], &t, &l, &a, &c));
-            }
-        }
-    }
-    if (!dual)  // which one-qubit chains the forward kernel fuses
-        for (const ChainCand& cc : jit_chains(pr, pi)) put(key, (int)cc.fusable);
+    const std::string key = jit_plan_key(pr, pi, c64, threads, min_blocks, persistent, dual);
     PlanCache& pc = plan_cache();
     std::lock_guard<std::mutex> lk(pc.mu);
     auto it = pc.map.find(key);

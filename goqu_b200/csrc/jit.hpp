@@ -129,6 +129,12 @@ struct CachedPlan {
     const void* fn = nullptr;  // compiled kernel, once ready
     bool failed = false;    // compilation or loading failed
 };
+// The plan cache's key of pass `pass`: everything the generated kernel's text
+// depends on (launch shape, tile and phase tables, op kinds, bits, controls
+// and pass-relative pool offsets, which unitaries take the shear form, which
+// chains fuse), not the numbers.
+std::string jit_plan_key(const Program& pr, size_t pass, bool c64, int threads, int min_blocks, bool persistent,
+                         bool dual);
 const CachedPlan* jit_cached_plan(const Program& pr, size_t pass, bool c64, int threads, int min_blocks,
                                   bool persistent, bool dual = false);
 // The compiled kernel of a cached plan (queues its compilation on first call);

@@ -163,6 +163,59 @@ using PendT = std::vector<Pend>;
 
 }  // namespace
 
+namespace {
+template <class V>
+void put_key(std::string& k, const V& v) {
+    k.append(reinterpret_cast<const char*>(&v), sizeof(V));
+}
+}  // namespace
+
+std::string jit_plan_key(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, bool persistent,
+                         bool dual) {
+    const PassDesc& pd = pr.passes[pi];
+    uint32_t op_base, pool_base;
+    jit_bases(pr, pi, &op_base, &pool_base);
+    std::string key;
+    key.reserve(4096);
+    put_key(key, (int)c64);
+    put_key(key, threads);
+    put_key(key, min_blocks);
+    put_key(key, (int)persistent);
+    put_key(key, (int)dual);
+    put_key(key, pd.m);
+    put_key(key, pd.n_outer);
+    put_key(key, pd.n_phases);
+    key.append((const char*)pd.tile_q, sizeof(int32_t) * pd.m);
+    key.append((const char*)pd.acol, sizeof(uint32_t) * pd.m);
+    key.append((const char*)pd.outer_q, sizeof(int32_t) * pd.n_outer);
+    for (int p = 0; p < pd.n_phases; ++p) {
+        const PhaseDesc& ph = pr.phases[pd.phase0 + p];
+        key.append((const char*)ph.rslot, sizeof(ph.rslot));
+        key.append((const char*)ph.tlo_slot, sizeof(ph.tlo_slot));
+        key.append((const char*)ph.thi_slot, sizeof(ph.thi_slot));
+        key.append((const char*)ph.tlo_glob, sizeof(ph.tlo_glob));
+        key.append((const char*)ph.thi_glob, sizeof(ph.thi_glob));
+        put_key(key, ph.op_end - ph.op_begin);
+        for (int o = ph.op_begin; o < ph.op_end; ++o) {
+            const KOp& op = pr.ops[o];
+            const uint8_t b[8] = {op.type, op.t0, op.t1, op.t2, op.creg, op.nreg, op.flags, (uint8_t)op.slot};
+            key.append((const char*)b, 8);
+            put_key(key, op.mat - pool_base);
+            put_key(key, op.cmask);
+            put_key(key, op.dmask);
+            put_key(key, op.ridx);
+            if (op.type == K_U1 && !op.cmask) {
+                double t;
+                Z l, a, c;
+                put_key(key, (int)u1_decompose(&pr.pool[op.mat], &t, &l, &a, &c));
+            }
+        }
+    }
+    if (!dual)  // which one-qubit chains the forward kernel fuses
+        for (const ChainCand& cc : jit_chains(pr, pi)) put_key(key, (int)cc.fusable);
+    return key;
+}
+
 bool u1_decompose(const Z* m, double* t, Z* lam, Z* post0, Z* post1) {
     // unitary: columns orthonormal
     const double n0 = m[0].re * m[0].re + m[0].im * m[0].im + m[2].re * m[2].re + m[2].im * m[2].im;

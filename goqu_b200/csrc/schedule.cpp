@@ -1185,7 +1185,18 @@ int adjoint_gates(int nq, const gq_op* ops, size_t n_ops, size_t n_params, std::
                 return GQ_EINVAL;
             }
             std::vector<Z> du((const Z*)op.dmatrix[p], (const Z*)op.dmatrix[p] + dim * dim);
-            int rc = grad_gate(mul(du, ud, dim), qs, ctrl, pi, reverse, err);
+            // G = dU U^dagger. For rotations it does not depend on the angle
+            // (-i/2 times a Pauli string), but the product's zero entries
+            // carry rounding noise of a few ulps that depends on it. Entries
+            // below 1e-12 of the largest are zero, so G's structure (controls,
+            // diagonal, X-type), and with it the specialised kernels' cache
+            // key, stays the same when the angles change.
+            std::vector<Z> g = mul(du, ud, dim);
+            double gmax = 0.0;
+            for (const Z& v : g) gmax = std::max(gmax, std::hypot(v.re, v.im));
+            for (Z& v : g)
+                if (std::hypot(v.re, v.im) <= 1e-12 * gmax) v = Z{0.0, 0.0};
+            int rc = grad_gate(g, qs, ctrl, pi, reverse, err);
             if (rc != GQ_OK) {
                 err = "op " + std::to_string(ii) + ": " + err;
                 return rc;

@@ -111,3 +111,23 @@ def test_adam_on_a_quadratic():
     assert r.FuncEvals == r.Iterations + 1 and r.GradEvals == r.Iterations
     with pytest.raises(ValueError, match="gradient function required"):
         optim.Adam().Minimize(f, np.zeros(3), None)
+
+
+def test_reverse_plans_do_not_depend_on_the_angles(emu):
+    # G = dU U^dagger of a rotation is -i/2 times a Pauli string at every
+    # angle; the reverse passes' kernel keys must not change with theta, or
+    # an optimisation loop would compile new kernels at every step
+    from goqu_b200 import workloads
+    f = emu.gqx_adjoint_plan_digest
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_abi.gq_op), ctypes.c_size_t, ctypes.c_size_t,
+                  ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int64)]
+    c, names = workloads.hardware_efficient_ansatz(20, 10)
+    digests = set()
+    for seed in range(4):
+        x = np.random.default_rng(seed).uniform(0, 2 * np.pi, len(names))
+        s = encode.statevector_ops(c, {nm: float(x[i]) for i, nm in enumerate(names)}, names)
+        d, n = ctypes.c_uint64(), ctypes.c_int64()
+        assert f(20, _abi.GQ_C128, s.ptr(), len(s), len(names), ctypes.byref(d), ctypes.byref(n)) == 0
+        digests.add(d.value)
+    assert len(digests) == 1 and n.value > 10
