@@ -80,17 +80,27 @@ class Batch:
         return self.run_encoded(streams, terms, [len(e[1]) for e in evaluations], gradients)
 
 
-def split_by_work(evaluations, world):
-    """Indices of each rank's share of a batch, balanced by state size: the
-    largest circuits first, each to the rank with the least work so far
-    (work = 2^n per circuit)."""
+def circuit_work(evaluation, gradients=True):
+    """Device work of one batch item, in amplitude-ops: the state size 2^n
+    times its gate count, the reverse sweep (two states, every gate again)
+    counting twice more when gradients are taken. Depth matters as much as
+    size: a QAOA circuit of depth 4 costs about four times one of depth 1."""
+    c = evaluation[0]
+    gates = sum(1 for op in c.Ops() if op.Gate is not None)
+    return (1 << c.NumQubits()) * max(1, gates) * (3 if gradients else 1)
+
+
+def split_by_work(evaluations, world, gradients=True):
+    """Indices of each rank's share of a batch, balanced by device work
+    (circuit_work): the largest items first, each to the rank with the least
+    work so far."""
+    work = [circuit_work(e, gradients) for e in evaluations]
     load = [0] * world
     shares = [[] for _ in range(world)]
-    order = sorted(range(len(evaluations)), key=lambda i: -(1 << evaluations[i][0].NumQubits()))
-    for i in order:
+    for i in sorted(range(len(evaluations)), key=lambda i: -work[i]):
         r = min(range(world), key=lambda k: (load[k], k))
         shares[r].append(i)
-        load[r] += 1 << evaluations[i][0].NumQubits()
+        load[r] += work[i]
     return [sorted(x) for x in shares]
 
 
@@ -99,7 +109,7 @@ def run_sharded(evaluations, rank, world, precision=_abi.GQ_C64, gradients=True,
     its own device and the energies and gradients are all-gathered; returns
     the whole batch's results in input order on every rank. The gather of
     scalars is the only collective (torch.distributed, any backend)."""
-    share = split_by_work(evaluations, world)[rank]
+    share = split_by_work(evaluations, world, gradients)[rank]
     mine = [evaluations[i] for i in share]
     if runner is None:
         b = Batch(precision)

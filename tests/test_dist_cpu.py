@@ -63,10 +63,18 @@ def test_two_rank_plumbing_and_sharded_batch():
         assert all(np.allclose(a, b) for a, b in zip(g, want_g))
 
 
-def test_split_by_work_balances_state_sizes():
+def test_split_by_work_balances_size_and_depth():
     from goqu_b200 import batch, workloads
     evals = workloads.qaoa_batch(200, seed=5)
     shares = batch.split_by_work(evals, 4)
     assert sorted(i for s in shares for i in s) == list(range(200))
-    work = [sum(1 << evals[i][0].NumQubits() for i in s) for s in shares]
-    assert max(work) - min(work) <= 1 << 20  # within one of the largest circuits
+    w = [batch.circuit_work(e) for e in evals]
+    work = [sum(w[i] for i in s) for s in shares]
+    assert max(work) - min(work) <= max(w)  # within one of the largest items
+    # depth counts: circuits of equal size but four times the layers weigh about four times as much
+    deep = [e for e in evals if e[0].NumQubits() == 20]
+    p_of = [len(e[1]) // 2 for e in deep]
+    w1 = [batch.circuit_work(e) for e, p in zip(deep, p_of) if p == 1]
+    w4 = [batch.circuit_work(e) for e, p in zip(deep, p_of) if p == 4]
+    if w1 and w4:
+        assert 3.0 < min(w4) / max(w1) < 4.5
