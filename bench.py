@@ -343,6 +343,33 @@ def extra_vqe(iters=20):
             "max_abs_x_diff_library_vs_host": float(np.max(np.abs(r_dev.X - r_host.X)))}
 
 
+def first_call(n=28):
+    """Seconds of the first Evolve of the benchmark circuit in this process
+    (specialised kernels compiled, or read from the on-disk cache, and loaded)."""
+    from goqu_b200 import _abi, statevector
+    c, stream, gates = build_workload(n)
+    sim = statevector.New(n)
+    sim.set_option(_abi.GQ_OPT_JIT, 2)
+    t0 = time.perf_counter()
+    sim.evolve_ops(stream)
+    sim.Close()
+    return time.perf_counter() - t0
+
+
+def extra_cold_start():
+    """The first call of a fresh process, once the kernels this run compiled
+    are in the on-disk cache (GQ_JIT_CACHE_DIR), against this process's first
+    call, which compiled them."""
+    out = subprocess.run([sys.executable, os.path.abspath(__file__), "--first-call"], capture_output=True,
+                         text=True, env=dict(os.environ), timeout=600)
+    line = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    if out.returncode != 0 or not line:
+        return {"error": (out.stderr or out.stdout)[-400:]}
+    return {"workload": workload_name(28, "c128"),
+            "first_call_s_new_process_disk_cache": json.loads(line[-1])["first_call_s"],
+            "cache": "on-disk cubins keyed by compiler, header and kernel text (GQ_JIT_CACHE_DIR)"}
+
+
 def extra_density():
     """Noisy 12-qubit density matrix: 30 U3 + CNOT brickwork layers,
     depolarizing 1e-3 after every gate, amplitude damping 1e-3 on idle qubits."""
@@ -627,7 +654,8 @@ def run_gpu(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_extras:
         extras = {}
         for name, fn in (("parity_20q", extra_parity), ("adjoint", extra_adjoint), ("density_matrix", extra_density),
-                         ("qaoa_batch", extra_qaoa), ("vqe_loop", extra_vqe), ("parity_28q", extra_parity_28q)):
+                         ("qaoa_batch", extra_qaoa), ("vqe_loop", extra_vqe), ("cold_start", extra_cold_start),
+                         ("parity_28q", extra_parity_28q)):
             try:
                 extras[name] = fn()
             except Exception as exc:  # an extra must not hide the headline line
@@ -652,16 +680,25 @@ def main():
     ap.add_argument("--jit", type=int, choices=[0, 1, 2], default=2,
                     help="specialised pass kernels: 0 off, 1 when compiled, 2 wait for them (default)")
     ap.add_argument("--only-extra", choices=["parity_20q", "adjoint", "density_matrix", "qaoa_batch", "parity_28q",
-                                             "vqe_loop"],
+                                             "vqe_loop", "cold_start"],
                     help="run one extra workload alone and print its JSON (profiling)")
     ap.add_argument("--qaoa-qubits", type=int, default=0, help="qaoa_batch: keep the circuits of this size")
     ap.add_argument("--qaoa-count", type=int, default=0, help="qaoa_batch: keep the first N circuits")
     ap.add_argument("--qaoa-calls", type=int, default=3)
     ap.add_argument("--qaoa-graph", type=int, choices=[0, 1], default=1)
+    ap.add_argument("--first-call", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.first_call:
+        print(json.dumps({"first_call_s": first_call(args.qubits)}))
+        return
+    # the run's first call compiles its kernels: a private, empty on-disk cache
+    # (the cold_start extra then measures a new process reading it)
+    if "GQ_JIT_CACHE_DIR" not in os.environ:
+        import tempfile
+        os.environ["GQ_JIT_CACHE_DIR"] = tempfile.mkdtemp(prefix="gqb200_jit_")
     if args.only_extra:
         fns = {"parity_20q": extra_parity, "adjoint": extra_adjoint, "density_matrix": extra_density,
-               "parity_28q": extra_parity_28q, "vqe_loop": extra_vqe,
+               "parity_28q": extra_parity_28q, "vqe_loop": extra_vqe, "cold_start": extra_cold_start,
                "qaoa_batch": lambda: extra_qaoa(args.qaoa_qubits, args.qaoa_count, args.qaoa_calls,
                                                 args.qaoa_graph == 1)}
         print(json.dumps({args.only_extra: fns[args.only_extra]()}))

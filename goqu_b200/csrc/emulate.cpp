@@ -630,4 +630,19 @@ int gqx_adjoint_plan_digest(int nq, int precision, const gq_op* ops, size_t n_op
     return GQ_OK;
 }
 
+// jit_compile_cached on a kernel text (cache directory from the environment):
+// *from_disk tells whether the cubin came from the cache; returns its size.
+int64_t gqx_jit_compile_cached(const char* source, int* from_disk) {
+    std::vector<char> bin;
+    std::string log;
+    bool disk = false;
+    const std::string err = gq::jit_compile_cached(source, &bin, &log, &disk);
+    if (!err.empty()) {
+        g_err = err.substr(0, 4000);
+        return -1;
+    }
+    *from_disk = disk ? 1 : 0;
+    return (int64_t)bin.size();
+}
+
 }  // extern "C"

@@ -33,7 +33,7 @@ struct Cache {
     bool stopping = false;
     std::vector<std::thread> workers;
     double compile_ms = 0;
-    int64_t compiled = 0, failed = 0;
+    int64_t compiled = 0, failed = 0, from_cache = 0;
 
     void start() {
         if (!workers.empty()) return;
@@ -62,7 +62,8 @@ struct Cache {
             std::vector<char> bin;
             std::string log;
             const auto t0 = std::chrono::steady_clock::now();
-            const std::string err = jit_compile_only(*key, &bin, &log);
+            bool from_disk = false;
+            const std::string err = jit_compile_cached(*key, &bin, &log, &from_disk);
             const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             {
                 std::lock_guard<std::mutex> lk(mu);
@@ -70,8 +71,9 @@ struct Cache {
                 compile_ms += ms;
                 if (err.empty()) {
                     e.cubin.swap(bin);
-                    e.state = JIT_PENDING;  // compiled; loaded by the next lookup
+                    e.state = JIT_PENDING;  // compiled (or read from disk); loaded by the next lookup
                     ++compiled;
+                    if (from_disk) ++from_cache;
                 } else {
                     e.state = JIT_FAILED;
                     ++failed;

@@ -129,6 +129,14 @@ struct CachedPlan {
     const void* fn = nullptr;  // compiled kernel, once ready
     bool failed = false;    // compilation or loading failed
 };
+// Compiles with NVRTC through an on-disk cache: a cubin stored under a hash of
+// everything it depends on (options, NVRTC version, the tile header, the
+// kernel text) is reused when its stored identity equals this one byte for
+// byte; new binaries are written through a temporary file and a rename.
+// Directory: $GQ_JIT_CACHE_DIR ("off" disables), else
+// $XDG_CACHE_HOME/goqu_b200/jit, else ~/.cache/goqu_b200/jit.
+std::string jit_cache_dir();
+std::string jit_compile_cached(const std::string& source, std::vector<char>* cubin, std::string* log, bool* from_disk);
 // The plan cache's key of pass `pass`: everything the generated kernel's text
 // depends on (launch shape, tile and phase tables, op kinds, bits, controls
 // and pass-relative pool offsets, which unitaries take the shear form, which

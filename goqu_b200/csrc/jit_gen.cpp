@@ -4,13 +4,18 @@
 #include "jit.hpp"
 
 #include <dlfcn.h>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <nvrtc.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <thread>
 
 namespace gq {
 
@@ -1208,6 +1213,7 @@ struct Nvrtc {
     nvrtcResult (*cubin_size)(nvrtcProgram, size_t*);
     nvrtcResult (*cubin)(nvrtcProgram, char*);
     nvrtcResult (*destroy)(nvrtcProgram*);
+    nvrtcResult (*version)(int*, int*) = nullptr;
     Nvrtc() {
         const char* names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"};
         void* h = nullptr;
@@ -1221,6 +1227,7 @@ struct Nvrtc {
         cubin_size = (decltype(cubin_size))dlsym(h, "nvrtcGetCUBINSize");
         cubin = (decltype(cubin))dlsym(h, "nvrtcGetCUBIN");
         destroy = (decltype(destroy))dlsym(h, "nvrtcDestroyProgram");
+        version = (decltype(version))dlsym(h, "nvrtcVersion");
         ok = create && compile && log_size && log && cubin_size && cubin && destroy;
     }
 };
@@ -1234,6 +1241,11 @@ Nvrtc& nvrtc() {
 
 bool jit_available() { return nvrtc().ok; }
 
+namespace {
+const char* const kJitOpts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--ptxas-options=-v"};
+constexpr int kJitNumOpts = 3;
+}  // namespace
+
 std::string jit_compile_only(const std::string& source, std::vector<char>* cubin, std::string* log) {
     Nvrtc& N = nvrtc();
     if (!N.ok) return "libnvrtc not found";
@@ -1242,8 +1254,7 @@ std::string jit_compile_only(const std::string& source, std::vector<char>* cubin
     const char* hdr_name[] = {"tile_core.cuh"};
     if (N.create(&prog, source.c_str(), "gqj_pass.cu", 1, hdr_src, hdr_name) != NVRTC_SUCCESS)
         return "nvrtcCreateProgram failed";
-    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--ptxas-options=-v"};
-    const nvrtcResult rc = N.compile(prog, 3, opts);
+    const nvrtcResult rc = N.compile(prog, kJitNumOpts, kJitOpts);
     size_t ls = 0;
     N.log_size(prog, &ls);
     std::string lg(ls, '\0');
@@ -1260,6 +1271,94 @@ std::string jit_compile_only(const std::string& source, std::vector<char>* cubin
         N.cubin(prog, cubin->data());
     }
     N.destroy(&prog);
+    return "";
+}
+
+// ---- on-disk cache of compiled kernels -------------------------------------
+
+namespace {
+
+// Everything the binary depends on: cache format, compiler options, NVRTC
+// version, the embedded tile header and the kernel text.
+std::string jit_identity(const std::string& source) {
+    std::string id = "goqu_b200 jit cubin v1\n";
+    for (int i = 0; i < kJitNumOpts; ++i) id += std::string(kJitOpts[i]) + "\n";
+    int maj = 0, mnr = 0;
+    if (nvrtc().version) nvrtc().version(&maj, &mnr);
+    id += "nvrtc " + std::to_string(maj) + "." + std::to_string(mnr) + "\n";
+    id += kTileCore;
+    id += "\n";
+    id += source;
+    return id;
+}
+
+uint64_t fnv1a(const std::string& s) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char c : s) h = (h ^ c) * 1099511628211ull;
+    return h;
+}
+
+}  // namespace
+
+std::string jit_cache_dir() {
+    const char* env = std::getenv("GQ_JIT_CACHE_DIR");
+    if (env) return std::string(env) == "off" ? std::string() : std::string(env);
+    const char* xdg = std::getenv("XDG_CACHE_HOME");
+    if (xdg && *xdg) return std::string(xdg) + "/goqu_b200/jit";
+    const char* home = std::getenv("HOME");
+    return home && *home ? std::string(home) + "/.cache/goqu_b200/jit" : std::string();
+}
+
+std::string jit_compile_cached(const std::string& source, std::vector<char>* cubin, std::string* log, bool* from_disk) {
+    *from_disk = false;
+    const std::string dir = jit_cache_dir();
+    if (dir.empty()) return jit_compile_only(source, cubin, log);
+    const std::string id = jit_identity(source);
+    char name[32];
+    std::snprintf(name, sizeof(name), "%016llx.cubin", (unsigned long long)fnv1a(id));
+    const std::string path = dir + "/" + name;
+    // a hit needs the stored identity to equal this one byte for byte
+    if (FILE* f = std::fopen(path.c_str(), "rb")) {
+        uint64_t idn = 0, cn = 0;
+        std::string stored;
+        std::vector<char> bin;
+        bool ok = std::fread(&idn, 8, 1, f) == 1 && idn == id.size();
+        if (ok) {
+            stored.resize(idn);
+            ok = std::fread(&stored[0], 1, idn, f) == idn && stored == id && std::fread(&cn, 8, 1, f) == 1 &&
+                 cn > 0 && cn < (1ull << 30);
+        }
+        if (ok) {
+            bin.resize(cn);
+            ok = std::fread(bin.data(), 1, cn, f) == cn;
+        }
+        std::fclose(f);
+        if (ok) {
+            if (cubin) cubin->swap(bin);
+            if (log) log->clear();
+            *from_disk = true;
+            return "";
+        }
+    }
+    std::vector<char> bin;
+    const std::string err = jit_compile_only(source, &bin, log);
+    if (!err.empty()) return err;
+    // write to a private temporary file, then rename over the final name
+    std::string cmd_dir = dir;
+    for (size_t i = 1; i <= cmd_dir.size(); ++i)
+        if (i == cmd_dir.size() || cmd_dir[i] == '/') mkdir(cmd_dir.substr(0, i).c_str(), 0700);
+    const std::string tmp = path + "." + std::to_string((long long)getpid()) + "." +
+                            std::to_string((unsigned long long)std::hash<std::thread::id>()(std::this_thread::get_id())) +
+                            ".tmp";
+    if (FILE* f = std::fopen(tmp.c_str(), "wb")) {
+        const uint64_t idn = id.size(), cn = bin.size();
+        const bool ok = std::fwrite(&idn, 8, 1, f) == 1 && std::fwrite(id.data(), 1, idn, f) == idn &&
+                        std::fwrite(&cn, 8, 1, f) == 1 && std::fwrite(bin.data(), 1, cn, f) == cn;
+        const bool closed = std::fclose(f) == 0;
+        if (ok && closed) std::rename(tmp.c_str(), path.c_str());
+        else std::remove(tmp.c_str());
+    }
+    if (cubin) cubin->swap(bin);
     return "";
 }
 

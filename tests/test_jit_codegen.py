@@ -261,3 +261,31 @@ def test_dual_kernels_compile(emu, precision):
         assert rc == 0, emu.gqx_last_error().decode()[:3000]
         passes, planned, compiled = list(out)
         assert planned == passes >= 1 and compiled >= 1
+
+
+def test_on_disk_kernel_cache(emu, tmp_path, monkeypatch):
+    # compiled kernels are stored under a hash of everything they depend on and
+    # reused by later compilations (other processes included); a stored file
+    # whose identity differs is never used
+    f = emu.gqx_jit_compile_cached
+    f.restype = ctypes.c_int64
+    f.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+    monkeypatch.setenv("GQ_JIT_CACHE_DIR", str(tmp_path / "jit"))
+    src = b"extern \"C\" __global__ void gqj_pass(double* x) { x[threadIdx.x] *= 2.0; }\n"
+    hit = ctypes.c_int()
+    n1 = f(src, ctypes.byref(hit))
+    assert n1 > 0 and hit.value == 0
+    files = list((tmp_path / "jit").iterdir())
+    assert len(files) == 1 and files[0].suffix == ".cubin"
+    n2 = f(src, ctypes.byref(hit))
+    assert n2 == n1 and hit.value == 1
+    # a different kernel text is a different entry
+    assert f(src.replace(b"2.0", b"3.0"), ctypes.byref(hit)) > 0 and hit.value == 0
+    # a file whose stored identity does not match is ignored and rewritten
+    data = bytearray(files[0].read_bytes())
+    data[20] ^= 0xFF
+    files[0].write_bytes(bytes(data))
+    assert f(src, ctypes.byref(hit)) == n1 and hit.value == 0
+    assert f(src, ctypes.byref(hit)) == n1 and hit.value == 1
+    monkeypatch.setenv("GQ_JIT_CACHE_DIR", "off")
+    assert f(src, ctypes.byref(hit)) == n1 and hit.value == 0
