@@ -151,6 +151,14 @@ GQ_PG = {"RX": 1, "RY": 2, "RZ": 3, "P": 4, "U1": 5, "U2": 6, "U3": 7, "Rot": 8,
          "RZZ": 12, "FSim": 13, "PSwap": 14, "GlobalPhase": 15}
 
 
+class gq_qaoa_item(ctypes.Structure):
+    _fields_ = [
+        ("num_qubits", ctypes.c_int32), ("p", ctypes.c_int32), ("edges", ctypes.POINTER(ctypes.c_int32)),
+        ("n_edges", ctypes.c_size_t), ("gammas", ctypes.POINTER(ctypes.c_double)),
+        ("betas", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
 class GQError(RuntimeError):
     """An engine call returned a non-zero status."""
 
@@ -227,6 +235,7 @@ SIGNATURES = {
                                     _DBL_P, _DBL_P]),
     "gq_sv_minimize_adam": (_I, [_VP, _OPP, _SZ, ctypes.POINTER(gq_param_gate), _SZ, _TP, _SZ, _SZ, _DBL_P,
                                  ctypes.POINTER(gq_adam_options), ctypes.POINTER(gq_optim_result), _DBL_P, _SZ]),
+    "gq_qaoa_maxcut_batch": (_I, [_I, ctypes.POINTER(gq_qaoa_item), _SZ, _I, _DBL_P, _DBL_P]),
     "gq_unitary": (_I, [_I, _OPP, _SZ, _DBL_P, _SZ]),
     "gq_equivalent": (_I, [_I, _OPP, _SZ, _OPP, _SZ, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),
     "gq_equivalent_on_zero": (_I, [_I, _OPP, _SZ, _OPP, _SZ, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]),

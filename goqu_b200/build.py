@@ -17,7 +17,7 @@ NVCC_FLAGS = [
     "-shared",
 ]
 
-ENGINE_SOURCES = ["engine.cu", "noalloc.cu", "schedule.cpp", "jit.cpp", "jit_gen.cpp", "params.cpp"]
+ENGINE_SOURCES = ["engine.cu", "noalloc.cu", "qaoa.cu", "schedule.cpp", "jit.cpp", "jit_gen.cpp", "params.cpp"]
 EMULATOR_SOURCES = ["emulate.cpp", "schedule.cpp", "jit_gen.cpp", "params.cpp"]
 HEADERS = ["tile_core.cuh", "kernels.cuh", "counts.cuh", "verify.cuh", "schedule.hpp", "jit.hpp", "params.hpp", os.path.join("..", "..", "include", "gqb200.h")]
 # tile_core.cuh as a C++ string literal, compiled into the engine for the

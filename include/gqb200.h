@@ -374,6 +374,30 @@ int gq_batch_run(gq_batch* b, const gq_batch_item* items, size_t n_items, int wa
 int gq_batch_set_option(gq_batch* b, int key, int64_t value);
 int gq_batch_stats(const gq_batch* b, gq_stats* out);
 
+/* ---- MaxCut QAOA batches: the evaluations of algorithm/qaoa -----------------
+ * Energies and gradients of many QAOA circuits of goqu's qaoa.Run form
+ * (qaoa.go:68-93, 164-196) for MaxCut Hamiltonians (maxcut.go:13-35): H on
+ * every qubit, then per layer k an RZZ(gamma_k) per edge and RX(2 beta_k) on
+ * every qubit; energy <H> with H = sum_e (-1/2 + 1/2 Z_i Z_j). The same
+ * circuits as gq_batch_run items built from those gates, evaluated by a
+ * dedicated path: a per-circuit table of cut counts makes each cost layer a
+ * lookup, circuits of up to 12 qubits run whole in one CTA's shared memory,
+ * larger ones in batched tile passes. grads_out receives 2p values per item,
+ * [gamma_0, beta_0, gamma_1, beta_1, ...] (the circuit's FreeParameters
+ * order), items concatenated. complex64 only (GQ_EUNSUPPORTED otherwise);
+ * 4 <= num_qubits <= 26, 1 <= n_edges <= 255, 1 <= p <= 64. */
+typedef struct gq_qaoa_item {
+    int32_t num_qubits;
+    int32_t p;
+    const int32_t* edges; /* n_edges pairs (i, j), 0 <= i != j < num_qubits */
+    size_t n_edges;
+    const double* gammas; /* p values */
+    const double* betas;  /* p values */
+} gq_qaoa_item;
+
+int gq_qaoa_maxcut_batch(int precision, const gq_qaoa_item* items, size_t n_items, int want_gradients,
+                         double* energies_out, double* grads_out);
+
 /* ---- sweeps: replaces sweep.RunSim / RunDensitySim (sweep/run.go:27-171) ----
  * Every point is the same circuit bound to different values: `num_qubits`
  * qubits from |0...0> (rho = |0><0| for density matrices), the point's op
