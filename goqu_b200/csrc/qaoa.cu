@@ -391,13 +391,11 @@ __global__ void __launch_bounds__(NT) k_qaoa_reverse(const Group g, const Pass p
 template <bool REV>
 __device__ void small_mixer(float2* sp, float2* sl, int n, uint32_t t, float c, float s, double* gb) {
     const int rounds = (n + 3) / 4;
-    const bool active = t < (1u << (n - 4));  // 2^(n-4) threads hold 16 amplitudes each
+    // 2^(n-4) threads hold 16 amplitudes each; the block's other threads (a
+    // warp is the smallest block) only pass the same barriers: every thread
+    // executes both __syncthreads of every round, at the same instructions.
+    const bool active = t < (1u << (n - 4));
     for (int r = 0; r < rounds; ++r) {
-        if (!active) {  // the block's other threads only take part in its barriers
-            __syncthreads();
-            __syncthreads();
-            continue;
-        }
         // register bits: qubits q[0..3]; rotated: those < n not yet rotated
         int q[4];
         uint32_t m = 0;
@@ -422,23 +420,27 @@ __device__ void small_mixer(float2* sp, float2* sl, int n, uint32_t t, float c, 
             idx[j] = v;
         }
         float2 a[16], b[16];
+        if (active) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) a[j] = sp[idx[j]];
-        if (REV) {
+            for (int j = 0; j < 16; ++j) a[j] = sp[idx[j]];
+            if (REV) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) b[j] = sl[idx[j]];
-            *gb += xgrad_masked(a, b, m);
-            rx_masked(a, m, c, -s);
-            rx_masked(b, m, c, -s);
-        } else {
-            rx_masked(a, m, c, s);
+                for (int j = 0; j < 16; ++j) b[j] = sl[idx[j]];
+                *gb += xgrad_masked(a, b, m);
+                rx_masked(a, m, c, -s);
+                rx_masked(b, m, c, -s);
+            } else {
+                rx_masked(a, m, c, s);
+            }
         }
         __syncthreads();
+        if (active) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) sp[idx[j]] = a[j];
-        if (REV) {
+            for (int j = 0; j < 16; ++j) sp[idx[j]] = a[j];
+            if (REV) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) sl[idx[j]] = b[j];
+                for (int j = 0; j < 16; ++j) sl[idx[j]] = b[j];
+            }
         }
         __syncthreads();
     }
