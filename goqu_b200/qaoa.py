@@ -38,38 +38,53 @@ def from_evaluation(ev):
     return c.NumQubits(), edges_of(h), x[0::2].copy(), x[1::2].copy()
 
 
-class MaxCutBatch:
-    """Energies (and gradients) of MaxCut QAOA circuits on one device."""
+class Encoded:
+    """Items packed for gq_qaoa_maxcut_batch (the arrays the records point to
+    are kept alive here); reuse it while the circuits stay the same."""
 
-    def __init__(self, precision=_abi.GQ_C64):
-        self.precision = precision
-
-    def Run(self, items, gradients=True):
-        """items: (n, edges, gammas, betas) each; returns (energies, list of gradient arrays or None)."""
-        keep = []
-        arr = (_abi.gq_qaoa_item * max(1, len(items)))()
-        total = 0
+    def __init__(self, items):
+        self.keep = []
+        self.arr = (_abi.gq_qaoa_item * max(1, len(items)))()
+        self.n = len(items)
+        self.sizes = []
         for i, (n, edges, gammas, betas) in enumerate(items):
             e = np.ascontiguousarray(np.asarray(edges, dtype=np.int32).reshape(-1))
             g = np.ascontiguousarray(gammas, dtype=np.float64)
             b = np.ascontiguousarray(betas, dtype=np.float64)
             if g.size != b.size:
                 raise ValueError("qaoa: gammas and betas differ in length")
-            keep += [e, g, b]
-            arr[i].num_qubits, arr[i].p = int(n), int(g.size)
-            arr[i].edges = e.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
-            arr[i].n_edges = e.size // 2
-            arr[i].gammas, arr[i].betas = g.ctypes.data_as(_D), b.ctypes.data_as(_D)
-            total += 2 * g.size
-        energies = np.empty(max(1, len(items)), dtype=np.float64)
-        grads = np.empty(max(1, total), dtype=np.float64)
-        _abi.check(_abi.lib().gq_qaoa_maxcut_batch(self.precision, arr, len(items), 1 if gradients else 0,
+            self.keep += [e, g, b]
+            self.arr[i].num_qubits, self.arr[i].p = int(n), int(g.size)
+            self.arr[i].edges = e.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            self.arr[i].n_edges = e.size // 2
+            self.arr[i].gammas, self.arr[i].betas = g.ctypes.data_as(_D), b.ctypes.data_as(_D)
+            self.sizes.append(2 * g.size)
+        self.total = int(sum(self.sizes))
+
+
+class MaxCutBatch:
+    """Energies (and gradients) of MaxCut QAOA circuits on one device."""
+
+    def __init__(self, precision=_abi.GQ_C64):
+        self.precision = precision
+
+    @staticmethod
+    def encode(items):
+        return Encoded(items)
+
+    def run_encoded(self, enc, gradients=True):
+        energies = np.empty(max(1, enc.n), dtype=np.float64)
+        grads = np.empty(max(1, enc.total), dtype=np.float64)
+        _abi.check(_abi.lib().gq_qaoa_maxcut_batch(self.precision, enc.arr, enc.n, 1 if gradients else 0,
                                                   energies.ctypes.data_as(_D), grads.ctypes.data_as(_D)))
         if not gradients:
-            return energies[:len(items)], None
+            return energies[:enc.n], None
         out, off = [], 0
-        for n, edges, gammas, betas in items:
-            k = 2 * len(gammas)
+        for k in enc.sizes:
             out.append(grads[off:off + k].copy())
             off += k
-        return energies[:len(items)], out
+        return energies[:enc.n], out
+
+    def Run(self, items, gradients=True):
+        """items: (n, edges, gammas, betas) each; returns (energies, list of gradient arrays or None)."""
+        return self.run_encoded(Encoded(items), gradients)
