@@ -643,6 +643,21 @@ def run_gpu(args, world, rank, local):
         sim.evolve_ops(stream)
         if w == 0:
             t_first = time.perf_counter() - t_first
+    # the autotuner picks the launch choices (pass budget, tile variant, CTAs
+    # per SM) for this circuit, untimed; the timed steps run with its choice
+    tuned = None
+    if args.autotune and not args.budget:
+        from goqu_b200 import autotune
+        t0 = time.perf_counter()
+        tuned = autotune.tune_statevector(sim, stream)
+        tuned = {"best": {str(k): v for k, v in tuned["best"].items()},
+                 "candidates": [{str(k): v for k, v in c.items()} for c in autotune.STATEVECTOR_CANDIDATES],
+                 "timings_ms": tuned.get("timings_ms"), "tuning_s": time.perf_counter() - t0,
+                 "keys": "option numbers of include/gqb200.h (2 pass budget, 5 kernel variant, 11 jit min blocks)"}
+        sim.set_option(_abi.GQ_OPT_TIMING, 1)
+        sim.set_option(_abi.GQ_OPT_JIT, args.jit)
+        for _ in range(2):
+            sim.evolve_ops(stream)
     barrier(world)
     step_ms, pass_ms, launches, passes, jit_passes = [], [], 0, 0, 0
     with ClockSampler(local) as clk:
@@ -705,6 +720,7 @@ def run_gpu(args, world, rank, local):
         "jit": {"mode": args.jit, "passes_specialised_per_step": jit_passes / args.steps,
                 "first_call_s": t_first, "compile_ms_total": sim.stats()["jit_compile_ms"]},
         "clocks": clk.summary(),
+        "autotune": tuned,
     }
     sim.Close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -736,6 +752,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3, help="stratified CPU samples for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--autotune", type=int, choices=[0, 1], default=1,
+                    help="1: the autotuner picks the launch choices before the timed steps (default)")
     ap.add_argument("--jit", type=int, choices=[0, 1, 2], default=2,
                     help="specialised pass kernels: 0 off, 1 when compiled, 2 wait for them (default)")
     ap.add_argument("--only-extra", choices=["parity_20q", "adjoint", "density_matrix", "qaoa_batch", "parity_28q",
