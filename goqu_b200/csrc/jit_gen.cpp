@@ -427,6 +427,14 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
     seg_out += "    }\n";
 
     std::vector<std::string> seg_ph;
+    // The first phase may load its amplitudes straight from global memory and
+    // the last store them straight back (no staging through shared memory, two
+    // barriers fewer) when the phase's lanes run along the lowest qubits
+    // (128-byte runs, as the staging copies) and each register bit is one
+    // tile qubit. direct_in / direct_out record whether they do.
+    const bool direct_ok = !persistent;
+    bool direct_in = false, direct_out = false;
+    const int lane_run = c64 ? 4 : 3;  // lowest qubits a 128-byte run spans
     for (int p = 0; p < pd.n_phases; ++p) {
         const PhaseDesc& ph = pr.phases[pd.phase0 + p];
         out.phase_shears.emplace_back();
@@ -504,8 +512,30 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
                 b += " | (((base & " + hex64(upred[k]) + ") == " + hex64(upred[k]) + ") ? " + hex32(1u << k) + " : 0u)";
             b += ";\n";
         }
+        // global offset of each register slot: register bit k is the tile
+        // qubit whose staging column is rslot[1 << k]
+        uint64_t greg[NREG];
+        bool direct = direct_ok && tbits >= lane_run;
+        for (int k = 0; k < lane_run && direct; ++k) direct = tq[k] == k;
+        for (int k = 0; k < RQ && direct; ++k) {
+            int hit = -1;
+            for (int bb = 0; bb < m; ++bb)
+                if (pd.acol[bb] == ph.rslot[1 << k]) hit = bb;
+            if (hit < 0) direct = false;
+            else greg[1 << k] = 1ull << pd.tile_q[hit];
+        }
+        if (direct) {
+            greg[0] = 0;
+            for (int j = 1; j < NREG; ++j) greg[j] = greg[j & (j - 1)] | greg[j & -j];
+        }
+        const bool load_global = direct && p == 0;
+        const bool store_global = direct && p == pd.n_phases - 1;
+        if (p == 0) direct_in = load_global;
+        if (p == pd.n_phases - 1) direct_out = store_global;
         b += "        cplx<T> a[16];\n";
-        for (int j = 0; j < NREG; ++j) b += "        a[" + num(j) + "] = sm[sb ^ " + hex32(ph.rslot[j]) + "];\n";
+        for (int j = 0; j < NREG; ++j)
+            b += load_global ? "        a[" + num(j) + "] = st[g0 | " + hex64(greg[j]) + "];\n"
+                             : "        a[" + num(j) + "] = sm[sb ^ " + hex32(ph.rslot[j]) + "];\n";
 
         PendT pend[NREG];
         for (int j = 0; j < NREG; ++j) pend[j].assign(NC, Pend());
@@ -762,7 +792,9 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
         flush(0xffffffffu);
         for (int j = 0; j < NREG; ++j) resolve(j);
         if (gen.overflow) return PLAN_OVERFLOW;
-        for (int j = 0; j < NREG; ++j) b += "        sm[sb ^ " + hex32(ph.rslot[j]) + "] = a[" + num(j) + "];\n";
+        for (int j = 0; j < NREG; ++j)
+            b += store_global ? "        st[g0 | " + hex64(greg[j]) + "] = a[" + num(j) + "];\n"
+                              : "        sm[sb ^ " + hex32(ph.rslot[j]) + "] = a[" + num(j) + "];\n";
         b += "    }\n";
         seg_ph.push_back(b);
     }
@@ -786,9 +818,14 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
     if (!persistent) {
         s += "    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);\n";
         s += "    const uint64_t cta = blockIdx.x;\n";
-        s += pro + seg_in + "    __syncthreads();\n";
-        for (const std::string& ph : seg_ph) s += ph + "    __syncthreads();\n";
-        s += seg_out + "}\n";
+        s += pro;
+        if (!direct_in) s += seg_in + "    __syncthreads();\n";
+        for (size_t k = 0; k < seg_ph.size(); ++k) {
+            s += seg_ph[k];
+            if (k + 1 < seg_ph.size() || !direct_out) s += "    __syncthreads();\n";
+        }
+        if (!direct_out) s += seg_out;
+        s += "}\n";
     } else {
         // persistent CTAs, two tile buffers: the next tile's amplitudes are
         // copied asynchronously while the current one runs its phases
@@ -828,9 +865,9 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
         auto loop = [&](const std::string& seg) {
             h += "    for (uint32_t t = 0; t < " + num(threads) + "u; ++t) {\n" + pro + seg + "    }\n";
         };
-        loop(seg_in);
+        if (!direct_in) loop(seg_in);
         for (const std::string& ph : seg_ph) loop(ph);
-        loop(seg_out);
+        if (!direct_out) loop(seg_out);
         h += "    }\n}\n";
     }
     return PLAN_OK;
