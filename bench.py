@@ -630,6 +630,8 @@ def run_gpu(args, world, rank, local):
     sim.set_option(_abi.GQ_OPT_JIT, args.jit)
     if args.budget:
         sim.set_option(_abi.GQ_OPT_PASS_BUDGET, args.budget)
+    if args.variant is not None:
+        sim.set_option(_abi.GQ_OPT_KERNEL_VARIANT, args.variant)
     lib = _abi.lib()
     u = statevector.uniforms(SHOTS, np.random.default_rng(SEED))
     u_p = u.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
@@ -646,7 +648,7 @@ def run_gpu(args, world, rank, local):
     # the autotuner picks the launch choices (pass budget, tile variant, CTAs
     # per SM) for this circuit, untimed; the timed steps run with its choice
     tuned = None
-    if args.autotune and not args.budget:
+    if args.autotune and not args.budget and args.variant is None:
         from goqu_b200 import autotune
         t0 = time.perf_counter()
         tuned = autotune.tune_statevector(sim, stream)
@@ -749,6 +751,7 @@ def main():
     ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
     ap.add_argument("--qubits", type=int, default=28)
     ap.add_argument("--budget", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=None, help="fixed tile-pass launch shape (profiling; no autotuning)")
     ap.add_argument("--cpu-steps", type=int, default=3, help="stratified CPU samples for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
