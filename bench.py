@@ -393,7 +393,9 @@ def extra_density():
     tr = dm.Trace()
     dm.Close()
     peak, peak_kind = peaks()
-    pass_bytes = 2 * 16 * (1 << 24)  # rho (2^24 complex128 entries) read and written once per pass
+    # rho (2^24 complex128 entries) read and written once per pass, less the
+    # tiles the first passes skip while they are still zero
+    pass_bytes = st["tile_bytes"] / max(1, st["passes"])
     pass_ms = float(np.median(pms)) / max(1, st["passes"])
     achieved = pass_bytes / (pass_ms / 1000.0) / 1e9
 
@@ -497,15 +499,16 @@ def extra_parity_28q(n=28, steps=3):
         sim.set_option(_abi.GQ_OPT_JIT, 2)
         for _ in range(2):
             sim.evolve_ops(stream)
-        ms, pms, passes = [], [], 0
+        ms, pms, passes, tbytes = [], [], 0, 0
         for _ in range(steps):
             sim.evolve_ops(stream)
             st = sim.stats()
             ms.append(st["last_ms"])
             pms.append(st["pass_ms"])
             passes += st["passes"]
+            tbytes += st["tile_bytes"]
         launch_ms = float(np.sum(pms)) / max(1, passes)
-        achieved = 2 * amp * (1 << n) / (launch_ms / 1000.0) / 1e9
+        achieved = tbytes / max(1, passes) / (launch_ms / 1000.0) / 1e9
         out[tag] = {"gates_per_s": gates / (float(np.median(ms)) / 1000.0), "ms_device": float(np.median(ms)),
                     "passes": passes // steps,
                     "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -661,7 +664,7 @@ def run_gpu(args, world, rank, local):
         for _ in range(2):
             sim.evolve_ops(stream)
     barrier(world)
-    step_ms, pass_ms, launches, passes, jit_passes = [], [], 0, 0, 0
+    step_ms, pass_ms, launches, passes, jit_passes, tile_bytes = [], [], 0, 0, 0, 0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             sim.evolve_ops(stream)
@@ -671,6 +674,7 @@ def run_gpu(args, world, rank, local):
             launches += st["kernel_launches"]
             passes += st["passes"]
             jit_passes += st["jit_passes"]
+            tile_bytes += st["tile_bytes"]
     barrier(world)
     total_ms = max_over_ranks(float(np.sum(step_ms)), world)
     value = world * gates * args.steps / (total_ms / 1000.0)
@@ -692,17 +696,21 @@ def run_gpu(args, world, rank, local):
     # ---- roofline of the dominant kernel (the tile pass)
     peak, peak_kind = peaks()
     amp_bytes = 8 if args.precision == "c64" else 16
-    alg_bytes = 2 * amp_bytes * (1 << n)  # one read + one write of the state per pass
+    full_bytes = 2 * amp_bytes * (1 << n)  # one read + one write of the whole state
+    # bytes of the tiles the passes launched (the first passes from the reset
+    # state skip the tiles that are still zero), averaged over the launches
+    alg_bytes = tile_bytes / max(1, passes)
     per_launch_ms = float(np.sum(pass_ms)) / max(1, passes)
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
-    traffic = None
+    traffic = traffic_full = None
     tf = os.path.join(ROOT, "profiles", "tile_pass_traffic.json")
     if os.path.exists(tf):
         with open(tf) as f:
             tj = json.load(f)
         t = tj.get(args.precision, {})
         if t.get("bytes_per_launch"):
-            traffic = t["bytes_per_launch"] * 2.0 ** (n - t["qubits"])  # traffic scales with 2^n
+            traffic_full = t["bytes_per_launch"] * 2.0 ** (n - t["qubits"])  # a full-state launch; scales with 2^n
+            traffic = traffic_full * alg_bytes / full_bytes
 
     line = {
         "metric": f"{n}q gates/s", "value": value, "unit": "gates/s", "n_gpus": world, "steps": args.steps,
@@ -712,12 +720,15 @@ def run_gpu(args, world, rank, local):
         "config": {"workload": workload_name(n, args.precision), "qubits": n, "gates": gates, "seed": SEED,
                    "precision": args.precision, "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": f"state {amp_bytes << n >> 20} MiB vs 126 MB L2 (no flush between steps)",
-                   "passes_per_step": passes / args.steps, "pass_ms_per_step": float(np.mean(pass_ms))},
+                   "passes_per_step": passes / args.steps, "pass_ms_per_step": float(np.mean(pass_ms)),
+                   "zero_tile_skip": {"tile_bytes_per_step": tile_bytes / args.steps,
+                                      "full_state_bytes_per_step": full_bytes * passes / args.steps}},
         "e2e": {"value": e2e, "unit": "gates/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": per_launch_ms},
+                     "traffic": traffic, "traffic_full_state_launch": traffic_full, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_bytes, "full_state_bytes_per_launch": full_bytes,
+                     "launch_ms": per_launch_ms},
         "gpu_launches": launches,
         "jit": {"mode": args.jit, "passes_specialised_per_step": jit_passes / args.steps,
                 "first_call_s": t_first, "compile_ms_total": sim.stats()["jit_compile_ms"]},

@@ -55,6 +55,7 @@ GQ_OPT_JIT_MIN_QUBITS = 10
 GQ_OPT_JIT_MIN_BLOCKS = 11
 GQ_OPT_JIT_PERSISTENT = 12
 GQ_OPT_DM_DENSE_CHANNELS = 13
+GQ_OPT_ZERO_TILES = 14
 
 GQ_NOALLOC_MAX_TERMS = 2048
 
@@ -98,6 +99,7 @@ class gq_stats(ctypes.Structure):
         ("jit_passes", ctypes.c_int64),
         ("jit_compile_ms", ctypes.c_double),
         ("host_ms", ctypes.c_double),
+        ("tile_bytes", ctypes.c_int64),
     ]
 
 

@@ -23,6 +23,17 @@
 namespace {
 
 thread_local std::string g_err;
+// Support of the start state the next scheduling hooks assume
+// (SchedOptions::support0; gqx_set_support0), and the CTAs their programs
+// launch (gqx_last_ctas).
+thread_local uint64_t g_support0 = ~0ull;
+thread_local int64_t g_ctas = 0;
+
+int64_t count_ctas(const gq::Program& prog) {
+    int64_t c = 0;
+    for (const gq::PassDesc& pd : prog.passes) c += 1ll << pd.n_outer;
+    return c;
+}
 
 template <class T>
 void run_pass(std::vector<gq::cplx<T>>& st, const gq::Program& prog, const std::vector<gq::cplx<T>>& pool, size_t pi) {
@@ -134,6 +145,9 @@ extern "C" {
 
 const char* gqx_last_error(void) { return g_err.c_str(); }
 
+void gqx_set_support0(uint64_t support0) { g_support0 = support0; }
+int64_t gqx_last_ctas(void) { return g_ctas; }
+
 // Applies ops to a host state (2^nq interleaved doubles) through the
 // scheduler and the tile-pass code, emulated on the CPU. precision GQ_C64
 // runs the float instantiation. Returns GQ_OK or an error code.
@@ -165,8 +179,10 @@ static int emulate_sv_impl(int nq, int precision, double* state, const gq_op* op
     opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
     opt.low_qubits = precision == GQ_C64 ? 4 : 3;
     opt.fuse_dense = fuse != 0;
+    opt.support0 = g_support0;
     gq::Program prog;
     gq::schedule(gates, nphys, opt, prog);
+    g_ctas = count_ctas(prog);
     const uint64_t n = 1ull << nphys;
     if (precision == GQ_C64) {
         std::vector<gq::cplx<float>> st(n, {0.f, 0.f});
@@ -218,6 +234,47 @@ int gqx_schedule_stats(int nq, int precision, const gq_op* ops, size_t n_ops, in
     out[3] = cost;
     out[4] = pairsums;
     return GQ_OK;
+}
+
+// Per pass of the statevector schedule: out[5*i ..] = {phases, ops, FMA-per-
+// amplitude cost, tile qubit mask, CTA-index bits}; returns the pass count
+// (at most `max_passes` rows are written) or a negative error code.
+int64_t gqx_schedule_passes(int nq, int precision, const gq_op* ops, size_t n_ops, int tile_qubits, int budget,
+                            int64_t* out, int64_t max_passes) {
+    const int nphys = nq < gq::RQ ? gq::RQ : nq;
+    std::vector<gq::NGate> gates;
+    for (size_t i = 0; i < n_ops; ++i) {
+        int rc = gq::normalize_op(ops[i], nq, gates, g_err);
+        if (rc != GQ_OK) return -rc;
+    }
+    gq::SchedOptions opt;
+    if (tile_qubits > 0) opt.tile_qubits = tile_qubits;
+    if (budget > 0) opt.budget = budget;
+    opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
+    opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    opt.support0 = g_support0;
+    gq::Program prog;
+    gq::schedule(gates, nphys, opt, prog);
+    g_ctas = count_ctas(prog);
+    for (size_t p = 0; p < prog.passes.size() && (int64_t)p < max_passes; ++p) {
+        const gq::PassDesc& pd = prog.passes[p];
+        int64_t n = 0, cost = 0, tmask = 0;
+        for (int b = 0; b < pd.m; ++b) tmask |= 1ll << pd.tile_q[b];
+        for (int f = pd.phase0; f < pd.phase0 + pd.n_phases; ++f)
+            for (int k = prog.phases[f].op_begin; k < prog.phases[f].op_end; ++k) {
+                static const int c[] = {0, 8, 16, 32, 64, 1, 1, 3, 1, 4, 16, 6};
+                const gq::KOp& op = prog.ops[k];
+                cost += c[op.type];
+                ++n;
+            }
+        int64_t* o = out + 5 * p;
+        o[0] = pd.n_phases;
+        o[1] = n;
+        o[2] = cost;
+        o[3] = tmask;
+        o[4] = pd.n_outer;
+    }
+    return (int64_t)prog.passes.size();
 }
 
 // Density matrix: rho (dim*dim interleaved doubles, row-major) evolved by the
@@ -479,8 +536,10 @@ int gqx_jit_emulate(int nq, int precision, double* state, const gq_op* ops, size
     opt.budget = budget > 0 ? budget : 320;
     opt.swizzle_width = precision == GQ_C64 ? 4 : 3;
     opt.low_qubits = precision == GQ_C64 ? 4 : 3;
+    opt.support0 = g_support0;
     gq::Program prog;
     gq::schedule(gates, nphys, opt, prog);
+    g_ctas = count_ctas(prog);
     const uint64_t n = 1ull << nphys, nv = 1ull << nvec;
     int64_t jitted = 0;
     int rc;

@@ -213,6 +213,7 @@ struct Engine {
     int jit_min_blocks = 0;   // GQ_OPT_JIT_MIN_BLOCKS (0: the variant's)
     int jit_persistent = 0;   // GQ_OPT_JIT_PERSISTENT (measured slower: 3 CTAs/SM)
     int jit_minb = 4;         // CTAs per SM of the last specialised launch shape
+    bool skip_zero_tiles = true;  // GQ_OPT_ZERO_TILES
     int num_sms = 148;
     template <class T>
     size_t jit_smem(int m) const {
@@ -522,12 +523,18 @@ struct Engine {
 
     bool jit_on() const { return jit_mode != 0 && nphys >= jit_min_qubits && jit_available(); }
 
-    int run_gates(const std::vector<NGate>& gates) {
+    // support: when given, the qubits that may be 1 in a nonzero amplitude of
+    // the state before the gates (SchedOptions::support0); it receives the
+    // support after them. Only callers that have just reset the state pass it.
+    int run_gates(const std::vector<NGate>& gates, uint64_t* support = nullptr) {
         Program pr;
         SchedOptions o = opt;
         o.fuse_pairs = !jit_on();  // specialised kernels take diagonals as free pending factors
+        if (support && skip_zero_tiles) o.support0 = *support;
         schedule(gates, nphys, o, pr);
+        if (support) *support = skip_zero_tiles ? pr.support_out : ~0ull;
         stats.gates_in += pr.gates;
+        for (const PassDesc& pd : pr.passes) stats.tile_bytes += (int64_t)(2 * amp_bytes()) << (pd.m + pd.n_outer);
         return prec == GQ_C64 ? run_program_t<float>(pr) : run_program_t<double>(pr);
     }
 
@@ -811,7 +818,8 @@ int gq_sv_reset(gq_sv* sv) {
     return sv->e.reset_basis(0);
 }
 
-static int sv_apply_impl(gq_sv* sv, const gq_op* ops, size_t n_ops) {
+// support: see Engine::run_gates (null: the state is arbitrary).
+static int sv_apply_impl(gq_sv* sv, const gq_op* ops, size_t n_ops, uint64_t* support = nullptr) {
     if (n_ops && !ops) return fail(GQ_EINVAL, "null ops");
     std::vector<NGate> gates;
     std::string err;
@@ -821,7 +829,7 @@ static int sv_apply_impl(gq_sv* sv, const gq_op* ops, size_t n_ops) {
         if (rc != GQ_OK) return fail(rc, "op " + std::to_string(i) + ": " + err);
         if (!gates.empty() && gates.back().src < 0) gates.back().src = (int)i;
     }
-    return sv->e.run_gates(gates);
+    return sv->e.run_gates(gates, support);
 }
 
 namespace {
@@ -829,8 +837,9 @@ int sv_apply_timed(gq_sv* sv, const gq_op* ops, size_t n_ops, bool reset) {
     if (!sv) return fail(GQ_EINVAL, "null handle");
     sv->e.clear_stats();
     GQ_TRY(sv->e.time_begin());
+    uint64_t support = 0;  // |0...0>: no qubit is 1 in a nonzero amplitude
     if (reset) GQ_TRY(sv->e.reset_basis(0));
-    GQ_TRY(sv_apply_impl(sv, ops, n_ops));
+    GQ_TRY(sv_apply_impl(sv, ops, n_ops, reset ? &support : nullptr));
     return sv->e.time_end();
 }
 }  // namespace
@@ -1031,6 +1040,9 @@ int gq_sv_set_option(gq_sv* sv, int key, int64_t value) {
         case GQ_OPT_FUSE_DENSE:
             e.opt.fuse_dense = value != 0;
             return GQ_OK;
+        case GQ_OPT_ZERO_TILES:
+            e.skip_zero_tiles = value != 0;
+            return GQ_OK;
         case GQ_OPT_JIT:
         case GQ_OPT_JIT_MIN_QUBITS:
         case GQ_OPT_JIT_MIN_BLOCKS:
@@ -1074,11 +1086,12 @@ int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_p
         return j;
     };
     GQ_TRY(e.reset_basis(0));
+    uint64_t support = 0;
     for (int j = 0; j < segs; ++j) {
         std::vector<NGate> part;
         for (size_t k = 0; k < fwd.size(); ++k)
             if (seg_of(fo[k]) == j) part.push_back(fwd[k]);
-        GQ_TRY(e.run_gates(part));
+        GQ_TRY(e.run_gates(part, &support));
         if (j + 1 < segs)
             GQ_CUDA(cudaMemcpyAsync((char*)e.ckpt.p + sbytes * j, e.state.p, sbytes, cudaMemcpyDeviceToDevice, e.stream));
     }
@@ -1157,7 +1170,8 @@ int gq_dm_reset(gq_dm* dm) {
     return dm->e.reset_basis(0);
 }
 
-static int dm_apply_impl(gq_dm* dm, const gq_op* ops, size_t n_ops) {
+// support: see Engine::run_gates (null: the state is arbitrary).
+static int dm_apply_impl(gq_dm* dm, const gq_op* ops, size_t n_ops, uint64_t* support = nullptr) {
     if (n_ops && !ops) return fail(GQ_EINVAL, "null ops");
     std::vector<NGate> gates;
     {
@@ -1165,15 +1179,16 @@ static int dm_apply_impl(gq_dm* dm, const gq_op* ops, size_t n_ops) {
         int rc = dm_gates(dm->nq, ops, n_ops, gates, err, !dm->dense_channels);
         if (rc != GQ_OK) return fail(rc, err);
     }
-    return dm->e.run_gates(gates);
+    return dm->e.run_gates(gates, support);
 }
 
 static int dm_apply_timed(gq_dm* dm, const gq_op* ops, size_t n_ops, bool reset) {
     if (!dm) return fail(GQ_EINVAL, "null handle");
     dm->e.clear_stats();
     GQ_TRY(dm->e.time_begin());
+    uint64_t support = 0;  // |0...0><0...0| is entry 0 of the vectorised matrix
     if (reset) GQ_TRY(dm->e.reset_basis(0));
-    GQ_TRY(dm_apply_impl(dm, ops, n_ops));
+    GQ_TRY(dm_apply_impl(dm, ops, n_ops, reset ? &support : nullptr));
     return dm->e.time_end();
 }
 
@@ -1208,6 +1223,10 @@ int gq_dm_set_option(gq_dm* dm, int key, int64_t value) {
         return dm->e.set_jit_option(key, value);
     if (key == GQ_OPT_DM_DENSE_CHANNELS) {
         dm->dense_channels = value != 0;
+        return GQ_OK;
+    }
+    if (key == GQ_OPT_ZERO_TILES) {
+        dm->e.skip_zero_tiles = value != 0;
         return GQ_OK;
     }
     return fail(GQ_EINVAL, "unknown option");

@@ -614,6 +614,8 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
     for (size_t i = 0; i < gates.size(); ++i) remaining[i] = (int)i;
 
     std::mt19937_64 rng(12345);
+    // Support of the state before the current pass (SchedOptions::support0).
+    uint64_t support = opt.support0 | ~all;
     while (!remaining.empty()) {
         // ---- pass: the tile holds the targets of every absorbed gate.
         std::vector<std::vector<int>> pgroups;
@@ -672,7 +674,7 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
             if (T & (1ull << q)) {
                 tb_of[q] = nt;
                 tile_q[nt++] = q;
-            } else {
+            } else if (support & (1ull << q)) {
                 pd.outer_q[pd.n_outer++] = q;
             }
         }
@@ -858,7 +860,9 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
         (void)tb_of;
         prog.passes.push_back(pd);
         prog.pass_params.push_back(slot_params);
+        for (int gi : absorbed) support |= gates[gi].barrier ? ~0ull : gates[gi].nd_mask;
     }
+    prog.support_out = (support & all) == all ? ~0ull : (support & all);
 }
 
 // ---- density matrix ----------------------------------------------------

@@ -50,6 +50,14 @@ struct SchedOptions {
     bool fuse_dense = false;  // fold runs of register-local gates of a phase into one dense block
                               // (measured slower on the layered benchmark: dense blocks reload
                               // their matrix per amplitude group)
+    // Qubits that may be 1 in a nonzero amplitude of the state the program
+    // starts from (every amplitude whose index has a bit outside the mask is
+    // exactly zero); all ones when nothing is known. A pass maps an all-zero
+    // tile to an all-zero tile, so a pass launches only the CTAs whose outer
+    // bits lie inside the support reached so far: the others keep their
+    // zeros in place. After a reset to |0...0> the support is empty, and each
+    // pass adds the qubits its non-diagonal ops act on.
+    uint64_t support0 = ~0ull;
 };
 
 struct Program {
@@ -60,6 +68,7 @@ struct Program {
     int64_t gates = 0;
     int64_t conflict_phases = 0;  // phases whose lane groups could not be made conflict free
     std::vector<std::vector<int>> pass_params;  // K_GRAD: parameter of each slot, per pass
+    uint64_t support_out = ~0ull;  // the support after the last pass (SchedOptions::support0)
 };
 
 // Appends the NGates of one op (0 when it is an identity or a barrier).

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define GQ_ABI_VERSION 4
+#define GQ_ABI_VERSION 5
 
 /* ---- status codes ------------------------------------------------------ */
 #define GQ_OK 0
@@ -119,6 +119,10 @@ typedef struct gq_stats {
     double jit_compile_ms;   /* process total: milliseconds spent compiling them    */
     double host_ms;          /* batches: host time of the last call before its first
                                 launch (analysis, scheduling, table packing, upload) */
+    int64_t tile_bytes;      /* bytes the last call's tile passes read and wrote: 2 x
+                                amplitude size x amplitudes of the CTAs launched
+                                (passes x 2 x state_bytes unless GQ_OPT_ZERO_TILES
+                                skipped tiles)                                      */
 } gq_stats;
 
 /* ---- library ------------------------------------------------------------- */
@@ -296,6 +300,13 @@ int gq_sv_stats(const gq_sv* sv, gq_stats* out);
  * diagonal and the population map (default 0); 1 folds every channel into a
  * dense superoperator with the gate before it. */
 #define GQ_OPT_DM_DENSE_CHANNELS 13
+/* Evolve and Run from the reset state (and the adjoint's forward sweep):
+ * every amplitude whose index has a 1 on a qubit that no earlier pass acted
+ * on with a non-diagonal op is exactly zero, and a pass maps an all-zero tile
+ * to an all-zero tile, so each pass launches only the CTAs whose outer
+ * qubits lie in that support; the skipped tiles keep the zeros of the reset
+ * (default 1; results are identical either way; Apply never skips). */
+#define GQ_OPT_ZERO_TILES 14
 int gq_sv_set_option(gq_sv* sv, int key, int64_t value);
 
 /* ---- density matrix: replaces densitymatrix.New/Sim ---------------------- */

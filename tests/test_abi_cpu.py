@@ -31,11 +31,11 @@ def test_struct_layouts_match_header():
     # gq_op: 4 int32 + 16 int32 qubits + pointer + 3 int32 + pad int32 + 3 pointers
     assert ctypes.sizeof(_abi.gq_op) == 4 * 4 + 16 * 4 + 8 + 4 * 4 + 3 * 8
     assert ctypes.sizeof(_abi.gq_pauli_term) == 32
-    assert ctypes.sizeof(_abi.gq_stats) == 96
+    assert ctypes.sizeof(_abi.gq_stats) == 104
 
 
 def test_abi_version():
-    assert _abi.lib().gq_abi_version() == 4
+    assert _abi.lib().gq_abi_version() == 5
 
 
 @pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES") is None and os.path.exists("/dev/nvidia0"),

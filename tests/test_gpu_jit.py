@@ -154,3 +154,54 @@ def test_specialised_reverse_passes_general_gates():
         assert ev_j.sim.stats()["jit_passes"] == ev_j.sim.stats()["passes"]
         assert abs(e_j - e_i) < tol
         np.testing.assert_allclose(g_j, g_i, atol=tol, rtol=0)
+
+
+@pytest.mark.parametrize("n,seed,variant", [(16, 51, 0), (22, 52, 2)])
+def test_zero_tile_skip_is_bit_identical(n, seed, variant):
+    # Evolve from the reset state launches only the tiles inside the support
+    # (GQ_OPT_ZERO_TILES, default on): the state must be bit-identical to the
+    # run that launches every tile, and the tile bytes smaller
+    c = workloads.random_layers_qft(n, 3, seed) if n > 16 else random_circuit(n, 120, seed, allow_reset=True)
+    states, tb = [], []
+    for skip in (0, 1):
+        sim = jit_sim(n)
+        sim.set_option(_abi.GQ_OPT_KERNEL_VARIANT, variant)
+        sim.set_option(_abi.GQ_OPT_ZERO_TILES, skip)
+        sim.Evolve(c)
+        st = sim.stats()
+        assert st["jit_passes"] == st["passes"] >= 1
+        states.append(sim.StateVector())
+        tb.append(st["tile_bytes"])
+        sim.Close()
+    assert np.array_equal(states[0], states[1])
+    assert tb[0] == st["passes"] * 2 * st["state_bytes"] and tb[1] < tb[0]
+    if n <= 16:
+        np.testing.assert_allclose(states[1], orc.sv_evolve(encode.statevector_ops(c)), atol=1e-12, rtol=0)
+
+
+def test_zero_tile_skip_density_matrix_and_apply():
+    c, nm = workloads.noisy_brickwork(10, layers=3, seed=53)
+    rhos = []
+    for skip in (0, 1):
+        dm = densitymatrix.New(10).WithNoise(nm)
+        dm.set_option(_abi.GQ_OPT_JIT, 2)
+        dm.set_option(_abi.GQ_OPT_JIT_MIN_QUBITS, 0)
+        dm.set_option(_abi.GQ_OPT_ZERO_TILES, skip)
+        dm.Evolve(c)
+        st = dm.stats()
+        assert (st["tile_bytes"] < st["passes"] * 2 * st["state_bytes"]) == bool(skip)
+        rhos.append(dm.DensityMatrix())
+        dm.Close()
+    assert np.array_equal(rhos[0], rhos[1])
+    # Apply composes on the current state: nothing may be skipped there
+    g = random_circuit(16, 60, 54)
+    sim = jit_sim(16)
+    sim.Evolve(g)
+    sim.Apply(g)
+    st = sim.stats()
+    assert st["tile_bytes"] == st["passes"] * 2 * st["state_bytes"]
+    sim2 = jit_sim(16)
+    sim2.set_option(_abi.GQ_OPT_ZERO_TILES, 0)
+    sim2.Evolve(g)
+    sim2.Apply(g)
+    assert np.array_equal(sim.StateVector(), sim2.StateVector())

@@ -289,3 +289,41 @@ def test_on_disk_kernel_cache(emu, tmp_path, monkeypatch):
     assert f(src, ctypes.byref(hit)) == n1 and hit.value == 1
     monkeypatch.setenv("GQ_JIT_CACHE_DIR", "off")
     assert f(src, ctypes.byref(hit)) == n1 and hit.value == 0
+
+
+@pytest.mark.parametrize("n,seed,tile", [(10, 41, 6), (12, 42, 7)])
+def test_generated_code_skipping_zero_tiles(emu, tmp_path, n, seed, tile):
+    # from the reset state, passes launch only the tiles inside the support
+    # (fewer CTA-index bits, controls on zero qubits outside every table)
+    emu.gqx_set_support0.argtypes = [ctypes.c_uint64]
+    emu.gqx_last_ctas.restype = ctypes.c_int64
+    c = random_circuit(n, 100, seed, allow_reset=True)
+    ops = encode.statevector_ops(c)
+    emu.gqx_set_support0(0)
+    try:
+        got = jit_emulate(emu, ops, n, tmp_path, tile=tile)
+        ctas = emu.gqx_last_ctas()
+    finally:
+        emu.gqx_set_support0(2 ** 64 - 1)
+    np.testing.assert_allclose(got, orc.sv_evolve(ops), atol=1e-12, rtol=0)
+    full = jit_emulate(emu, ops, n, tmp_path, tile=tile)
+    assert np.array_equal(got, full)
+    assert ctas < emu.gqx_last_ctas()
+
+
+def test_generated_code_density_matrix_skipping_zero_tiles(emu, tmp_path):
+    # the vectorised |0><0| has entry 0 only: the same support rule holds
+    c, nm = workloads.noisy_brickwork(5, layers=3, seed=3)
+    ops = encode.density_ops(c, nm)
+    emu.gqx_set_support0.argtypes = [ctypes.c_uint64]
+    emu.gqx_last_ctas.restype = ctypes.c_int64
+    emu.gqx_set_support0(0)
+    try:
+        got = jit_emulate(emu, ops, 5, tmp_path, dm=1, tile=5)
+        ctas = emu.gqx_last_ctas()
+    finally:
+        emu.gqx_set_support0(2 ** 64 - 1)
+    np.testing.assert_allclose(got, orc.dm_evolve(ops), atol=1e-12, rtol=0)
+    full = jit_emulate(emu, ops, 5, tmp_path, dm=1, tile=5)
+    assert np.array_equal(got, full)
+    assert ctas < emu.gqx_last_ctas()

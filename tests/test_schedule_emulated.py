@@ -283,3 +283,70 @@ def test_adjoint_checkpoints_fit_free_memory(emu):
     # an explicit request is kept (capped at the op count only)
     assert f(5, 1, 2000, s33, 0) == 5
     assert f(5, 0, 3, s33, 0) == 3
+
+
+# ---- passes from the reset state skip the tiles that are still zero ---------
+# (SchedOptions::support0, GQ_OPT_ZERO_TILES): a pass launches only the CTAs
+# whose outer qubits lie in the support reached so far.
+
+def _with_support(emu, support0, fn):
+    emu.gqx_set_support0.argtypes = [ctypes.c_uint64]
+    emu.gqx_last_ctas.restype = ctypes.c_int64
+    emu.gqx_set_support0(support0)
+    try:
+        return fn(), emu.gqx_last_ctas()
+    finally:
+        emu.gqx_set_support0(ctypes.c_uint64(~0 & (2 ** 64 - 1)))
+
+
+@pytest.mark.parametrize("n,seed,tile,budget", [(8, 31, 5, 8), (10, 32, 6, 0), (12, 33, 7, 16), (13, 34, 6, 4),
+                                                (11, 35, 9, 0)])
+def test_zero_tile_skip_matches_oracle(emu, n, seed, tile, budget):
+    # controls and diagonals on qubits outside the support, resets, 3-qubit gates
+    c = random_circuit(n, 90, seed, allow_reset=True)
+    ops = encode.statevector_ops(c)
+    want = orc.sv_evolve(ops)
+    full, ctas_full = _with_support(emu, 2 ** 64 - 1, lambda: run_emu(emu, ops, tile=tile, budget=budget)[0])
+    got, ctas = _with_support(emu, 0, lambda: run_emu(emu, ops, tile=tile, budget=budget)[0])
+    assert np.array_equal(got, full)  # the launched tiles compute exactly what they did before
+    np.testing.assert_allclose(got, want, atol=1e-12, rtol=0)
+    assert ctas < ctas_full
+
+
+def test_zero_tile_skip_late_support():
+    # a circuit that touches qubit 0 only: every pass runs one tile
+    from goqu_b200 import gate as G
+    c = ir.Circuit("narrow", 12, 0, [ir.Operation(G.H, [0]), ir.Operation(G.RZ(0.3), [11]),
+                                     ir.Operation(G.CNOT, [11, 0]), ir.Operation(G.RX(0.2), [0])])
+    ops = encode.statevector_ops(c)
+    h = ctypes.CDLL(EMU)
+    h.gqx_emulate_sv.restype = ctypes.c_int
+    h.gqx_emulate_sv.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(_abi.gq_op), ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    h.gqx_last_error.restype = ctypes.c_char_p
+    got, ctas = _with_support(h, 0, lambda: run_emu(h, ops, tile=4)[0])
+    np.testing.assert_allclose(got, orc.sv_evolve(ops), atol=1e-14, rtol=0)
+    assert ctas == 1  # qubit 11 stays 0, so its control and diagonal act on zeros only
+
+
+def test_zero_tile_skip_headline_openers(emu):
+    # 28 qubits, 40 U3+CNOT brickwork layers + QFT28, 12-qubit tiles: the
+    # first pass runs one CTA and the second 2^9 of 2^16; the rest are full
+    f = emu.gqx_schedule_passes
+    f.restype = ctypes.c_int64
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_abi.gq_op), ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                  ctypes.POINTER(ctypes.c_int64), ctypes.c_int64]
+    c = workloads.random_layers_qft(28, 40, 2028)
+    ops = encode.statevector_ops(c)
+    out_full = (ctypes.c_int64 * (5 * 400))()
+    out = (ctypes.c_int64 * (5 * 400))()
+    (np_full, _) = _with_support(emu, 2 ** 64 - 1, lambda: f(28, 0, ops.ptr(), len(ops), 12, 0, out_full, 400))
+    (np_zero, _) = _with_support(emu, 0, lambda: f(28, 0, ops.ptr(), len(ops), 12, 0, out, 400))
+    assert np_full == np_zero
+    bits = [out[5 * i + 4] for i in range(np_zero)]
+    assert [out_full[5 * i + 4] for i in range(np_full)] == [16] * np_full
+    assert bits[0] == 0 and bits[1] == 9 and all(b == 16 for b in bits[2:])
+    # the schedule is otherwise the same pass for pass
+    for i in range(np_zero):
+        assert [out[5 * i + k] for k in range(4)] == [out_full[5 * i + k] for k in range(4)]
