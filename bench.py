@@ -539,9 +539,11 @@ def extra_qaoa_dedicated(calls=3):
     general batch path and the FP64 oracle."""
     from goqu_b200 import _abi, batch, qaoa
     evals = workloads_qaoa_4096()
+    t0 = time.perf_counter()
     items = [qaoa.from_evaluation(e) for e in evals]
     b = qaoa.MaxCutBatch()
     enc = b.encode(items)  # host packing of the records, once (as for the general batch)
+    host_encode_s = time.perf_counter() - t0
     b.run_encoded(enc)  # buffers sized, kernels loaded
     ms = []
     for _ in range(calls):
@@ -576,6 +578,7 @@ def extra_qaoa_dedicated(calls=3):
             "ms_call": best, "circuits_per_s": len(items) / (best / 1000.0),
             "timing": "wall time of the whole gq_qaoa_maxcut_batch call (host tables, upload, launches, results); "
                       "records packed once beforehand",
+            "host_encode_s": host_encode_s,
             "max_abs_energy_diff_vs_general_batch": float(np.max(np.abs(np.asarray(e_fast) - np.asarray(e_gen)))),
             "max_abs_grad_diff_vs_general_batch": float(max(np.max(np.abs(a - c)) for a, c in zip(g_fast, g_gen))),
             "max_abs_energy_error_vs_fp64_oracle": e_err, "max_abs_grad_error_vs_fp64_central_difference": g_err,
@@ -712,6 +715,7 @@ def run_gpu(args, world, rank, local):
             traffic_full = t["bytes_per_launch"] * 2.0 ** (n - t["qubits"])  # a full-state launch; scales with 2^n
             traffic = traffic_full * alg_bytes / full_bytes
 
+    clocks = clk.summary()
     line = {
         "metric": f"{n}q gates/s", "value": value, "unit": "gates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -721,6 +725,9 @@ def run_gpu(args, world, rank, local):
                    "precision": args.precision, "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": f"state {amp_bytes << n >> 20} MiB vs 126 MB L2 (no flush between steps)",
                    "passes_per_step": passes / args.steps, "pass_ms_per_step": float(np.mean(pass_ms)),
+                   # pass time in SM clock cycles: comparable across runs at other clocks
+                   "pass_sm_mcycles_per_step": (float(np.mean(pass_ms)) * clocks["sm_mhz"] / 1000.0
+                                                if clocks.get("sm_mhz") else None),
                    "zero_tile_skip": {"tile_bytes_per_step": tile_bytes / args.steps,
                                       "full_state_bytes_per_step": full_bytes * passes / args.steps}},
         "e2e": {"value": e2e, "unit": "gates/s", "h2d_bytes_per_step": h2d // args.steps,
@@ -732,7 +739,7 @@ def run_gpu(args, world, rank, local):
         "gpu_launches": launches,
         "jit": {"mode": args.jit, "passes_specialised_per_step": jit_passes / args.steps,
                 "first_call_s": t_first, "compile_ms_total": sim.stats()["jit_compile_ms"]},
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "autotune": tuned,
     }
     sim.Close()
