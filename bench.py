@@ -661,7 +661,8 @@ def run_gpu(args, world, rank, local):
         tuned = {"best": {str(k): v for k, v in tuned["best"].items()},
                  "candidates": [{str(k): v for k, v in c.items()} for c in autotune.STATEVECTOR_CANDIDATES],
                  "timings_ms": tuned.get("timings_ms"), "tuning_s": time.perf_counter() - t0,
-                 "keys": "option numbers of include/gqb200.h (2 pass budget, 5 kernel variant, 11 jit min blocks)"}
+                 "keys": "option numbers of include/gqb200.h (2 pass budget, 5 kernel variant, 11 jit min blocks, "
+                         "12 persistent CTAs)"}
         sim.set_option(_abi.GQ_OPT_TIMING, 1)
         sim.set_option(_abi.GQ_OPT_JIT, args.jit)
         for _ in range(2):

@@ -33,6 +33,9 @@ STATEVECTOR_CANDIDATES = [
     {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_PASS_BUDGET: 400},
     {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_PASS_BUDGET: 480},
     {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_JIT_MIN_BLOCKS: 3},
+    # persistent CTAs that prefetch their next tile during the last phase
+    {_abi.GQ_OPT_JIT_PERSISTENT: 1},
+    {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_JIT_PERSISTENT: 1},
 ]
 BATCH_CANDIDATES = [
     {},

@@ -28,6 +28,8 @@ thread_local std::string g_err;
 // launch (gqx_last_ctas).
 thread_local uint64_t g_support0 = ~0ull;
 thread_local int64_t g_ctas = 0;
+// Persistent kernel texts in gqx_jit_check (gqx_set_persistent).
+thread_local bool g_persistent = false;
 
 int64_t count_ctas(const gq::Program& prog) {
     int64_t c = 0;
@@ -146,6 +148,7 @@ extern "C" {
 const char* gqx_last_error(void) { return g_err.c_str(); }
 
 void gqx_set_support0(uint64_t support0) { g_support0 = support0; }
+void gqx_set_persistent(int on) { g_persistent = on != 0; }
 int64_t gqx_last_ctas(void) { return g_ctas; }
 
 // Applies ops to a host state (2^nq interleaved doubles) through the
@@ -492,7 +495,8 @@ int gqx_jit_check(int nq, int precision, const gq_op* ops, size_t n_ops, int til
     for (size_t i = 0; i < prog.passes.size(); ++i) {
         gq::JitPlan pl;
         const int threads = 1 << (prog.passes[i].m - gq::RQ);
-        if (!gq::jit_plan(prog, i, precision == GQ_C64, threads, 4, false, pl)) continue;  // the engine's default shape
+        // the engine's default shape (persistent: the 12-qubit-tile shape's 2 CTAs per SM)
+        if (!gq::jit_plan(prog, i, precision == GQ_C64, threads, g_persistent ? 2 : 4, g_persistent, pl)) continue;
         ++planned;
         if (!texts.insert(pl.source).second || compiled >= max_compile) continue;
         std::string log;

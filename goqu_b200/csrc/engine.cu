@@ -211,13 +211,13 @@ struct Engine {
     int jit_mode = 1;         // GQ_OPT_JIT
     int jit_min_qubits = 20;  // GQ_OPT_JIT_MIN_QUBITS
     int jit_min_blocks = 0;   // GQ_OPT_JIT_MIN_BLOCKS (0: the variant's)
-    int jit_persistent = 0;   // GQ_OPT_JIT_PERSISTENT (measured slower: 3 CTAs/SM)
+    int jit_persistent = 0;   // GQ_OPT_JIT_PERSISTENT (an autotuner candidate)
     int jit_minb = 4;         // CTAs per SM of the last specialised launch shape
     bool skip_zero_tiles = true;  // GQ_OPT_ZERO_TILES
     int num_sms = 148;
     template <class T>
     size_t jit_smem(int m) const {
-        return (sizeof(cplx<T>) << m) * (jit_persistent ? 2 : 1);
+        return sizeof(cplx<T>) << m;  // one tile buffer (persistent CTAs refill it in place)
     }
     size_t amp_bytes() const { return prec == GQ_C64 ? 8 : 16; }
     int max_tile() const {
@@ -325,11 +325,11 @@ struct Engine {
         std::vector<const CachedPlan*> plans(np, nullptr);
         if (jit_on()) {
             // One tile per CTA: 4 CTAs of 128 threads per SM (128 registers)
-            // measured fastest for both precisions. Persistent: as many CTAs
-            // per SM as two tile buffers each allow (3 for complex128).
+            // measured fastest for both precisions. Persistent: the launch
+            // shape's CTAs per SM, as far as one tile buffer each allows.
             const TileVariant tv = prec == GQ_C64 ? kVariantsC64[variant] : kVariantsC128[variant];
             int minb = tv.threads == 128 ? std::max(tv.min_blocks, 4) : tv.min_blocks;
-            if (jit_persistent) minb = std::max(1, std::min(minb, (int)((227u << 10) / (2 * (sizeof(cplx<T>) << max_tile())))));
+            if (jit_persistent) minb = std::max(1, std::min(minb, (int)((227u << 10) / (sizeof(cplx<T>) << max_tile()))));
             if (jit_min_blocks > 0) minb = jit_min_blocks;
             jit_minb = minb;
             for (size_t i = 0; i < np; ++i) {

@@ -432,7 +432,6 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
     // barriers fewer) when the phase's lanes run along the lowest qubits
     // (128-byte runs, as the staging copies) and each register bit is one
     // tile qubit. direct_in / direct_out record whether they do.
-    const bool direct_ok = !persistent;
     bool direct_in = false, direct_out = false;
     const int lane_run = c64 ? 4 : 3;  // lowest qubits a 128-byte run spans
     for (int p = 0; p < pd.n_phases; ++p) {
@@ -515,7 +514,7 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
         // global offset of each register slot: register bit k is the tile
         // qubit whose staging column is rslot[1 << k]
         uint64_t greg[NREG];
-        bool direct = direct_ok && tbits >= lane_run;
+        bool direct = tbits >= lane_run;
         for (int k = 0; k < lane_run && direct; ++k) direct = tq[k] == k;
         for (int k = 0; k < RQ && direct; ++k) {
             int hit = -1;
@@ -528,7 +527,8 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
             greg[0] = 0;
             for (int j = 1; j < NREG; ++j) greg[j] = greg[j & (j - 1)] | greg[j & -j];
         }
-        const bool load_global = direct && p == 0;
+        // (persistent CTAs find their tile in shared memory, prefetched)
+        const bool load_global = direct && p == 0 && !persistent;
         const bool store_global = direct && p == pd.n_phases - 1;
         if (p == 0) direct_in = load_global;
         if (p == pd.n_phases - 1) direct_out = store_global;
@@ -536,6 +536,18 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
         for (int j = 0; j < NREG; ++j)
             b += load_global ? "        a[" + num(j) + "] = st[g0 | " + hex64(greg[j]) + "];\n"
                              : "        a[" + num(j) + "] = sm[sb ^ " + hex32(ph.rslot[j]) + "];\n";
+        // the last phase's registers are loaded: a persistent CTA may refill
+        // the tile buffer with its next tile from here on
+        if (store_global && persistent) {
+            // every thread's registers of this tile are loaded: each thread
+            // refills its own sixteen slots with the next tile's amplitudes
+            b += "        __syncthreads();\n        if (nxt < ntiles) {\n            uint64_t nb = 0;\n";
+            emit_deposit(b, "            ", "nb", "nxt", pd.outer_q, pd.n_outer);
+            b += "            const uint64_t gq = nb | (g0 ^ base);\n";
+            for (int j = 0; j < NREG; ++j)
+                b += "            cp_async_amp(sm + (sb ^ " + hex32(ph.rslot[j]) + "), st + (gq | " + hex64(greg[j]) + "));\n";
+            b += "        }\n        cp_async_commit();\n";
+        }
 
         PendT pend[NREG];
         for (int j = 0; j < NREG; ++j) pend[j].assign(NC, Pend());
@@ -827,28 +839,34 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
         if (!direct_out) s += seg_out;
         s += "}\n";
     } else {
-        // persistent CTAs, two tile buffers: the next tile's amplitudes are
-        // copied asynchronously while the current one runs its phases
-        auto issue = [&](const char* buf) {
-            std::string r;
+        // Persistent CTAs (grid = SMs x CTAs per SM), one tile buffer each: the
+        // next tile's amplitudes are copied in asynchronously (cp.async) once
+        // the current tile's last phase has loaded its registers (each thread
+        // into the slots it read), so the copy overlaps that phase's
+        // arithmetic and its direct stores; the CTA waits for the copy before
+        // the next tile's first phase. Without direct stores the last phase
+        // writes the buffer back first and the copy starts after the staged
+        // write-out.
+        auto issue = [&]() {
+            std::string r = "    if (nxt < ntiles) {\n" + make_pro("nxt");
             for (int it = 0; it < NREG; ++it)
-                r += "    cp_async_amp(" + std::string(buf) + " + (stt ^ " + hex32(S[it]) + "), st + (gt | " +
-                     hex64(G[it]) + "));\n";
+                r += "    cp_async_amp(sm + (stt ^ " + hex32(S[it]) + "), st + (gt | " + hex64(G[it]) + "));\n";
+            r += "    }\n    cp_async_commit();\n";
             return r;
         };
-        s += "    cplx<T>* const buf0 = reinterpret_cast<cplx<T>*>(smraw);\n";
-        s += "    cplx<T>* const buf1 = buf0 + " + num(1ll << m) + ";\n";
+        s += "    cplx<T>* const sm = reinterpret_cast<cplx<T>*>(smraw);\n";
         s += "    const uint64_t ntiles = 1ull << " + num(pd.n_outer) + ";\n";
         s += "    uint64_t cta = blockIdx.x;\n    if (cta >= ntiles) return;\n";
-        s += "    {\n" + pro + issue("buf0") + "    }\n    cp_async_commit();\n";
-        s += "    for (uint32_t k = 0;; ++k) {\n";
-        s += "    cplx<T>* const sm = (k & 1u) ? buf1 : buf0;\n";
+        s += "    {\n" + pro + seg_in + "    }\n    __syncthreads();\n";
+        s += "    for (;;) {\n";
         s += "    const uint64_t nxt = cta + gridDim.x;\n";
-        s += "    if (nxt < ntiles) {\n" + make_pro("nxt") + issue("((k & 1u) ? buf0 : buf1)") + "    }\n";
-        s += "    cp_async_commit();\n    cp_async_wait_prev();\n    __syncthreads();\n";
         s += "    {\n" + pro;
-        for (const std::string& ph : seg_ph) s += ph + "    __syncthreads();\n";
-        s += seg_out + "    }\n    __syncthreads();\n";
+        for (size_t k = 0; k < seg_ph.size(); ++k) {
+            s += seg_ph[k];  // the last one, with direct stores, issues the copy itself
+            if (k + 1 < seg_ph.size()) s += "    __syncthreads();\n";
+        }
+        if (!direct_out) s += "    __syncthreads();\n" + seg_out + "    __syncthreads();\n    {\n" + issue() + "    }\n";
+        s += "    }\n    cp_async_wait_all();\n    __syncthreads();\n";
         s += "    cta = nxt;\n    if (cta >= ntiles) break;\n    }\n}\n";
     }
 

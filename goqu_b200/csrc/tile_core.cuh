@@ -148,9 +148,9 @@ GQ_HD cplx<float> ldc_v(const cplx<float>* p, uint32_t i) {
 #endif
 }
 
-// Asynchronous global -> shared copy of one amplitude (cp.async; the
-// specialised kernels prefetch their next tile while computing the current
-// one). Host code copies directly.
+// Asynchronous global -> shared copy of one amplitude (cp.async; persistent
+// specialised kernels prefetch their next tile while the current one
+// finishes). Host code copies directly.
 #if defined(__CUDA_ARCH__)
 __device__ __forceinline__ void cp_async_amp(cplx<double>* dst, const cplx<double>* src) {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
@@ -161,8 +161,8 @@ __device__ __forceinline__ void cp_async_amp(cplx<float>* dst, const cplx<float>
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// Waits until at most one committed group (the most recent) is in flight.
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+// Waits until every committed copy of this thread has landed.
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 #endif
 
 // Matrix held in kernel parameter space (the specialised pass kernels pass

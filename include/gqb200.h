@@ -294,7 +294,10 @@ int gq_sv_stats(const gq_sv* sv, gq_stats* out);
 #define GQ_OPT_JIT 9
 #define GQ_OPT_JIT_MIN_QUBITS 10 /* smallest state (physical qubits) that uses them (default 20) */
 #define GQ_OPT_JIT_MIN_BLOCKS 11 /* their CTAs per SM (register bound); 0 = the launch shape's */
-#define GQ_OPT_JIT_PERSISTENT 12 /* 1: persistent CTAs prefetching the next tile; 0: one CTA per tile (default) */
+/* 1: persistent CTAs (SMs x CTAs per SM), one tile buffer each, refilled with
+ * the next tile (cp.async) while the current tile's last phase computes and
+ * stores; 0: one CTA per tile (default). */
+#define GQ_OPT_JIT_PERSISTENT 12
 /* Density matrices: channels that only mix populations and scale coherences
  * (depolarizing, amplitude and phase damping) run as permutations, a
  * diagonal and the population map (default 0); 1 folds every channel into a

@@ -205,3 +205,38 @@ def test_zero_tile_skip_density_matrix_and_apply():
     sim2.Evolve(g)
     sim2.Apply(g)
     assert np.array_equal(sim.StateVector(), sim2.StateVector())
+
+
+@pytest.mark.parametrize("variant", [0, 2])
+def test_persistent_kernels_match_one_tile_per_cta(variant):
+    # GQ_OPT_JIT_PERSISTENT: persistent CTAs refill their tile buffer with the
+    # next tile during the last phase; the state must be bit-identical to one
+    # CTA per tile, and match the oracle
+    n = 20
+    c = workloads.random_layers_qft(n, 4, 61)
+    want = orc.sv_evolve(encode.statevector_ops(c))
+    states = []
+    for persistent in (0, 1):
+        sim = jit_sim(n)
+        sim.set_option(_abi.GQ_OPT_KERNEL_VARIANT, variant)
+        sim.set_option(_abi.GQ_OPT_JIT_PERSISTENT, persistent)
+        sim.Evolve(c)
+        st = sim.stats()
+        assert st["jit_passes"] == st["passes"] >= 1
+        states.append(sim.StateVector())
+        sim.Close()
+    assert np.array_equal(states[0], states[1])
+    np.testing.assert_allclose(states[1], want, atol=1e-12, rtol=0)
+
+
+def test_persistent_kernels_complex64_and_random_gates():
+    c = random_circuit(18, 150, 62, allow_reset=True)
+    want = orc.sv_evolve(encode.statevector_ops(c))
+    for prec, tol in ((_abi.GQ_C128, 1e-12), (_abi.GQ_C64, 5e-5)):
+        sim = jit_sim(18, prec)
+        sim.set_option(_abi.GQ_OPT_JIT_PERSISTENT, 1)
+        sim.Evolve(c)
+        st = sim.stats()
+        assert st["jit_passes"] == st["passes"] >= 1
+        assert np.max(np.abs(sim.StateVector() - want)) < tol
+        sim.Close()

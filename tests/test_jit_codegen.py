@@ -327,3 +327,25 @@ def test_generated_code_density_matrix_skipping_zero_tiles(emu, tmp_path):
     full = jit_emulate(emu, ops, 5, tmp_path, dm=1, tile=5)
     assert np.array_equal(got, full)
     assert ctas < emu.gqx_last_ctas()
+
+
+@pytest.mark.parametrize("precision", [_abi.GQ_C128, _abi.GQ_C64])
+def test_persistent_kernels_compile(emu, precision):
+    # persistent CTAs with one tile buffer refilled during the last phase
+    # (GQ_OPT_JIT_PERSISTENT): the texts compile with NVRTC (at 2 CTAs of 256
+    # threads per SM the loop holds up to 128 registers; the heaviest passes
+    # spill a few words, which the autotuner's timing accounts for)
+    emu.gqx_set_persistent.argtypes = [ctypes.c_int]
+    c = workloads.random_layers_qft(24, 6, 7)
+    s = encode.statevector_ops(c)
+    out = (ctypes.c_int64 * 5)()
+    emu.gqx_set_persistent(1)
+    try:
+        rc = emu.gqx_jit_check(24, precision, s.ptr(), len(s), 12, 0, 0, 4, out)
+    finally:
+        emu.gqx_set_persistent(0)
+    if rc == _abi.GQ_EUNSUPPORTED:
+        pytest.skip("libnvrtc not available")
+    assert rc == 0, emu.gqx_last_error().decode()[:3000]
+    passes, planned, texts, compiled, spilled = list(out)
+    assert planned == passes >= 1 and compiled >= 1 and spilled <= compiled
