@@ -28,7 +28,7 @@ STATEVECTOR_CANDIDATES = [
     {_abi.GQ_OPT_JIT_MIN_BLOCKS: 3},
     # the larger tiles (variant 2: 12 qubits for complex128, 13 for complex64)
     # with other budgets and occupancies
-    {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_PASS_BUDGET: 160},
+    {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_PASS_BUDGET: 200},
     {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_PASS_BUDGET: 240},
     {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_PASS_BUDGET: 400},
     {_abi.GQ_OPT_KERNEL_VARIANT: 2, _abi.GQ_OPT_PASS_BUDGET: 480},

@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <string>
 #include <random>
 
 namespace gq {
@@ -620,6 +622,16 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
         // ---- pass: the tile holds the targets of every absorbed gate.
         std::vector<std::vector<int>> pgroups;
         std::vector<uint64_t> pmasks;
+        // A pass launches at most 2^(support qubits outside the low ones) CTAs
+        // (SchedOptions::support0): while that is below a full pass's
+        // 2^(nphys - m), its arithmetic costs proportionally less, and its
+        // budget grows by the same factor (up to 64x).
+        int budget = opt.budget;
+        {
+            const int full_outer = nphys - m, sup_outer = popc(support & all & ~low_mask);
+            if (sup_outer < full_outer)
+                budget = (int)std::min<int64_t>((int64_t)opt.budget << std::min(6, full_outer - sup_outer), 1 << 28);
+        }
         {
             std::vector<int> take, rest;
             uint64_t T = low_mask, bnd = 0, bd = 0;
@@ -630,7 +642,7 @@ void schedule(const std::vector<NGate>& gates, int nphys, const SchedOptions& op
                     !(g.nd_mask & (bnd | bd)) && !(g.d_mask & bnd) && (!g.barrier || (bnd | bd) == 0);
                 const uint64_t nt = T | g.nd_mask;
                 const bool grad_ok = g.type != K_GRAD || ngrad < MAX_GRAD_SLOTS;
-                if (free && grad_ok && popc(nt) <= m && (used + g.cost <= opt.budget || take.empty())) {
+                if (free && grad_ok && popc(nt) <= m && (used + g.cost <= budget || take.empty())) {
                     T = nt;
                     used += g.cost;
                     ngrad += g.type == K_GRAD;
@@ -994,6 +1006,25 @@ int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, 
         for (int i = 0; i < op.num_qubits; ++i) q.push_back(op.qubits[i]);       // column qubits
         return q;
     };
+    // A noise model applies the same few Kraus sets after many gates: each
+    // distinct set's superoperator and population / coherence form is
+    // computed once per call (keyed by its arity and Kraus entries).
+    struct ChanForm {
+        std::vector<Z> sop, pop_t, coh_d;
+        bool pc = false;
+    };
+    std::map<std::string, ChanForm> chan_forms;
+    auto chan_form = [&](const gq_op& c) -> const ChanForm& {
+        const int kk = c.num_qubits, dd = 1 << kk;
+        std::string key((const char*)&kk, sizeof(kk));
+        key.append((const char*)c.matrix, sizeof(Z) * (size_t)c.num_kraus * dd * dd);
+        auto it = chan_forms.find(key);
+        if (it != chan_forms.end()) return it->second;
+        ChanForm f;
+        f.sop = superop((const Z*)c.matrix, c.num_kraus, kk);
+        f.pc = kk <= 2 && population_coherence(f.sop, kk, f.pop_t, f.coh_d);
+        return chan_forms.emplace(std::move(key), std::move(f)).first->second;
+    };
     for (size_t i = 0; i < n_ops; ++i) {
         const gq_op& op = ops[i];
         if (op.kind == GQ_OP_BARRIER) continue;
@@ -1018,15 +1049,16 @@ int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, 
             rq.push_back(op.qubits[j] + nq);
             cq.push_back(op.qubits[j]);
         }
-        std::vector<Z> sop, pop_t, coh_d;
+        std::vector<Z> sop;
         if (op.kind == GQ_OP_CHANNEL) {
             if (op.num_kraus < 1) { err = "channel without Kraus operators"; return GQ_EINVAL; }
-            sop = superop((const Z*)op.matrix, op.num_kraus, k);
-            if (structured && k <= 2 && population_coherence(sop, k, pop_t, coh_d)) {
-                int rc = emit_population_coherence(pop_t, coh_d, rq, cq, (int)i, gates, err);
+            const ChanForm& cf = chan_form(op);
+            if (structured && cf.pc) {
+                int rc = emit_population_coherence(cf.pop_t, cf.coh_d, rq, cq, (int)i, gates, err);
                 if (rc != GQ_OK) { err = "op " + std::to_string(i) + ": " + err; return rc; }
                 continue;
             }
+            sop = cf.sop;
         } else {
             std::vector<Z> u;
             if (op.kind == GQ_OP_CONTROLLED)
@@ -1036,12 +1068,11 @@ int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, 
             const bool fold = k <= 2 && i + 1 < n_ops && ops[i + 1].kind == GQ_OP_CHANNEL &&
                               ops[i + 1].num_qubits == k && std::equal(ops[i + 1].qubits, ops[i + 1].qubits + k, op.qubits) &&
                               ops[i + 1].matrix && ops[i + 1].num_kraus >= 1;
-            std::vector<Z> chan;
-            if (fold) chan = superop((const Z*)ops[i + 1].matrix, ops[i + 1].num_kraus, k);
-            if (fold && !(structured && population_coherence(chan, k, pop_t, coh_d))) {
+            const ChanForm* cf = fold ? &chan_form(ops[i + 1]) : nullptr;
+            if (fold && !(structured && cf->pc)) {
                 // The channel that follows on the same qubits folds into one
                 // superoperator S * (U (x) conj(U)).
-                sop = matmul(chan, unitary_superop(u, k), d * d);
+                sop = matmul(cf->sop, unitary_superop(u, k), d * d);
                 ++i;
             } else {
                 // U on the row qubits, conj(U) on the column qubits, then the
@@ -1051,7 +1082,7 @@ int dm_gates(int nq, const gq_op* ops, size_t n_ops, std::vector<NGate>& gates, 
                 int rc = analyze_matrix(u, rq, 0, (int)i, gates, err);
                 if (rc == GQ_OK) rc = analyze_matrix(uc, cq, 0, (int)i, gates, err);
                 if (rc == GQ_OK && fold) {
-                    rc = emit_population_coherence(pop_t, coh_d, rq, cq, (int)(i + 1), gates, err);
+                    rc = emit_population_coherence(cf->pop_t, cf->coh_d, rq, cq, (int)(i + 1), gates, err);
                     ++i;
                 }
                 if (rc != GQ_OK) { err = "op " + std::to_string(i) + ": " + err; return rc; }

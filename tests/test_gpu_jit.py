@@ -157,10 +157,11 @@ def test_specialised_reverse_passes_general_gates():
 
 
 @pytest.mark.parametrize("n,seed,variant", [(16, 51, 0), (22, 52, 2)])
-def test_zero_tile_skip_is_bit_identical(n, seed, variant):
+def test_zero_tile_skip_matches_full_launch(n, seed, variant):
     # Evolve from the reset state launches only the tiles inside the support
-    # (GQ_OPT_ZERO_TILES, default on): the state must be bit-identical to the
-    # run that launches every tile, and the tile bytes smaller
+    # (GQ_OPT_ZERO_TILES, default on): the state must match the run that
+    # launches every tile (the short passes' larger budgets may change the
+    # schedule and its rounding, not the result), and the tile bytes shrink
     c = workloads.random_layers_qft(n, 3, seed) if n > 16 else random_circuit(n, 120, seed, allow_reset=True)
     states, tb = [], []
     for skip in (0, 1):
@@ -170,11 +171,13 @@ def test_zero_tile_skip_is_bit_identical(n, seed, variant):
         sim.Evolve(c)
         st = sim.stats()
         assert st["jit_passes"] == st["passes"] >= 1
+        if not skip:
+            assert st["tile_bytes"] == st["passes"] * 2 * st["state_bytes"]
         states.append(sim.StateVector())
         tb.append(st["tile_bytes"])
         sim.Close()
-    assert np.array_equal(states[0], states[1])
-    assert tb[0] == st["passes"] * 2 * st["state_bytes"] and tb[1] < tb[0]
+    np.testing.assert_allclose(states[1], states[0], atol=1e-13, rtol=0)
+    assert tb[1] < tb[0]
     if n <= 16:
         np.testing.assert_allclose(states[1], orc.sv_evolve(encode.statevector_ops(c)), atol=1e-12, rtol=0)
 
@@ -192,7 +195,7 @@ def test_zero_tile_skip_density_matrix_and_apply():
         assert (st["tile_bytes"] < st["passes"] * 2 * st["state_bytes"]) == bool(skip)
         rhos.append(dm.DensityMatrix())
         dm.Close()
-    assert np.array_equal(rhos[0], rhos[1])
+    np.testing.assert_allclose(rhos[1], rhos[0], atol=1e-13, rtol=0)
     # Apply composes on the current state: nothing may be skipped there
     g = random_circuit(16, 60, 54)
     sim = jit_sim(16)
@@ -204,7 +207,7 @@ def test_zero_tile_skip_density_matrix_and_apply():
     sim2.set_option(_abi.GQ_OPT_ZERO_TILES, 0)
     sim2.Evolve(g)
     sim2.Apply(g)
-    assert np.array_equal(sim.StateVector(), sim2.StateVector())
+    np.testing.assert_allclose(sim.StateVector(), sim2.StateVector(), atol=1e-13, rtol=0)
 
 
 @pytest.mark.parametrize("variant", [0, 2])

@@ -307,7 +307,7 @@ def test_generated_code_skipping_zero_tiles(emu, tmp_path, n, seed, tile):
         emu.gqx_set_support0(2 ** 64 - 1)
     np.testing.assert_allclose(got, orc.sv_evolve(ops), atol=1e-12, rtol=0)
     full = jit_emulate(emu, ops, n, tmp_path, tile=tile)
-    assert np.array_equal(got, full)
+    np.testing.assert_allclose(got, full, atol=1e-13, rtol=0)
     assert ctas < emu.gqx_last_ctas()
 
 
@@ -325,7 +325,7 @@ def test_generated_code_density_matrix_skipping_zero_tiles(emu, tmp_path):
         emu.gqx_set_support0(2 ** 64 - 1)
     np.testing.assert_allclose(got, orc.dm_evolve(ops), atol=1e-12, rtol=0)
     full = jit_emulate(emu, ops, 5, tmp_path, dm=1, tile=5)
-    assert np.array_equal(got, full)
+    np.testing.assert_allclose(got, full, atol=1e-13, rtol=0)
     assert ctas < emu.gqx_last_ctas()
 
 

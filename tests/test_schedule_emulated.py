@@ -308,7 +308,8 @@ def test_zero_tile_skip_matches_oracle(emu, n, seed, tile, budget):
     want = orc.sv_evolve(ops)
     full, ctas_full = _with_support(emu, 2 ** 64 - 1, lambda: run_emu(emu, ops, tile=tile, budget=budget)[0])
     got, ctas = _with_support(emu, 0, lambda: run_emu(emu, ops, tile=tile, budget=budget)[0])
-    assert np.array_equal(got, full)  # the launched tiles compute exactly what they did before
+    # the short passes take larger budgets, so the schedule (and the rounding) may differ
+    np.testing.assert_allclose(got, full, atol=1e-13, rtol=0)
     np.testing.assert_allclose(got, want, atol=1e-12, rtol=0)
     assert ctas < ctas_full
 
@@ -332,7 +333,9 @@ def test_zero_tile_skip_late_support():
 
 def test_zero_tile_skip_headline_openers(emu):
     # 28 qubits, 40 U3+CNOT brickwork layers + QFT28, 12-qubit tiles: the
-    # first pass runs one CTA and the second 2^9 of 2^16; the rest are full
+    # first pass runs one CTA and the second 2^9 of 2^16; the rest are full.
+    # The two short passes take larger budgets (64x), so they absorb more of
+    # the opening layers and the full passes that follow carry less
     f = emu.gqx_schedule_passes
     f.restype = ctypes.c_int64
     f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_abi.gq_op), ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
@@ -343,10 +346,11 @@ def test_zero_tile_skip_headline_openers(emu):
     out = (ctypes.c_int64 * (5 * 400))()
     (np_full, _) = _with_support(emu, 2 ** 64 - 1, lambda: f(28, 0, ops.ptr(), len(ops), 12, 0, out_full, 400))
     (np_zero, _) = _with_support(emu, 0, lambda: f(28, 0, ops.ptr(), len(ops), 12, 0, out, 400))
-    assert np_full == np_zero
+    assert np_zero <= np_full
     bits = [out[5 * i + 4] for i in range(np_zero)]
     assert [out_full[5 * i + 4] for i in range(np_full)] == [16] * np_full
     assert bits[0] == 0 and bits[1] == 9 and all(b == 16 for b in bits[2:])
-    # the schedule is otherwise the same pass for pass
-    for i in range(np_zero):
-        assert [out[5 * i + k] for k in range(4)] == [out_full[5 * i + k] for k in range(4)]
+    cost = [out[5 * i + 2] for i in range(np_zero)]
+    cost_full = [out_full[5 * i + 2] for i in range(np_full)]
+    assert sum(cost) == sum(cost_full)  # the same gates, placed differently
+    assert cost[0] > cost_full[0] and max(cost[2:]) <= max(cost_full)
