@@ -280,6 +280,8 @@ def extra_adjoint():
         _, g_adj = ev(x)
         dev.append(ev.sim.stats()["last_ms"])
     wall = (time.perf_counter() - t0) / 10
+    st = ev.sim.stats()
+    adj_stats = {k: st[k] for k in ("passes", "jit_passes", "kernel_launches", "pass_ms")}
     f = gradient.CostFunc(c, h, names)
     f.sim.set_option(_abi.GQ_OPT_TIMING, 1)
     f.sim.set_option(_abi.GQ_OPT_JIT, 2)
@@ -304,6 +306,7 @@ def extra_adjoint():
             "max_abs_diff_vs_oracle_param_shift": float(np.max(np.abs(g_adj[sel] - g_or))),
             "oracle_sample": f"{len(sel)} parameters: RY and RZ of 2 qubits in each of the 10 layers",
             "adjoint_grads_per_s": 1000.0 / adj_ms, "adjoint_ms_device": adj_ms, "adjoint_ms_wall": wall * 1e3,
+            "adjoint_ms_device_calls": [round(v, 3) for v in dev], "adjoint_call_stats": adj_stats,
             "param_shift_grads_per_s": 1000.0 / ps_dev, "param_shift_ms_device": ps_dev,
             "param_shift_ms_wall": ps_wall * 1e3, "speedup_device": ps_dev / adj_ms,
             "speedup_wall": ps_wall / wall,
