@@ -15,6 +15,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <future>
 #include <vector>
 
 #include "../../include/gqb200.h"
@@ -199,10 +200,14 @@ struct Engine {
     DevBuf hist;                              // shot histograms (counts.cuh)
     int adj_nparams = 0;                      // parameters of the current gradient
     int adj_segments = 0;                     // forward checkpoints (0: automatic)
-    PinnedBuf staging, hostio;
-    cudaEvent_t staged = nullptr, ev0 = nullptr, ev1 = nullptr, ev_pass0 = nullptr, ev_pass1 = nullptr;
+    // Two host staging buffers used in turn: a program is packed into one
+    // while the upload from the other may still wait behind running passes.
+    PinnedBuf staging[2], hostio;
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    int stage_slot = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_pass0 = nullptr, ev_pass1 = nullptr;
     bool pass_timed = false;
-    bool staged_pending = false;
+    bool staged_pending[2] = {false, false};
     SchedOptions opt;
     bool timing = false;
     gq_stats stats{};
@@ -231,7 +236,7 @@ struct Engine {
         n_amps = 1ull << nphys;
         GQ_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         GQ_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
-        GQ_CUDA(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+        for (cudaEvent_t& ev : staged) GQ_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         GQ_CUDA(cudaEventCreate(&ev0));
         GQ_CUDA(cudaEventCreate(&ev1));
         GQ_CUDA(cudaEventCreate(&ev_pass0));
@@ -259,9 +264,10 @@ struct Engine {
         adj_partial.release();
         adj_grad.release();
         hist.release();
-        staging.release();
+        for (PinnedBuf& b : staging) b.release();
         hostio.release();
-        if (staged) cudaEventDestroy(staged);
+        for (cudaEvent_t& ev : staged)
+            if (ev) cudaEventDestroy(ev);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (ev_pass0) cudaEventDestroy(ev_pass0);
@@ -281,22 +287,23 @@ struct Engine {
         return GQ_OK;
     }
 
-    // Host staging buffer is reused: wait for the previous upload to finish.
+    // The next staging buffer: wait for the upload that last used it.
     int stage(size_t bytes, void** host) {
-        if (staged_pending) {
-            GQ_CUDA(cudaEventSynchronize(staged));
-            staged_pending = false;
+        stage_slot ^= 1;
+        if (staged_pending[stage_slot]) {
+            GQ_CUDA(cudaEventSynchronize(staged[stage_slot]));
+            staged_pending[stage_slot] = false;
         }
-        GQ_TRY(staging.ensure(bytes));
-        *host = staging.p;
+        GQ_TRY(staging[stage_slot].ensure(bytes));
+        *host = staging[stage_slot].p;
         return GQ_OK;
     }
     int upload(DevBuf& dst, size_t bytes) {
         GQ_TRY(dst.ensure(bytes));
         stats.h2d_bytes += (int64_t)bytes;
-        GQ_CUDA(cudaMemcpyAsync(dst.p, staging.p, bytes, cudaMemcpyHostToDevice, stream));
-        GQ_CUDA(cudaEventRecord(staged, stream));
-        staged_pending = true;
+        GQ_CUDA(cudaMemcpyAsync(dst.p, staging[stage_slot].p, bytes, cudaMemcpyHostToDevice, stream));
+        GQ_CUDA(cudaEventRecord(staged[stage_slot], stream));
+        staged_pending[stage_slot] = true;
         return GQ_OK;
     }
 
@@ -513,11 +520,14 @@ struct Engine {
         return GQ_OK;
     }
 
-    int run_adjoint(const std::vector<NGate>& gates) {
+    // Scheduling options of the reverse sweep (two-state tiles of up to
+    // 2^(log2 kAdjThreads + RQ) amplitudes).
+    SchedOptions adjoint_options() const {
         SchedOptions o = opt;
         o.tile_qubits = std::min(o.tile_qubits, log2i(kAdjThreads) + RQ);
-        Program pr;
-        schedule(gates, nphys, o, pr);
+        return o;
+    }
+    int run_adjoint(const Program& pr) {
         return prec == GQ_C64 ? run_adjoint_t<float>(pr) : run_adjoint_t<double>(pr);
     }
 
@@ -589,6 +599,18 @@ struct Engine {
 
     // ---- reductions -----------------------------------------------------
     int reduce_grid() const { return 148 * 4; }
+
+    // The same without waiting: the sum lands in the second 16 bytes of
+    // hostio once the stream has passed this point (read it after a sync).
+    int finish_reduce_async(int nblocks) {
+        k_final_reduce<<<1, 1024, 0, stream>>>((const double2*)scratch.p, nblocks, (double2*)scratch.p + nblocks);
+        GQ_CUDA(cudaGetLastError());
+        GQ_TRY(hostio.ensure(64));
+        GQ_CUDA(cudaMemcpyAsync((char*)hostio.p + 16, (double2*)scratch.p + nblocks, sizeof(double2),
+                                cudaMemcpyDeviceToHost, stream));
+        stats.kernel_launches += 2;
+        return GQ_OK;
+    }
 
     int finish_reduce(int nblocks, double* re, double* im) {
         k_final_reduce<<<1, 1024, 0, stream>>>((const double2*)scratch.p, nblocks, (double2*)scratch.p + nblocks);
@@ -1085,6 +1107,18 @@ int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_p
         while (j + 1 < segs && (size_t)op_index >= bound[j + 1]) ++j;
         return j;
     };
+    // The reverse programs depend on the gates only: a worker thread
+    // schedules them while this thread schedules and launches the forward
+    // sweep (the future joins on every return path).
+    std::vector<std::vector<NGate>> rparts(segs);
+    for (size_t k = 0; k < rev.size(); ++k) rparts[seg_of(ro[k])].push_back(rev[k]);
+    const SchedOptions ropt = e.adjoint_options();
+    const int nphys = e.nphys;
+    auto rprogs = std::async(std::launch::async, [&rparts, &ropt, nphys] {
+        std::vector<Program> progs(rparts.size());
+        for (size_t j = 0; j < rparts.size(); ++j) schedule(rparts[j], nphys, ropt, progs[j]);
+        return progs;
+    });
     GQ_TRY(e.reset_basis(0));
     uint64_t support = 0;
     for (int j = 0; j < segs; ++j) {
@@ -1116,26 +1150,23 @@ int gq_sv_adjoint_gradient(gq_sv* sv, const gq_op* ops, size_t n_ops, const gq_p
                                                             na, (const DGroup*)d, ng, (const DTerm*)(d + ot),
                                                             (double2*)e.scratch.p);
         GQ_CUDA(cudaGetLastError());
-        double en = 0.0;
-        GQ_TRY(e.finish_reduce(nb, &en, nullptr));
-        if (energy_out) *energy_out = en;
+        GQ_TRY(e.finish_reduce_async(nb));  // read after the final synchronisation
         ++e.stats.kernel_launches;
     }
     // reverse sweep
     GQ_CUDA(cudaMemsetAsync(e.adj_grad.p, 0, std::max<size_t>(1, n_params) * sizeof(double), e.stream));
+    const std::vector<Program> rp = rprogs.get();
     for (int j = segs - 1; j >= 0; --j) {
         if (j + 1 < segs)
             GQ_CUDA(cudaMemcpyAsync(e.state.p, (char*)e.ckpt.p + sbytes * j, sbytes, cudaMemcpyDeviceToDevice, e.stream));
-        std::vector<NGate> part;
-        for (size_t k = 0; k < rev.size(); ++k)
-            if (seg_of(ro[k]) == j) part.push_back(rev[k]);
-        GQ_TRY(e.run_adjoint(part));
+        GQ_TRY(e.run_adjoint(rp[j]));
     }
     if (n_params) {
         GQ_CUDA(cudaMemcpyAsync(grad_out, e.adj_grad.p, n_params * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
         e.stats.d2h_bytes += (int64_t)(n_params * sizeof(double));
     }
     GQ_CUDA(cudaStreamSynchronize(e.stream));
+    if (energy_out) *energy_out = ((const double2*)((const char*)e.hostio.p + 16))->x;
     return e.time_end();
 }
 
