@@ -301,12 +301,18 @@ def extra_adjoint():
     adj_ms = float(np.median(dev))
     from oracle import gradient as og
     sel = og.stratified_hea_params(20, 10)
+    t_or = time.perf_counter()
     g_or = og.parameter_shift(c, names, x, h, sel, threads=os.cpu_count() or 1)
+    t_or = time.perf_counter() - t_or
     return {"workload": "adjoint gradient, 20q HEA 10 layers, 400 params, Ising H (39 terms), complex128",
             "max_abs_diff_vs_oracle_param_shift": float(np.max(np.abs(g_adj[sel] - g_or))),
             "oracle_sample": f"{len(sel)} parameters: RY and RZ of 2 qubits in each of the 10 layers",
             "adjoint_grads_per_s": 1000.0 / adj_ms, "adjoint_ms_device": adj_ms, "adjoint_ms_wall": wall * 1e3,
             "adjoint_ms_device_calls": [round(v, 3) for v in dev], "adjoint_call_stats": adj_stats,
+            "cpu_oracle": {"what": "FP64 oracle parameter shift (2 evaluations per parameter, prefixes shared) "
+                                   "of the sampled parameters on the host cores",
+                           "params": len(sel), "seconds": t_or, "cores": os.cpu_count(),
+                           "grads_per_s_all_400_params": len(sel) / (len(names) * t_or)},
             "param_shift_grads_per_s": 1000.0 / ps_dev, "param_shift_ms_device": ps_dev,
             "param_shift_ms_wall": ps_wall * 1e3, "speedup_device": ps_dev / adj_ms,
             "speedup_wall": ps_wall / wall,
@@ -405,7 +411,9 @@ def extra_density():
     def check(n, layers):
         cc, nn = workloads.noisy_brickwork(n, layers=layers, seed=12)
         ss = encode.density_ops(cc, nn)
+        t_or = time.perf_counter()
         want = orc.dm_evolve(ss, threads=os.cpu_count() or 1)
+        t_or = time.perf_counter() - t_or
         d = densitymatrix.New(n).WithNoise(nn)
         d.set_option(_abi.GQ_OPT_JIT, 2)
         d.set_option(_abi.GQ_OPT_JIT_MIN_QUBITS, 0)
@@ -415,7 +423,8 @@ def extra_density():
                     for q in range(n))
         out = {"layers": layers, "max_abs_rho_error_vs_fp64_oracle": float(np.max(np.abs(d.DensityMatrix() - want))),
                "max_abs_z_error_vs_fp64_oracle": z_err,
-               "trace_error_vs_fp64_oracle": abs(d.Trace() - np.trace(want.reshape(1 << n, 1 << n)))}
+               "trace_error_vs_fp64_oracle": abs(d.Trace() - np.trace(want.reshape(1 << n, 1 << n))),
+               "cpu_oracle_s": t_or, "cpu_cores": os.cpu_count()}
         d.Close()
         return out
 
@@ -557,6 +566,7 @@ def extra_qaoa_dedicated(calls=3):
     e_gen, g_gen = gen.Run(evals)
     from oracle import gradient as og
     th = os.cpu_count() or 1
+    t_or = time.perf_counter()
     e_err = g_err = 0.0
     for k in range(0, len(evals), max(1, len(evals) // 16)):
         c, names, h, x = evals[k]
@@ -564,6 +574,8 @@ def extra_qaoa_dedicated(calls=3):
         e_err = max(e_err, abs(e_fast[k] - og.energy(c, names, x, h, threads=th)))
         fd = og.parameter_shift(c, names, x, h, threads=th, shift=1e-6, denom=2e-6)
         g_err = max(g_err, float(np.max(np.abs(g_fast[k] - fd))))
+    t_or = time.perf_counter() - t_or
+    n_or = len(range(0, len(evals), max(1, len(evals) // 16)))
     # algorithmic bytes: per circuit above 12 qubits, every forward pass reads and
     # writes psi (8 B per amplitude), every reverse pass psi and lambda, plus the
     # cut table (1 B) wherever it is read; circuits of <= 12 qubits stay on chip
@@ -585,6 +597,10 @@ def extra_qaoa_dedicated(calls=3):
             "max_abs_energy_diff_vs_general_batch": float(np.max(np.abs(np.asarray(e_fast) - np.asarray(e_gen)))),
             "max_abs_grad_diff_vs_general_batch": float(max(np.max(np.abs(a - c)) for a, c in zip(g_fast, g_gen))),
             "max_abs_energy_error_vs_fp64_oracle": e_err, "max_abs_grad_error_vs_fp64_central_difference": g_err,
+            "cpu_oracle": {"what": "FP64 oracle energy + central-difference gradient (2 evaluations per parameter) "
+                                   "of the sampled circuits on the host cores",
+                           "circuits": n_or, "seconds": t_or, "cores": os.cpu_count(),
+                           "circuits_per_s": n_or / t_or},
             "roofline": {"bound": "hbm", "algorithmic_bytes": alg,
                          "achieved": alg / (best / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / (best / 1000.0) / 1e9 / peak, "peak_kind": peak_kind,
