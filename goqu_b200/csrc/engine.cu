@@ -350,7 +350,9 @@ struct Engine {
                     if (plans[i]->ok && !jfn[i]) jfn[i] = jit_plan_kernel(plans[i], jit_smem<T>(pr.passes[i].m));
             }
         }
-        if (timing) GQ_CUDA(cudaEventRecord(ev_pass0, stream));
+        // the span from the call's first pass to its last (a call may run
+        // several programs: checkpoint segments, a split density-matrix stream)
+        if (timing && !pass_timed) GQ_CUDA(cudaEventRecord(ev_pass0, stream));
         std::vector<cplx<T>> pblock;
         int64_t jitted = 0;
         for (size_t i = 0; i < np; ++i) {
@@ -538,10 +540,18 @@ struct Engine {
     // support after them. Only callers that have just reset the state pass it.
     int run_gates(const std::vector<NGate>& gates, uint64_t* support = nullptr) {
         Program pr;
+        schedule(gates, nphys, run_options(support), pr);
+        return run_scheduled(pr, support);
+    }
+    // The scheduling options of run_gates.
+    SchedOptions run_options(const uint64_t* support) const {
         SchedOptions o = opt;
         o.fuse_pairs = !jit_on();  // specialised kernels take diagonals as free pending factors
         if (support && skip_zero_tiles) o.support0 = *support;
-        schedule(gates, nphys, o, pr);
+        return o;
+    }
+    // Runs a program scheduled with run_options(support).
+    int run_scheduled(const Program& pr, uint64_t* support) {
         if (support) *support = skip_zero_tiles ? pr.support_out : ~0ull;
         stats.gates_in += pr.gates;
         for (const PassDesc& pd : pr.passes) stats.tile_bytes += (int64_t)(2 * amp_bytes()) << (pd.m + pd.n_outer);
@@ -1202,15 +1212,53 @@ int gq_dm_reset(gq_dm* dm) {
 }
 
 // support: see Engine::run_gates (null: the state is arbitrary).
+// Op streams at least this long are analysed and scheduled in two halves.
+constexpr size_t kDmSplitOps = 256;
+
 static int dm_apply_impl(gq_dm* dm, const gq_op* ops, size_t n_ops, uint64_t* support = nullptr) {
     if (n_ops && !ops) return fail(GQ_EINVAL, "null ops");
-    std::vector<NGate> gates;
-    {
+    const bool structured = !dm->dense_channels;
+    // A long stream is split at a gate (a gate keeps the channel after it): a
+    // worker thread analyses and schedules the second half while this thread
+    // does the first and launches it. Nothing launches before both halves
+    // passed the analysis, as for the whole stream.
+    size_t mid = n_ops >= kDmSplitOps ? n_ops / 2 : n_ops;
+    while (mid < n_ops && ops[mid].kind == GQ_OP_CHANNEL) ++mid;
+    if (mid >= n_ops) {
+        std::vector<NGate> gates;
         std::string err;
-        int rc = dm_gates(dm->nq, ops, n_ops, gates, err, !dm->dense_channels);
+        int rc = dm_gates(dm->nq, ops, n_ops, gates, err, structured);
         if (rc != GQ_OK) return fail(rc, err);
+        return dm->e.run_gates(gates, support);
     }
-    return dm->e.run_gates(gates, support);
+    const int nq = dm->nq, nphys = dm->e.nphys;
+    const SchedOptions o2 = dm->e.run_options(nullptr);  // the second half's start state is arbitrary
+    std::promise<int> analysed;
+    std::future<int> analysed_rc = analysed.get_future();
+    auto second = std::async(std::launch::async, [&analysed, &o2, ops, n_ops, mid, nq, nphys, structured] {
+        std::vector<NGate> g;
+        std::string err;
+        const int rc = dm_gates(nq, ops + mid, n_ops - mid, g, err, structured);
+        analysed.set_value(rc);
+        Program pr;
+        if (rc == GQ_OK) schedule(g, nphys, o2, pr);
+        return pr;
+    });
+    std::vector<NGate> gates;
+    std::string err;
+    int rc = dm_gates(nq, ops, mid, gates, err, structured);
+    if (rc != GQ_OK) return fail(rc, err);
+    Program first;
+    schedule(gates, nphys, dm->e.run_options(support), first);
+    if (analysed_rc.get() != GQ_OK) {
+        // the message names the op in the whole stream
+        std::vector<NGate> all;
+        rc = dm_gates(nq, ops, n_ops, all, err, structured);
+        return fail(rc != GQ_OK ? rc : GQ_EINVAL, err);
+    }
+    GQ_TRY(dm->e.run_scheduled(first, support));
+    const Program pr = second.get();
+    return dm->e.run_scheduled(pr, support ? support : nullptr);
 }
 
 static int dm_apply_timed(gq_dm* dm, const gq_op* ops, size_t n_ops, bool reset) {

@@ -112,7 +112,7 @@ typedef struct gq_stats {
     int64_t state_bytes;     /* bytes of one state (2^n * amplitude size)          */
     double last_ms;          /* device time of the last apply/evolve call, CUDA events
                                 on the handle's stream (GQ_OPT_TIMING only)           */
-    double pass_ms;          /* device time of its tile passes alone                */
+    double pass_ms;          /* device time of its tile passes alone (first to last) */
     int64_t h2d_bytes;       /* host->device bytes the last call copied (program, inputs) */
     int64_t d2h_bytes;       /* device->host bytes the last call copied (results)   */
     int64_t jit_passes;      /* passes of the last call run by a specialised kernel */

@@ -112,3 +112,23 @@ def test_readout_sampling_bit_exact():
     u = statevector.uniforms(2000, rng)
     assert np.array_equal(dm.Sample(u), orc.sample(probs, u))
     np.testing.assert_array_equal(dm.ApplyReadoutError(dm.DiagonalProbs()), probs)
+
+
+@pytest.mark.parametrize("dense", [0, 1])
+def test_long_stream_planned_in_two_halves(dense):
+    # streams of >= 256 ops are analysed and scheduled in two halves (the
+    # second on a worker thread): the result must not depend on it, in the
+    # channel-form and the dense-superoperator modes, with the JIT on and off
+    from goqu_b200 import _abi
+    c, nm = workloads.noisy_brickwork(10, layers=12, seed=71)
+    ops = encode.density_ops(c, nm)
+    assert len(ops) >= 256
+    want = orc.dm_evolve(ops, threads=8)
+    for jit in (0, 2):
+        dm = densitymatrix.New(10).WithNoise(nm)
+        dm.set_option(_abi.GQ_OPT_DM_DENSE_CHANNELS, dense)
+        dm.set_option(_abi.GQ_OPT_JIT, jit)
+        dm.set_option(_abi.GQ_OPT_JIT_MIN_QUBITS, 0)
+        dm.Evolve(c)
+        assert np.max(np.abs(dm.DensityMatrix() - want)) < TOL
+        dm.Close()
