@@ -476,11 +476,15 @@ __global__ void k_chunk_steps(P prob, uint64_t n, int chunk_log, const double* _
 // together). A chunk is taken in O(1) when it is clean in s's binade and
 // s plus its exact step count stays below 2^(e+1): the ends of the window's
 // leading run of such chunks are s plus the int64 window prefix times the
-// ulp of the binade (exact). The first chunk after that run is summed
-// element by element with goqu's own additions (the warp loads 32 elements
-// at a time; every lane adds them in order, so s stays warp-uniform); then
-// the next window starts after it.
+// ulp of the binade (exact). The first chunk after that run is summed in
+// sub-chunks of 64 elements with the same rule, now against the exact s: a
+// sub-chunk whose elements all round without a tie in s's binade and whose
+// end stays below 2^(e+1) adds its int64 step count times the ulp; any other
+// sub-chunk is summed element by element with goqu's own additions (every
+// lane adds the 64 elements in order, so s stays warp-uniform). Then the
+// next window starts after the chunk.
 constexpr int kWalkK = 8;
+constexpr int kSubChunk = 64;
 
 template <class P>
 __global__ void k_chunk_walk(P prob, uint64_t n, int chunk_log, const long long* __restrict__ steps,
@@ -498,6 +502,10 @@ __global__ void k_chunk_walk(P prob, uint64_t n, int chunk_log, const long long*
         const bool pos = s > 0.0;
         const int se = pos ? exponent_of(s) : 0;
         const double lim = pos ? ldexp(1.0, se + 1) : 0.0;
+        // ulp of s's binade; run * ulp equals ldexp(run, se - 52) exactly (a
+        // power-of-two scaling; it is only used for clean chunks, whose
+        // binade has se >= -1000)
+        const double ulp = pos ? ldexp(1.0, se - 52) : 0.0;
         long long st[kWalkK];
         bool ok[kWalkK];
         long long lsum = 0;
@@ -521,7 +529,7 @@ __global__ void k_chunk_walk(P prob, uint64_t n, int chunk_log, const long long*
 #pragma unroll
         for (int k = 0; k < kWalkK; ++k) {
             run += st[k];
-            const bool good = ok[k] && s + ldexp((double)run, se - 52) < lim;
+            const bool good = ok[k] && s + (double)run * ulp < lim;
             if (!good && bad == W) bad = lane * kWalkK + k;
         }
 #pragma unroll
@@ -533,23 +541,60 @@ __global__ void k_chunk_walk(P prob, uint64_t n, int chunk_log, const long long*
         for (int k = 0; k < kWalkK; ++k) {
             run += st[k];
             const int p = lane * kWalkK + k;
-            if (p < bad) ends[c + p] = s + ldexp((double)run, se - 52);
+            if (p < bad) ends[c + p] = s + (double)run * ulp;
             if (p == bad - 1) upto = run;
         }
         if (bad > 0) {
             upto = __shfl_sync(full, upto, (bad - 1) / kWalkK);
-            s = s + ldexp((double)upto, se - 52);
+            s = s + (double)upto * ulp;
         }
         c += (uint64_t)bad;
         if (bad == W || c >= nchunks) continue;
-        // chunk c: element by element
+        // chunk c: sub-chunk by sub-chunk
         ++seq;
         const uint64_t c0 = c << chunk_log;
         const uint64_t e1 = c0 + len < n ? c0 + len : n;
-        for (uint64_t b = c0; b < e1; b += 32) {
-            const double pv = b + lane < e1 ? prob(b + lane) : 0.0;
-            const int cnt = e1 - b < 32 ? (int)(e1 - b) : 32;
-            for (int k = 0; k < cnt; ++k) s = __dadd_rn(s, __shfl_sync(full, pv, k));
+        for (uint64_t b = c0; b < e1; b += kSubChunk) {
+            const double p0 = b + lane < e1 ? prob(b + lane) : 0.0;
+            const double p1 = b + 32 + lane < e1 ? prob(b + 32 + lane) : 0.0;
+            bool taken = false;
+            if (s > 0x1p-1000) {  // s normal: binade e, ulp 2^(e-52)
+                const int e = exponent_of(s);
+                const double lim = ldexp(1.0, e + 1);
+                double tot = p0 + p1;  // approximate sum (guards the scaling below against overflow)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(full, tot, o);
+                if (s + tot < lim * (1.0 - 0x1p-30)) {
+                    long long ks = 0;
+                    int tie = 0;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const double q = ldexp(h ? p1 : p0, 52 - e);  // exact: a power-of-two scaling, q < 2^53
+                        const double f = floor(q);
+                        const double fr = q - f;  // exact
+                        long long kk = (long long)f;
+                        if (fr > 0.5) ++kk;
+                        if (fr == 0.5) tie = 1;
+                        ks += kk;
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        ks += __shfl_xor_sync(full, ks, o);
+                        tie |= __shfl_xor_sync(full, tie, o);
+                    }
+                    if (!tie) {
+                        const double sn = s + ldexp((double)ks, e - 52);  // exact: on the binade's grid, below lim
+                        if (sn < lim) {
+                            s = sn;
+                            taken = true;
+                        }
+                    }
+                }
+            }
+            if (!taken) {
+                const int cnt = e1 - b < (uint64_t)kSubChunk ? (int)(e1 - b) : kSubChunk;
+                for (int k = 0; k < cnt; ++k) s = __dadd_rn(s, __shfl_sync(full, k < 32 ? p0 : p1, k & 31));
+            }
         }
         if (lane == 0) ends[c] = s;
         ++c;
