@@ -607,6 +607,30 @@ def extra_qaoa_dedicated(calls=3):
                          "note": "whole-call wall time; circuits of <= 12 qubits add no HBM bytes"}}
 
 
+def extra_sampling(n=28, calls=10):
+    """Exact sampling of the benchmark circuit's 28-qubit state: 1024 shots
+    per call (gq_sv_sample: chunk sums, scan, chunk step counts, the exact
+    walk, per-shot search), wall time of the whole call (uniform upload,
+    kernels, index download)."""
+    from goqu_b200 import _abi, statevector
+    c, stream, gates = build_workload(n)
+    sim = statevector.New(n)
+    sim.set_option(_abi.GQ_OPT_JIT, 2)
+    sim.evolve_ops(stream)
+    u = statevector.uniforms(SHOTS, np.random.default_rng(SEED))
+    first = sim.Sample(u)
+    ms = []
+    for _ in range(calls):
+        t0 = time.perf_counter()
+        idx = sim.Sample(u)
+        ms.append(1e3 * (time.perf_counter() - t0))
+    same = bool(np.array_equal(idx, first))
+    sim.Close()
+    return {"workload": f"{SHOTS} shots of the {n}q benchmark state (complex128)", "ms_call_wall": float(np.median(ms)),
+            "calls": calls, "repeatable": same,
+            "note": "indices are checked bit-exact against the oracle in parity_28q and the GPU tests"}
+
+
 def workloads_qaoa_4096():
     from goqu_b200 import workloads
     return workloads.qaoa_batch(4096, seed=4)
@@ -770,7 +794,7 @@ def run_gpu(args, world, rank, local):
         for name, fn in (("parity_20q", extra_parity), ("adjoint", extra_adjoint), ("density_matrix", extra_density),
                          ("qaoa_batch", extra_qaoa), ("qaoa_dedicated", extra_qaoa_dedicated),
                          ("vqe_loop", extra_vqe), ("cold_start", extra_cold_start),
-                         ("parity_28q", extra_parity_28q)):
+                         ("sampling", extra_sampling), ("parity_28q", extra_parity_28q)):
             try:
                 extras[name] = fn()
             except Exception as exc:  # an extra must not hide the headline line
@@ -798,7 +822,7 @@ def main():
     ap.add_argument("--jit", type=int, choices=[0, 1, 2], default=2,
                     help="specialised pass kernels: 0 off, 1 when compiled, 2 wait for them (default)")
     ap.add_argument("--only-extra", choices=["parity_20q", "adjoint", "density_matrix", "qaoa_batch", "parity_28q",
-                                             "vqe_loop", "cold_start", "qaoa_dedicated"],
+                                             "vqe_loop", "cold_start", "qaoa_dedicated", "sampling"],
                     help="run one extra workload alone and print its JSON (profiling)")
     ap.add_argument("--qaoa-qubits", type=int, default=0, help="qaoa_batch: keep the circuits of this size")
     ap.add_argument("--qaoa-count", type=int, default=0, help="qaoa_batch: keep the first N circuits")
@@ -817,7 +841,7 @@ def main():
     if args.only_extra:
         fns = {"parity_20q": extra_parity, "adjoint": extra_adjoint, "density_matrix": extra_density,
                "parity_28q": extra_parity_28q, "vqe_loop": extra_vqe, "cold_start": extra_cold_start,
-               "qaoa_dedicated": extra_qaoa_dedicated,
+               "qaoa_dedicated": extra_qaoa_dedicated, "sampling": extra_sampling,
                "qaoa_batch": lambda: extra_qaoa(args.qaoa_qubits, args.qaoa_count, args.qaoa_calls,
                                                 args.qaoa_graph == 1)}
         print(json.dumps({args.only_extra: fns[args.only_extra]()}))
