@@ -544,13 +544,18 @@ def extra_parity_28q(n=28, steps=3):
     return out
 
 
-def extra_qaoa_dedicated(calls=3):
+def extra_qaoa_dedicated(qubits=0, count=0, calls=3):
     """The same 4096 QAOA MaxCut circuits through the dedicated path
     (gq_qaoa_maxcut_batch): cut-count tables, whole circuits of <= 12 qubits
     in one CTA, batched tile passes above; energies and gradients against the
-    general batch path and the FP64 oracle."""
+    general batch path and the FP64 oracle. qubits / count keep only the
+    circuits of that size / the first `count` (profiling cases)."""
     from goqu_b200 import _abi, batch, qaoa
     evals = workloads_qaoa_4096()
+    if qubits:
+        evals = [e for e in evals if e[0].NumQubits() == qubits]
+    if count:
+        evals = evals[:count]
     t0 = time.perf_counter()
     items = [qaoa.from_evaluation(e) for e in evals]
     b = qaoa.MaxCutBatch()
@@ -588,8 +593,8 @@ def extra_qaoa_dedicated(calls=3):
         alg += (1 << n) * (passes * 16 + passes * 32 + 2 * p + 1)
     peak, peak_kind = peaks()
     best = min(ms)
-    return {"workload": "4096 QAOA MaxCut circuits (n 10..20, p 1..4), complex64, energies + gradients, "
-                        "dedicated path",
+    return {"workload": f"{len(items)} QAOA MaxCut circuits (n 10..20, p 1..4), complex64, energies + gradients, "
+                        "dedicated path" + (f" (only n = {qubits})" if qubits else ""),
             "ms_call": best, "circuits_per_s": len(items) / (best / 1000.0),
             "timing": "wall time of the whole gq_qaoa_maxcut_batch call (host tables, upload, launches, results); "
                       "records packed once beforehand",
@@ -841,7 +846,8 @@ def main():
     if args.only_extra:
         fns = {"parity_20q": extra_parity, "adjoint": extra_adjoint, "density_matrix": extra_density,
                "parity_28q": extra_parity_28q, "vqe_loop": extra_vqe, "cold_start": extra_cold_start,
-               "qaoa_dedicated": extra_qaoa_dedicated, "sampling": extra_sampling,
+               "qaoa_dedicated": lambda: extra_qaoa_dedicated(args.qaoa_qubits, args.qaoa_count),
+               "sampling": extra_sampling,
                "qaoa_batch": lambda: extra_qaoa(args.qaoa_qubits, args.qaoa_count, args.qaoa_calls,
                                                 args.qaoa_graph == 1)}
         print(json.dumps({args.only_extra: fns[args.only_extra]()}))
