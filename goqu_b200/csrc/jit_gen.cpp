@@ -175,6 +175,14 @@ void put_key(std::string& k, const V& v) {
 }
 }  // namespace
 
+// Whether the `count` pool entries from `at` are all real (the generator then
+// emits the real-matrix op bodies, which read only the real parts).
+static bool pool_real(const Program& pr, uint32_t at, uint32_t count) {
+    for (uint32_t k = 0; k < count; ++k)
+        if (pr.pool[at + k].im != 0.0) return false;
+    return true;
+}
+
 std::string jit_plan_key(const Program& pr, size_t pi, bool c64, int threads, int min_blocks, bool persistent,
                          bool dual) {
     const PassDesc& pd = pr.passes[pi];
@@ -209,11 +217,17 @@ std::string jit_plan_key(const Program& pr, size_t pi, bool c64, int threads, in
             put_key(key, op.cmask);
             put_key(key, op.dmask);
             put_key(key, op.ridx);
+            bool dense = op.type == K_U1 && op.cmask;
             if (op.type == K_U1 && !op.cmask) {
                 double t;
                 Z l, a, c;
-                put_key(key, (int)u1_decompose(&pr.pool[op.mat], &t, &l, &a, &c));
+                const bool dec = u1_decompose(&pr.pool[op.mat], &t, &l, &a, &c);
+                put_key(key, (int)dec);
+                dense = !dec;
             }
+            // dense one- and two-qubit matrices with real entries take the real op bodies
+            if (!dual && dense) put_key(key, (int)pool_real(pr, op.mat, 4));
+            if (!dual && op.type == K_U2) put_key(key, (int)pool_real(pr, op.mat, 16));
         }
     }
     if (!dual)  // which one-qubit chains the forward kernel fuses
@@ -699,16 +713,19 @@ PlanResult plan_forward(const Program& pr, size_t pi, bool c64, int threads, int
                         out.phase_shears.back().push_back((uint32_t)o);
                     } else {
                         for (const auto& g : groups(tm, op.creg)) normalize(g);
-                        b += "        " + cond + "k_u1<T, " + S0 + ", " + C + ">(a, " + pm(gen.copy(rm, 4)) +
-                             ", " + creg + ");\n";
+                        const char* fn = pool_real(pr, op.mat, 4) ? "k_u1r<T, " : "k_u1<T, ";
+                        b += "        " + cond + fn + S0 + ", " + C + ">(a, " + pm(gen.copy(rm, 4)) + ", " + creg +
+                             ");\n";
                     }
                     break;
                 }
-                case K_U2:
+                case K_U2: {
                     for (const auto& g : groups((1u << op.t0) | (1u << op.t1), op.creg)) normalize(g);
-                    b += "        " + cond + "k_u2<T, " + S0 + ", " + S1 + ", " + C + ">(a, " +
-                         pm(gen.copy(rm, 16)) + ", " + creg + ");\n";
+                    const char* fn = pool_real(pr, op.mat, 16) ? "k_u2r<T, " : "k_u2<T, ";
+                    b += "        " + cond + fn + S0 + ", " + S1 + ", " + C + ">(a, " + pm(gen.copy(rm, 16)) + ", " +
+                         creg + ");\n";
                     break;
+                }
                 case K_U3:
                     for (const auto& g : groups((1u << op.t0) | (1u << op.t1) | (1u << op.t2), op.creg)) normalize(g);
                     b += "        " + cond + "k_u3<T, " + S0 + ", " + S1 + ", " + S2 + ">(a, " +

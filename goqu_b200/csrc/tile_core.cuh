@@ -217,6 +217,21 @@ GQ_HD void k_u1(cplx<T> (&a)[NREG], MP m, uint32_t creg) {
     }
 }
 
+// The same for a real matrix (only the real parts of m are read): each
+// output takes two real multiply-adds per component instead of four.
+template <class T, int S, bool C, class MP>
+GQ_HD void k_u1r(cplx<T> (&a)[NREG], MP m, uint32_t creg) {
+    const T m0 = ldc(m, 0).x, m1 = ldc(m, 1).x, m2 = ldc(m, 2).x, m3 = ldc(m, 3).x;
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (j & (1 << S)) continue;
+        if (C && (j & creg) != creg) continue;
+        const cplx<T> a0 = a[j], a1 = a[j | (1 << S)];
+        a[j] = {m0 * a0.x + m1 * a1.x, m0 * a0.y + m1 * a1.y};
+        a[j | (1 << S)] = {m2 * a0.x + m3 * a1.x, m2 * a0.y + m3 * a1.y};
+    }
+}
+
 template <class T, int S0, int S1, bool C, class MP>
 GQ_HD void k_u2(cplx<T> (&a)[NREG], MP m, uint32_t creg) {
 #pragma unroll
@@ -233,6 +248,31 @@ GQ_HD void k_u2(cplx<T> (&a)[NREG], MP m, uint32_t creg) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) o = cfma(ldc_v(m, r * 4 + c), v[c], o);
             a[idx[r]] = o;
+        }
+    }
+}
+
+// A real 4x4 matrix (only the real parts of m are read).
+template <class T, int S0, int S1, bool C, class MP>
+GQ_HD void k_u2r(cplx<T> (&a)[NREG], MP m, uint32_t creg) {
+#pragma unroll
+    for (int j = 0; j < NREG; ++j) {
+        if (j & ((1 << S0) | (1 << S1))) continue;
+        if (C && (j & creg) != creg) continue;
+        const int idx[4] = {j, j | (1 << S0), j | (1 << S1), j | (1 << S0) | (1 << S1)};
+        cplx<T> v[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[c] = a[idx[c]];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            T ox = T(0), oy = T(0);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const T mr = ldc_v(m, r * 4 + c).x;
+                ox += mr * v[c].x;
+                oy += mr * v[c].y;
+            }
+            a[idx[r]] = {ox, oy};
         }
     }
 }
